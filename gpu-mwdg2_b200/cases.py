@@ -1,0 +1,274 @@
+"""Seeded synthetic inputs in the reference's file formats.
+
+Writes `.par`, ESRI-ASCII `.dem`/`.start`, `.bci`, `.bdy` and `.stage` files in the
+dialect the reference reads (keyword readers `input/read_keyword_*.cpp`, raster reader
+`input/read_raster_file.cpp:26-46`, boundary/point-source readers
+`classes/Boundary.h`, `classes/PointSources.h:251-279`, time series
+`classes/Boundary.h:427-466`, stage points `classes/StagePoints.h:124-137`).
+
+The same files feed this library, the CPU oracle and the reference build, so every
+implementation sees byte-identical inputs. Generators:
+
+* circular_dam_break  - flat bed, closed walls, radial depth step.
+* fbm_catchment       - fractional-Brownian-motion DEM, dry start, west-edge point
+                        inflow with a triangular hydrograph.
+* lake_at_rest        - still water over an fBm bed (well-balancing checks).
+
+Reference quirks the generators respect (they would otherwise change the physics):
+* `wall_height` is set above every bed value, because `operators/dg2_update.cu:46`
+  skips cells whose bed equals `wall_height` (a flat bed with wall_height 0 would
+  never update).
+* `initial_tstep` is always written, because dry cells report it as their CFL step
+  (`operators/dg2_update.cu:61`); a missing value makes dt collapse to 0.
+* Time series are padded beyond `sim_time`, because the interpolation in
+  `classes/PointSources.h:429-450` reads one row past the current one.
+* A point inflow of Q m^3/s is written as Q/dx, because `mra/reinsert_point_srcs.cu:25`
+  adds value*dt/dx to the free surface (the value is a unit-width discharge).
+"""
+from __future__ import annotations
+
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+# ----------------------------------------------------------------------------- writers
+
+def _format_grid(values: np.ndarray, decimals: int) -> bytes:
+    """Fast fixed-point ASCII formatting of a 2-D array, rows separated by newlines.
+
+    Values are rounded to `decimals` places and printed as plain decimals; the
+    result is byte-identical to '%.{decimals}f' for |v| < 1e12.
+    """
+    v = np.asarray(values, dtype=np.float64)
+    scale = 10 ** decimals
+    q = np.rint(v * scale).astype(np.int64)
+    neg = q < 0
+    a = np.abs(q)
+    ip = a // scale
+    fp = a % scale
+    # integer part digits (up to 12), fraction digits fixed width
+    nd_int = np.maximum(1, np.floor(np.log10(np.maximum(ip, 1))).astype(np.int64) + 1)
+    width = nd_int + neg.astype(np.int64) + (1 + decimals if decimals > 0 else 0)
+    rows, cols = v.shape
+    # each value followed by a separator (space, or newline at row end)
+    tot = width + 1
+    offs = np.concatenate([[0], np.cumsum(tot.ravel())])
+    out = np.full(int(offs[-1]), ord(" "), dtype=np.uint8)
+    start = offs[:-1].reshape(rows, cols)
+    flat_start = start.ravel()
+    flat_neg = neg.ravel()
+    flat_nd = nd_int.ravel()
+    flat_ip = ip.ravel()
+    flat_fp = fp.ravel()
+    out[flat_start[flat_neg]] = ord("-")
+    pos0 = flat_start + flat_neg.astype(np.int64)
+    max_nd = int(flat_nd.max()) if flat_nd.size else 1
+    for d in range(max_nd):
+        has = flat_nd > d
+        digit = (flat_ip // (10 ** (flat_nd - 1 - d).clip(0))) % 10
+        out[(pos0 + d)[has]] = (ord("0") + digit[has]).astype(np.uint8)
+    if decimals > 0:
+        dot = pos0 + flat_nd
+        out[dot] = ord(".")
+        for d in range(decimals):
+            digit = (flat_fp // 10 ** (decimals - 1 - d)) % 10
+            out[dot + 1 + d] = (ord("0") + digit).astype(np.uint8)
+    ends = (start + width)[:, -1]
+    out[ends] = ord("\n")
+    return out.tobytes()
+
+
+def write_esri_ascii(path: str, grid_north_up: np.ndarray, cellsize: float,
+                     xll: float = 0.0, yll: float = 0.0, decimals: int = 6) -> None:
+    """Write an ESRI ASCII raster; `grid_north_up[0]` is the northernmost row."""
+    nrows, ncols = grid_north_up.shape
+    header = (f"ncols        {ncols}\nnrows        {nrows}\nxllcorner    {xll:g}\n"
+              f"yllcorner    {yll:g}\ncellsize     {cellsize!r}\nNODATA_value -9999\n")
+    with open(path, "wb") as fp:
+        fp.write(header.encode())
+        fp.write(_format_grid(grid_north_up, decimals))
+
+
+@dataclass
+class Case:
+    """A generated case: the .par path plus what was generated (for tests and bench)."""
+    par: str
+    directory: str
+    L: int
+    solver: str
+    cellsize: float
+    sim_time: float
+    dem: np.ndarray | None = None          # south-up (row 0 = south), shape (ysz, xsz)
+    start_h: np.ndarray | None = None      # south-up
+    meta: dict = field(default_factory=dict)
+
+
+def _write_par(path: str, lines: list[str]) -> None:
+    with open(path, "w") as fp:
+        fp.write("\n".join(lines) + "\n")
+
+
+def _common_par(solver: str, L: int, eps: float, sim_time: float, wall_height: float,
+                manning: float, limitslopes: bool, tol_krivo: float, massint: float | None,
+                saveint: float | None, cfl: float | None, extra: list[str]) -> list[str]:
+    if solver not in ("mwdg2", "hwfv1"):
+        raise ValueError("solver must be 'mwdg2' or 'hwfv1'")
+    lines = [
+        solver,
+        "cuda",
+        f"max_ref_lvl   {L}",
+        f"epsilon       {eps!r}",
+        f"wall_height   {wall_height!r}",
+        "initial_tstep 1",
+        f"fpfric        {manning!r}",
+        f"sim_time      {sim_time!r}",
+    ]
+    if limitslopes:
+        lines += ["limitslopes", f"tol_Krivo     {tol_krivo!r}"]
+    if massint is not None:
+        lines.append(f"massint       {massint!r}")
+    if saveint is not None:
+        lines.append(f"saveint       {saveint!r}")
+    if cfl is not None:
+        # Not read by the reference (its CFL is fixed in classes/SolverParams.cu:18,23).
+        lines.append(f"CFL           {cfl!r}")
+    return lines + extra
+
+
+def _write_stage(path: str, points: list[tuple[float, float]]) -> None:
+    with open(path, "w") as fp:
+        fp.write(f"{len(points)}\n")
+        for x, y in points:
+            fp.write(f"{x!r} {y!r}\n")
+
+
+# ----------------------------------------------------------------------------- cases
+
+def circular_dam_break(directory: str, L: int = 8, solver: str = "mwdg2", eps: float = 1e-3,
+                       sim_time: float = 3.5, domain: float = 50.0, radius: float = 2.5,
+                       h_in: float = 2.5, h_out: float = 0.5, limitslopes: bool = True,
+                       tol_krivo: float = 10.0, massint: float | None = 0.1,
+                       cfl: float | None = None, manning: float = 0.0,
+                       stage_points: list[tuple[float, float]] | None = None) -> Case:
+    """Circular dam break on a flat bed with closed walls (BASELINE config 1 shape).
+
+    The start raster holds h = h_in inside `radius` of the domain centre and h_out
+    outside, sampled at raster-cell centres. The bed is 0 and `wall_height` is 100.
+    """
+    os.makedirs(directory, exist_ok=True)
+    n = 1 << L
+    dx = domain / n
+    c = (np.arange(n) + 0.5) * dx
+    X, Y = np.meshgrid(c, c)                       # Y increases northwards (south-up)
+    r = np.hypot(X - domain / 2, Y - domain / 2)
+    h = np.where(r < radius, h_in, h_out)
+    dem = np.zeros((n, n))
+    write_esri_ascii(os.path.join(directory, "case.dem"), dem[::-1], dx, decimals=1)
+    write_esri_ascii(os.path.join(directory, "case.start"), h[::-1], dx, decimals=3)
+    if stage_points is None:
+        stage_points = [(domain / 2 + dx / 2, domain / 2 + dx / 2),
+                        (domain / 2 + 5.0, domain / 2 + dx / 2),
+                        (domain / 2 + 10.0, domain / 2 + 7.5),
+                        (domain / 2 - 12.5, domain / 2 - 12.5)]
+    _write_stage(os.path.join(directory, "case.stage"), stage_points)
+    lines = _common_par(solver, L, eps, sim_time, 100.0, manning, limitslopes, tol_krivo,
+                        massint, None, cfl,
+                        ["DEMfile       case.dem", "startfile     case.start",
+                         "stagefile     case.stage"])
+    par = os.path.join(directory, "case.par")
+    _write_par(par, lines)
+    return Case(par=par, directory=directory, L=L, solver=solver, cellsize=dx,
+                sim_time=sim_time, dem=dem, start_h=h,
+                meta={"kind": "circular_dam_break", "radius": radius})
+
+
+def fbm_surface(n: int, hurst: float, seed: int, relief: float) -> np.ndarray:
+    """Fractional Brownian surface by spectral synthesis, rescaled to [0, relief].
+
+    Amplitude ~ k^-(H+1) with uniformly random phases (PCG64 stream `seed`).
+    """
+    rng = np.random.Generator(np.random.PCG64(seed))
+    kx = np.fft.fftfreq(n)[None, :]
+    ky = np.fft.fftfreq(n)[:, None]
+    k = np.hypot(kx, ky)
+    k[0, 0] = 1.0
+    amp = k ** (-(hurst + 1.0))
+    amp[0, 0] = 0.0
+    phase = rng.uniform(0.0, 2.0 * np.pi, size=(n, n))
+    spec = amp * np.exp(1j * phase)
+    z = np.real(np.fft.ifft2(spec))
+    z -= z.min()
+    zmax = z.max()
+    if zmax > 0:
+        z *= relief / zmax
+    return z
+
+
+def fbm_catchment(directory: str, L: int = 12, solver: str = "mwdg2", eps: float = 1e-3,
+                  sim_time: float = 7200.0, cellsize: float = 2.0, hurst: float = 0.8,
+                  relief: float = 30.0, manning: float = 0.03, peak_q: float = 50.0,
+                  t_peak: float = 1800.0, seed: int = 20261203, massint: float | None = None,
+                  limitslopes: bool = False, tol_krivo: float = 10.0,
+                  cfl: float | None = None, start_depth: np.ndarray | None = None,
+                  stage_points: list[tuple[float, float]] | None = None) -> Case:
+    """fBm catchment with a west-edge point inflow (BASELINE config 2 shape).
+
+    Dry start unless `start_depth` (south-up array) is given. The inflow is a
+    triangular hydrograph 0 -> peak_q m^3/s at t_peak -> 0 at 2*t_peak, written as
+    unit-width discharge peak_q/cellsize, padded to 2*sim_time + 2*t_peak.
+    """
+    os.makedirs(directory, exist_ok=True)
+    n = 1 << L
+    dem = fbm_surface(n, hurst, seed, relief)
+    write_esri_ascii(os.path.join(directory, "case.dem"), dem[::-1], cellsize, decimals=3)
+    extra = ["DEMfile       case.dem", "bcifile       case.bci", "bdyfile       case.bdy"]
+    if start_depth is not None:
+        write_esri_ascii(os.path.join(directory, "case.start"), start_depth[::-1], cellsize,
+                         decimals=4)
+        extra.append("startfile     case.start")
+    y_src = (n // 2) * cellsize + cellsize / 2
+    with open(os.path.join(directory, "case.bci"), "w") as fp:
+        fp.write(f"P {cellsize / 2!r} {y_src!r} QVAR HYD\n")
+    t_end = max(2.0 * sim_time, 2.0 * t_peak) + 2.0 * t_peak
+    rows = [(0.0, 0.0), (peak_q / cellsize, t_peak), (0.0, 2.0 * t_peak), (0.0, t_end),
+            (0.0, t_end + t_peak)]
+    with open(os.path.join(directory, "case.bdy"), "w") as fp:
+        fp.write("inflow hydrograph\nHYD\n")
+        fp.write(f"{len(rows)} seconds\n")
+        for v, t in rows:
+            fp.write(f"{v!r} {t!r}\n")
+    if stage_points is None:
+        ext = n * cellsize
+        stage_points = [(ext * 0.25 + cellsize / 2, ext * 0.5 + cellsize / 2),
+                        (ext * 0.5 + cellsize / 2, ext * 0.5 + cellsize / 2)]
+    _write_stage(os.path.join(directory, "case.stage"), stage_points)
+    extra.append("stagefile     case.stage")
+    lines = _common_par(solver, L, eps, sim_time, 1000.0, manning, limitslopes, tol_krivo,
+                        massint, None, cfl, extra)
+    par = os.path.join(directory, "case.par")
+    _write_par(par, lines)
+    return Case(par=par, directory=directory, L=L, solver=solver, cellsize=cellsize,
+                sim_time=sim_time, dem=dem, start_h=start_depth,
+                meta={"kind": "fbm_catchment", "seed": seed, "hurst": hurst})
+
+
+def lake_at_rest(directory: str, L: int = 7, solver: str = "mwdg2", eps: float = 1e-3,
+                 sim_time: float = 1.0, cellsize: float = 1.0, level: float = 1.0,
+                 relief: float = 0.8, seed: int = 7, manning: float = 0.0,
+                 limitslopes: bool = False) -> Case:
+    """Still water at surface `level` over an fBm bed (h = max(0, level - z))."""
+    os.makedirs(directory, exist_ok=True)
+    n = 1 << L
+    dem = fbm_surface(n, 0.8, seed, relief)
+    h = np.maximum(0.0, level - dem)
+    write_esri_ascii(os.path.join(directory, "case.dem"), dem[::-1], cellsize, decimals=4)
+    write_esri_ascii(os.path.join(directory, "case.start"), h[::-1], cellsize, decimals=4)
+    lines = _common_par(solver, L, eps, sim_time, 1000.0, manning, limitslopes, 10.0,
+                        None, None, None,
+                        ["DEMfile       case.dem", "startfile     case.start"])
+    par = os.path.join(directory, "case.par")
+    _write_par(par, lines)
+    return Case(par=par, directory=directory, L=L, solver=solver, cellsize=cellsize,
+                sim_time=sim_time, dem=dem, start_h=h, meta={"kind": "lake_at_rest"})
