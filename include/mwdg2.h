@@ -1,0 +1,126 @@
+/*
+ * mwdg2.h -- C ABI of the B200-native adaptive MWDG2/HWFV1 shallow-water time step.
+ *
+ * Drop-in boundary for the reference (al0vya/gpu-mwdg2). The reference has no library
+ * interface: its boundary is the process entry
+ *     gpu-mwdg2 [-epsilon e] [-solver hwfv1|mwdg2] [-dirroot d] case.par
+ * (source/MAIN.cu:3-24, source/input/read_command_line_params.cpp:3-47) and the
+ * in-process call
+ *     void run_simulation(int argc, char** argv)      (source/run_simulation.cuh:60-63).
+ * This header replaces the second with status-returning entry points; the
+ * `gpu-mwdg2` executable built from this library replaces the first.
+ *
+ * Conventions: every call returns mwdg2_status; no call exits the process; memory is
+ * owned by the library; one mwdg2_sim per host thread (calls on the same handle must
+ * not overlap). Arrays are plain host pointers. Leaf arrays are in the reference's
+ * leaf order (Z-order of the non-uniform grid, source/mra/traverse_tree_of_sig_details.cu)
+ * and hierarchy indices follow get_lvl_idx (source/utilities/get_lvl_idx.cuh:6-24).
+ */
+#ifndef MWDG2_H
+#define MWDG2_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum mwdg2_status
+{
+    MWDG2_OK          = 0,
+    MWDG2_ERR_IO      = 1,  /* an input file is missing or unreadable */
+    MWDG2_ERR_PARSE   = 2,  /* an input is malformed or unsupported */
+    MWDG2_ERR_CUDA    = 3,  /* a CUDA call failed or no device is available */
+    MWDG2_ERR_NUMERIC = 4,  /* NaN or negative depth detected in the state */
+    MWDG2_ERR_TIMEOUT = 5,  /* a bounded device wait gave up */
+    MWDG2_ERR_ARG     = 6,  /* invalid argument (null handle, short buffer, ...) */
+    MWDG2_ERR_STATE   = 7,  /* call not valid in the current state (e.g. run finished) */
+    MWDG2_DONE        = 8   /* mwdg2_step: simulated time already reached; nothing done */
+} mwdg2_status;
+
+typedef struct mwdg2_sim mwdg2_sim;
+
+typedef struct mwdg2_opts
+{
+    int         precision;        /* 32 or 64 (arithmetic type of the state); 0 = 64 */
+    int         device;           /* CUDA device ordinal; -1 = current */
+    double      epsilon;          /* < 0: take from the .par (CLI -epsilon) */
+    int         solver;           /* 0: from the .par; 1: HWFV1; 2: MWDG2 (CLI -solver) */
+    const char* dirroot;          /* NULL: from the .par (CLI -dirroot) */
+    int         write_outputs;    /* 1: write res.stage / res.cumu as the reference does */
+    int         verbose;          /* 1: print the reference's progress lines */
+} mwdg2_opts;
+
+/* Fill opts with defaults (precision 64, device -1, epsilon -1, solver 0, dirroot NULL,
+ * write_outputs 1, verbose 0). */
+void mwdg2_default_opts(mwdg2_opts* opts);
+
+/* Text of the last error on this thread (never NULL). */
+const char* mwdg2_last_error(void);
+
+/* Read the case and set up device state (replaces the initialisation part of
+ * run_simulation, source/run_simulation.cu:9-222). Relative file names in the .par are
+ * opened relative to the working directory, as the reference does. */
+mwdg2_status mwdg2_create(const char* par_path, const mwdg2_opts* opts, mwdg2_sim** out);
+
+/* Advance one adaptive time step (one iteration of run_simulation.cu:226-774).
+ * dt_out: the CFL step computed at the end of this step (the next step's dt);
+ * n_leaves_out: number of leaves (active cells) updated in this step.
+ * Returns MWDG2_DONE without work once the simulated time has reached sim_time. */
+mwdg2_status mwdg2_step(mwdg2_sim* sim, double* dt_out, int64_t* n_leaves_out);
+
+/* Advance up to max_steps steps (<= 0: until sim_time), writing outputs at massint as
+ * the reference does. steps_done_out and leaf_updates_out may be NULL. */
+mwdg2_status mwdg2_run(mwdg2_sim* sim, int64_t max_steps, int64_t* steps_done_out,
+                       int64_t* leaf_updates_out);
+
+/* Whole-process replacement of run_simulation(argc, argv): parse the reference's
+ * command line, create, run to sim_time with outputs, destroy. */
+mwdg2_status mwdg2_run_simulation(int argc, char** argv);
+
+/* Scalars: [0] current time, [1] dt, [2] timestep counter (next step number),
+ * [3] n_leaves, [4] max_ref_lvl, [5] xsz, [6] ysz, [7] dx, [8] epsilon, [9] solver,
+ * [10] precision, [11] sim_time, [12] n_details (get_lvl_idx(L)),
+ * [13] n_hierarchy (get_lvl_idx(L+1)). n must be >= 14. */
+mwdg2_status mwdg2_info(mwdg2_sim* sim, double* out, int n);
+
+/* Leaf list of the current grid: hierarchy index and level of each leaf, and its four
+ * neighbours (north, east, south, west) as hierarchy index (-1 at the domain border)
+ * and level, laid out [4][n]. Any pointer may be NULL. cap: capacity in leaves. */
+mwdg2_status mwdg2_get_leaves(mwdg2_sim* sim, int32_t* act_idcs, int32_t* levels,
+                              int32_t* nb_ids, int32_t* nb_levels, int64_t cap);
+
+/* Leaf state after the last step, 12 rows of n values laid out [12][n]:
+ * h0 qx0 qy0 z0 h1x qx1x qy1x z1x h1y qx1y qy1y z1y (HWFV1: the slope rows are 0). */
+mwdg2_status mwdg2_get_state(mwdg2_sim* sim, double* out, int64_t cap);
+
+/* Significance flags of all parents (n_details bytes, 1 = significant). */
+mwdg2_status mwdg2_get_sig(mwdg2_sim* sim, uint8_t* out, int64_t cap);
+
+/* One hierarchy array: field 0 eta, 1 qx, 2 qy, 3 z; mode 0, 1 (1x), 2 (1y);
+ * n_hierarchy values. */
+mwdg2_status mwdg2_get_hierarchy(mwdg2_sim* sim, int field, int mode, double* out, int64_t cap);
+
+/* Depth h = eta - z of the leaf containing each stage point, in .stage file order
+ * (the value written to res.stage, source/output/write_stage_point_data.cu:155-186). */
+mwdg2_status mwdg2_read_stage(mwdg2_sim* sim, double* out, int n);
+
+/* Device timing of the last step's kernels, in milliseconds, by phase:
+ * [0] maxes+reinsert, [1] encode+regularise, [2] decode+extra significance,
+ * [3] leaf topology, [4] solver stage 1 (or FV1), [5] stage-2 (re-encode, gather, update),
+ * [6] whole step. Requires opts.verbose >= 2 at create (adds events); else zeros. */
+mwdg2_status mwdg2_last_step_timing(mwdg2_sim* sim, double* out, int n);
+
+/* Counters of the last step used for the algorithmic-bytes roofline:
+ * [0] parents encoded (E), [1] parents re-encoded scale-only (E2), [2] parents decoded (D),
+ * [3] leaves (N_a), [4] detail slots (T = get_lvl_idx(L) - 3). n >= 5. */
+mwdg2_status mwdg2_last_step_counters(mwdg2_sim* sim, int64_t* out, int n);
+
+void mwdg2_destroy(mwdg2_sim* sim);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MWDG2_H */
