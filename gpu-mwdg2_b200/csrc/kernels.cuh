@@ -1,0 +1,647 @@
+// CUDA kernels of the adaptive MWDG2/HWFV1 time step for sm_100a.
+//
+// Data layout in HBM (one simulation):
+//   hierarchy  s[field][mode][h]   field eta,qx,qy,z; mode 0,1x,1y; h = get_lvl_idx(level)+Morton
+//   details    det[field][t*3+m][p] field eta,qx,qy; t alpha,beta,gamma; parents only
+//   norm[p], flags[p]              parents only (levels 0..L-1); flag bits F_SIG/F_ENC/F_PRE
+//   leaves     act, lvl, nb[4], nbl[4], un[9] (state), us[9] (RK stage-1 result), in Z order
+//
+// Work per step touches the significant part of the tree and the leaves only; no array
+// is cleared per step (the F_ENC bit marks which parents hold fresh details).
+#pragma once
+
+#include "mw_math.cuh"
+
+namespace mw {
+
+constexpr int kTileDepth = 5;        // a leaf-enumeration tile covers 4^5 finest cells
+constexpr int kTileThreads = 256;
+constexpr int kSolverThreads = 128;
+
+template <typename T> struct Hier
+{
+    T* s[4][3];
+    T* det[3][9];
+    T* norm;
+    uint8_t* flags;
+};
+
+template <typename T> struct Leaves
+{
+    int32_t* act;
+    uint8_t* lvl;
+    int32_t* nb[4];
+    uint8_t* nbl[4];
+    T* un[9];   // [field*3 + mode], field h, qx, qy
+    T* us[9];
+};
+
+template <typename T> struct Scalars
+{
+    T max_eta, max_h, max_qx, max_z;  // raw maxima of |.| over leaves (floored at 1 by users)
+    T max_h2;                         // max |h0| for the stage-2 limiter (not floored)
+    T dt_min;
+    int32_t n_leaves;
+    int32_t status;                   // bit 0: NaN seen in the state
+    unsigned long long enc, enc2, dec;
+};
+
+template <typename T> struct Params
+{
+    int L, M, xsz, ysz, limit;
+    T dx, tol_h, tol_q, tol_s, g, manning, CFL, initial_tstep, wall_height, tol_Krivo, eps;
+};
+
+template <typename T> struct Bnd
+{
+    int start[4], end[4], type[4];   // N, E, S, W
+    T inlet[4];
+};
+
+template <typename T> struct Src { int code, type; T value; };
+
+// ---------------------------------------------------------------- atomics on non-negative reals
+__device__ __forceinline__ void atomic_max_nn(double* a, double v)
+{
+    atomicMax(reinterpret_cast<unsigned long long*>(a), (unsigned long long)__double_as_longlong(v));
+}
+__device__ __forceinline__ void atomic_max_nn(float* a, float v)
+{
+    atomicMax(reinterpret_cast<unsigned int*>(a), __float_as_uint(v));
+}
+__device__ __forceinline__ void atomic_min_nn(double* a, double v)
+{
+    atomicMin(reinterpret_cast<unsigned long long*>(a), (unsigned long long)__double_as_longlong(v));
+}
+__device__ __forceinline__ void atomic_min_nn(float* a, float v)
+{
+    atomicMin(reinterpret_cast<unsigned int*>(a), __float_as_uint(v));
+}
+
+template <typename T> __device__ __forceinline__ T warp_max(T v)
+{
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+template <typename T> __device__ __forceinline__ T warp_min(T v)
+{
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Block-wide max of several values then one atomic per value per block.
+template <typename T, int N>
+__device__ __forceinline__ void block_max_atomic(T (&v)[N], T* const (&dst)[N])
+{
+    __shared__ T red[N][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < N; ++k) v[k] = warp_max(v[k]);
+    if (lane == 0)
+    {
+#pragma unroll
+        for (int k = 0; k < N; ++k) red[k][w] = v[k];
+    }
+    __syncthreads();
+    if (w == 0)
+    {
+        const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+        for (int k = 0; k < N; ++k)
+        {
+            T x = (lane < nw) ? red[k][lane] : T(0);
+            x = warp_max(x);
+            if (lane == 0) atomic_max_nn(dst[k], x);
+        }
+    }
+}
+
+// ---------------------------------------------------------------- step bookkeeping
+template <typename T> __global__ void k_step_begin(Scalars<T>* sc)
+{
+    sc->max_eta = T(0); sc->max_h = T(0); sc->max_qx = T(0); sc->max_z = T(0);
+    sc->max_h2 = T(0);
+    sc->dt_min = (sizeof(T) == 8) ? T(1.0e308) : T(3.0e38);
+    sc->enc = 0; sc->enc2 = 0; sc->dec = 0;
+}
+
+// Maxima of the leaf state (mra/get_max_scale_coeffs.cu:3-27, with the reference's
+// use of qx0 for the qy maximum) and re-insertion of the leaf state into the hierarchy
+// (mra/reinsert_assem_sol.cu:3-32).
+template <typename T, bool MW>
+__global__ void __launch_bounds__(256) k_maxes_reinsert(Leaves<T> lf, Hier<T> hr, Scalars<T>* sc, int n_fixed, bool reinsert)
+{
+    const int n = n_fixed >= 0 ? n_fixed : sc->n_leaves;
+    T me = T(0), mh = T(0), mq = T(0), mz = T(0);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        const int a = lf.act[i];
+        const T h0 = lf.un[0][i], qx0 = lf.un[3][i];
+        const T z0 = hr.s[3][0][a];
+        const T eta = h0 + z0;
+        me = fmax(me, fabs(eta));
+        mh = fmax(mh, fabs(h0));
+        mq = fmax(mq, fabs(qx0));
+        mz = fmax(mz, fabs(z0));
+        if (reinsert)
+        {
+            hr.s[0][0][a] = h0 + z0;
+            hr.s[1][0][a] = qx0;
+            hr.s[2][0][a] = lf.un[6][i];
+            if (MW)
+            {
+                hr.s[0][1][a] = lf.un[1][i] + hr.s[3][1][a];
+                hr.s[1][1][a] = lf.un[4][i];
+                hr.s[2][1][a] = lf.un[7][i];
+                hr.s[0][2][a] = lf.un[2][i] + hr.s[3][2][a];
+                hr.s[1][2][a] = lf.un[5][i];
+                hr.s[2][2][a] = lf.un[8][i];
+            }
+        }
+    }
+    T v[4] = {me, mh, mq, mz};
+    T* const dst[4] = {&sc->max_eta, &sc->max_h, &sc->max_qx, &sc->max_z};
+    block_max_atomic<T, 4>(v, dst);
+}
+
+// Point sources into the finest level (mra/reinsert_point_srcs.cu:3-29).
+template <typename T> __global__ void k_point_sources(Hier<T> hr, const Src<T>* src, int n, T dt, T dx, int L)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int h = lvl_idx(L) + src[i].code;
+    const int t = src[i].type;
+    if (t == HFIX || t == HVAR) hr.s[0][0][h] = src[i].value;
+    else if (t == QFIX || t == QVAR) hr.s[0][0][h] += src[i].value * dt / dx;
+}
+
+// ---------------------------------------------------------------- multiresolution analysis
+
+template <typename T> __device__ __forceinline__ void load4(const T* p, T (&out)[4])
+{
+    if constexpr (sizeof(T) == 4)
+    {
+        const float4 v = *reinterpret_cast<const float4*>(p);
+        out[0] = v.x; out[1] = v.y; out[2] = v.z; out[3] = v.w;
+    }
+    else
+    {
+        const double2 a = reinterpret_cast<const double2*>(p)[0];
+        const double2 b = reinterpret_cast<const double2*>(p)[1];
+        out[0] = a.x; out[1] = a.y; out[2] = b.x; out[3] = b.y;
+    }
+}
+template <typename T> __device__ __forceinline__ void store4(T* p, const T (&v)[4])
+{
+    if constexpr (sizeof(T) == 4)
+    {
+        *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+    }
+    else
+    {
+        reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+        reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+    }
+}
+
+// Epsilon of the threshold for a parent at `level` (mra/encode_flow_kernel_mw.cu:45);
+// levels below 4 use level 3's value, as the reference's single-block encode does
+// (mra/encode_flow_kernel_single_block_mw.cu:48).
+template <typename T> __device__ __forceinline__ T encode_eps(T eps, int L, int level)
+{
+    const int lv = (level >= 4) ? level : 3;
+    return eps / (1 << (L - lv));
+}
+
+// Encode one parent (mra/encode_flow_kernel_{mw,hw}.cu), threshold it and OR in the
+// children's significance (mra/regularisation_kernel.cu). FULL = false re-encodes scale
+// coefficients of significant parents only (run_simulation.cu:573-588).
+template <typename T, bool MW, bool FULL>
+__device__ __forceinline__ void encode_parent(const Hier<T>& hr, const Scalars<T>* sc, int L, int level, int idx, T eps,
+                                              unsigned& n_done)
+{
+    const int p = lvl_idx(level) + idx;
+    const uint8_t f = hr.flags[p];
+    const bool was_sig = (f & F_SIG) != 0;
+    const int c = lvl_idx(level + 1) + 4 * idx;
+    if (!FULL)
+    {
+        if (!was_sig) return;
+#pragma unroll
+        for (int fld = 0; fld < 3; ++fld)
+        {
+            if (MW)
+            {
+                T k[3][4];
+                load4(hr.s[fld][0] + c, k[0]); load4(hr.s[fld][1] + c, k[1]); load4(hr.s[fld][2] + c, k[2]);
+                T s[3];
+                mw_encode_scale(k, s);
+                hr.s[fld][0][p] = s[0]; hr.s[fld][1][p] = s[1]; hr.s[fld][2][p] = s[2];
+            }
+            else
+            {
+                T k[4];
+                load4(hr.s[fld][0] + c, k);
+                hr.s[fld][0][p] = hw_scale(k);
+            }
+        }
+        ++n_done;
+        return;
+    }
+    uint8_t nf = f & F_PRE;
+    if (was_sig)
+    {
+        nf |= F_ENC;
+        const T mx[3] = {fmax(T(1.0), sc->max_eta), fmax(T(1.0), sc->max_qx), fmax(T(1.0), sc->max_qx)};
+        T nd = T(0.0);
+#pragma unroll
+        for (int fld = 0; fld < 3; ++fld)
+        {
+            if (MW)
+            {
+                T k[3][4];
+                load4(hr.s[fld][0] + c, k[0]); load4(hr.s[fld][1] + c, k[1]); load4(hr.s[fld][2] + c, k[2]);
+                T s[3];
+                mw_encode_scale(k, s);
+                hr.s[fld][0][p] = s[0]; hr.s[fld][1][p] = s[1]; hr.s[fld][2][p] = s[2];
+                T d[3][3];
+                mw_encode_details(k, d);
+#pragma unroll
+                for (int t = 0; t < 3; ++t)
+#pragma unroll
+                    for (int m = 0; m < 3; ++m) hr.det[fld][t * 3 + m][p] = d[t][m];
+                nd = fmax(nd, mw_detail_max(d) / mx[fld]);
+            }
+            else
+            {
+                T k[4];
+                load4(hr.s[fld][0] + c, k);
+                hr.s[fld][0][p] = hw_scale(k);
+                const T a = hw_alpha(k), b = hw_beta(k), g = hw_gamma(k);
+                hr.det[fld][0][p] = a; hr.det[fld][3][p] = b; hr.det[fld][6][p] = g;
+                T m1 = fmax(fabs(a), fabs(b));
+                m1 = fmax(fabs(g), m1);
+                nd = fmax(nd, m1 / mx[fld]);
+            }
+        }
+        hr.norm[p] = nd;
+        if (nd >= encode_eps(eps, L, level) || (f & F_PRE)) nf |= F_SIG;
+        if (!(nf & F_SIG) && level <= L - 2)
+        {
+            const uint32_t ch = *reinterpret_cast<const uint32_t*>(hr.flags + c);
+            if (ch & 0x01010101u) nf |= F_SIG;
+        }
+        ++n_done;
+    }
+    hr.flags[p] = nf;
+}
+
+template <typename T, bool MW, bool FULL>
+__global__ void __launch_bounds__(256) k_encode_level(Hier<T> hr, Scalars<T>* sc, int L, int level, T eps)
+{
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned done = 0;
+    if (idx < (1 << (2 * level))) encode_parent<T, MW, FULL>(hr, sc, L, level, idx, eps, done);
+    const unsigned tot = __reduce_add_sync(0xffffffffu, done);
+    if ((threadIdx.x & 31) == 0 && tot) atomicAdd(FULL ? &sc->enc : &sc->enc2, (unsigned long long)tot);
+}
+
+// Levels `top`..0 in one block (bottom-up, __syncthreads between levels).
+template <typename T, bool MW, bool FULL>
+__global__ void __launch_bounds__(256) k_encode_top(Hier<T> hr, Scalars<T>* sc, int L, int top, T eps)
+{
+    unsigned done = 0;
+    for (int level = top; level >= 0; --level)
+    {
+        for (int idx = threadIdx.x; idx < (1 << (2 * level)); idx += blockDim.x)
+            encode_parent<T, MW, FULL>(hr, sc, L, level, idx, eps, done);
+        __syncthreads();
+    }
+    const unsigned tot = __reduce_add_sync(0xffffffffu, done);
+    if ((threadIdx.x & 31) == 0 && tot) atomicAdd(FULL ? &sc->enc : &sc->enc2, (unsigned long long)tot);
+}
+
+// Decode one significant parent into its four children (mra/decoding_kernel_{mw,hw}.cu)
+// and apply extra significance (mra/extra_significance_kernel.cu: parents whose norm
+// reaches eps_l * 2^(M_BAR+1) make all four children significant).
+template <typename T, bool MW>
+__device__ __forceinline__ void decode_parent(const Hier<T>& hr, int L, int level, int idx, T eps, unsigned& n_done)
+{
+    const int p = lvl_idx(level) + idx;
+    const uint8_t f = hr.flags[p];
+    if (!(f & F_SIG)) return;
+    const bool enc = (f & F_ENC) != 0;
+    const int c = lvl_idx(level + 1) + 4 * idx;
+#pragma unroll
+    for (int fld = 0; fld < 3; ++fld)
+    {
+        if (MW)
+        {
+            const T s[3] = {hr.s[fld][0][p], hr.s[fld][1][p], hr.s[fld][2][p]};
+            T d[3][3];
+#pragma unroll
+            for (int t = 0; t < 3; ++t)
+#pragma unroll
+                for (int m = 0; m < 3; ++m) d[t][m] = enc ? hr.det[fld][t * 3 + m][p] : T(0.0);
+            T k[3][4];
+            mw_decode(s, d, k);
+            store4(hr.s[fld][0] + c, k[0]); store4(hr.s[fld][1] + c, k[1]); store4(hr.s[fld][2] + c, k[2]);
+        }
+        else
+        {
+            const T u = hr.s[fld][0][p];
+            const T a = enc ? hr.det[fld][0][p] : T(0.0);
+            const T b = enc ? hr.det[fld][3][p] : T(0.0);
+            const T g = enc ? hr.det[fld][6][p] : T(0.0);
+            T k[4];
+            hw_decode(u, a, b, g, k);
+            store4(hr.s[fld][0] + c, k);
+        }
+    }
+    ++n_done;
+    if (level <= L - 2)
+    {
+        const T eps_local = eps / (1 << (L - level));
+        const T eps_extra = eps_local * pow(T(2.0), T(1.5) + 1);
+        const T nrm = enc ? hr.norm[p] : T(0.0);
+        if (nrm >= eps_extra) *reinterpret_cast<uint32_t*>(hr.flags + c) |= 0x01010101u;
+    }
+}
+
+template <typename T, bool MW>
+__global__ void __launch_bounds__(256) k_decode_level(Hier<T> hr, Scalars<T>* sc, int L, int level, T eps)
+{
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned done = 0;
+    if (idx < (1 << (2 * level))) decode_parent<T, MW>(hr, L, level, idx, eps, done);
+    const unsigned tot = __reduce_add_sync(0xffffffffu, done);
+    if ((threadIdx.x & 31) == 0 && tot) atomicAdd(&sc->dec, (unsigned long long)tot);
+}
+
+template <typename T, bool MW>
+__global__ void __launch_bounds__(256) k_decode_top(Hier<T> hr, Scalars<T>* sc, int L, int top, T eps)
+{
+    unsigned done = 0;
+    for (int level = 0; level <= top; ++level)
+    {
+        for (int idx = threadIdx.x; idx < (1 << (2 * level)); idx += blockDim.x)
+            decode_parent<T, MW>(hr, L, level, idx, eps, done);
+        __syncthreads();
+    }
+    const unsigned tot = __reduce_add_sync(0xffffffffu, done);
+    if ((threadIdx.x & 31) == 0 && tot) atomicAdd(&sc->dec, (unsigned long long)tot);
+}
+
+// Bed encoding of one level and preflagging (mra/encode_topography_kernel_{mw,hw}.cu).
+template <typename T, bool MW>
+__global__ void __launch_bounds__(256) k_topo_level(Hier<T> hr, Scalars<T>* sc, int L, int level, T eps)
+{
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (1 << (2 * level))) return;
+    const int p = lvl_idx(level) + idx, c = lvl_idx(level + 1) + 4 * idx;
+    const T eps_local = eps / (1 << (L - level));
+    const T mz = fmax(T(1.0), sc->max_z);
+    T mx;
+    if (MW)
+    {
+        T k[3][4];
+        load4(hr.s[3][0] + c, k[0]); load4(hr.s[3][1] + c, k[1]); load4(hr.s[3][2] + c, k[2]);
+        T s[3];
+        mw_encode_scale(k, s);
+        hr.s[3][0][p] = s[0]; hr.s[3][1][p] = s[1]; hr.s[3][2][p] = s[2];
+        T d[3][3];
+        mw_encode_details(k, d);
+        mx = mw_detail_max(d);
+    }
+    else
+    {
+        T k[4];
+        load4(hr.s[3][0] + c, k);
+        const T a = hw_alpha(k), b = hw_beta(k), g = hw_gamma(k);
+        hr.s[3][0][p] = hw_scale(k);
+        T m1 = fmax(fabs(a), fabs(b));
+        mx = fmax(fabs(g), m1);
+    }
+    if ((mx / mz) >= eps_local) hr.flags[p] |= F_PRE;
+}
+
+// ---------------------------------------------------------------- leaf topology
+//
+// The significance flags are closed upwards (a significant node's parent is significant),
+// so the leaves of the subtree below a significant node r are 1 + 3 x (number of
+// significant nodes in that subtree). Tiles are the nodes of level T = L - D; each tile
+// counts its leaves, an exclusive scan gives output offsets, and each tile then writes
+// its leaves in Z order (depth-first order of the quadtree, as the reference's
+// traversal + compaction produce: mra/traverse_tree_of_sig_details.cu,
+// neighbours/compaction.cu).
+
+// First level on the root -> tile path whose node is not significant; Tl if none.
+__device__ __forceinline__ int tile_leaf_level(const uint8_t* flags, int Tl, int tcode)
+{
+    for (int j = 0; j < Tl; ++j)
+        if (!(flags[lvl_idx(j) + (tcode >> (2 * (Tl - j)))] & F_SIG)) return j;
+    return Tl;
+}
+
+__global__ void __launch_bounds__(kTileThreads) k_tile_count(const uint8_t* flags, int L, int D, int32_t* counts)
+{
+    const int Tl = L - D;
+    const int tcode = blockIdx.x;
+    __shared__ int s_k;
+    if (threadIdx.x == 0) s_k = tile_leaf_level(flags, Tl, tcode);
+    __syncthreads();
+    const int k = s_k;
+    if (k < Tl)
+    {
+        if (threadIdx.x == 0) counts[tcode] = ((tcode & ((1 << (2 * (Tl - k))) - 1)) == 0) ? 1 : 0;
+        return;
+    }
+    // significant nodes of the subtree, levels Tl .. L-1 (1 + 4 + ... + 4^(D-1) nodes)
+    const int nodes = ((1 << (2 * D)) - 1) / 3;
+    int cnt = 0;
+    for (int i = threadIdx.x; i < nodes; i += blockDim.x)
+    {
+        int j = 0, base = 0;
+        while (i >= base + (1 << (2 * j))) { base += 1 << (2 * j); ++j; }
+        const int node = lvl_idx(Tl + j) + (tcode << (2 * j)) + (i - base);
+        cnt += (flags[node] & F_SIG) ? 1 : 0;
+    }
+    __shared__ int s_cnt;
+    if (threadIdx.x == 0) s_cnt = 0;
+    __syncthreads();
+    cnt = __reduce_add_sync(0xffffffffu, cnt);
+    if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(&s_cnt, cnt);
+    __syncthreads();
+    if (threadIdx.x == 0) counts[tcode] = 1 + 3 * s_cnt;
+}
+
+// Exclusive scan of n tile counts in one block; total -> sc->n_leaves.
+template <typename T> __global__ void __launch_bounds__(1024) k_tile_scan(int32_t* counts, int n, Scalars<T>* sc)
+{
+    __shared__ int32_t part[1024];
+    const int per = (n + blockDim.x - 1) / blockDim.x;
+    const int lo = min(n, (int)threadIdx.x * per), hi = min(n, lo + per);
+    int32_t s = 0;
+    for (int i = lo; i < hi; ++i) s += counts[i];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = 1; o < (int)blockDim.x; o <<= 1)
+    {
+        const int32_t v = (threadIdx.x >= (unsigned)o) ? part[threadIdx.x - o] : 0;
+        __syncthreads();
+        part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    int32_t run = (threadIdx.x == 0) ? 0 : part[threadIdx.x - 1];
+    for (int i = lo; i < hi; ++i)
+    {
+        const int32_t c = counts[i];
+        counts[i] = run;
+        run += c;
+    }
+    if (threadIdx.x == blockDim.x - 1) sc->n_leaves = part[blockDim.x - 1];
+}
+
+// Neighbour of a leaf (level l, finest reference cell code `ref`) across the finest cell
+// (tx, ty): the ancestor of the leaf containing that cell at min(l, its level)
+// (neighbours/find_neighbours.cu:100-108). Descends from the first level where the
+// two cells' paths differ, since all shared ancestors of a leaf are significant.
+__device__ __forceinline__ void descend(const uint8_t* flags, int L, int l, int ref, int tx, int ty, int32_t& id, uint8_t& lv)
+{
+    const int tc = morton(tx, ty);
+    const int b = 31 - __clz(tc ^ ref);
+    int j = L - (b >> 1);
+    if (j < 0) j = 0;
+    while (true)
+    {
+        const int node = lvl_idx(j) + (tc >> (2 * (L - j)));
+        if (j >= l) { id = node; lv = (uint8_t)l; return; }
+        if (!(flags[node] & F_SIG)) { id = node; lv = (uint8_t)j; return; }
+        ++j;
+    }
+}
+
+// Four neighbours of a leaf (north/east from its north-east finest cell, south/west from
+// its south-west finest cell; -1 and the leaf's level at the DEM or mesh border:
+// neighbours/find_neighbours.cu:51-428, neighbours/compaction.cu:109-151).
+__device__ __forceinline__ void leaf_neighbours(const uint8_t* flags, int L, int M, int xsz, int ysz, int act, int l,
+                                                int32_t (&id)[4], uint8_t (&lv)[4])
+{
+    const int code = act - lvl_idx(l);
+    const int x = compact(code), y = compact(code >> 1);
+    const int s = 1 << (L - l);
+    const int x0 = x * s, y0 = y * s, xe = x0 + s - 1, ye = y0 + s - 1;
+    const int ref = morton(x0, y0);
+    // north-east cell
+    {
+        const bool northern = (ye == M - 1 || ye == ysz - 1), southern = (ye == 0);
+        const bool eastern = (xe == M - 1 || xe == xsz - 1), western = (xe == 0);
+        if (northern && !southern) { id[0] = -1; lv[0] = (uint8_t)l; }
+        else descend(flags, L, l, ref, xe, ye + 1, id[0], lv[0]);
+        if (eastern && !western) { id[1] = -1; lv[1] = (uint8_t)l; }
+        else descend(flags, L, l, ref, xe + 1, ye, id[1], lv[1]);
+    }
+    // south-west cell
+    {
+        if (y0 == 0) { id[2] = -1; lv[2] = (uint8_t)l; }
+        else descend(flags, L, l, ref, x0, y0 - 1, id[2], lv[2]);
+        if (x0 == 0) { id[3] = -1; lv[3] = (uint8_t)l; }
+        else descend(flags, L, l, ref, x0 - 1, y0, id[3], lv[3]);
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void emit_leaf(const Leaves<T>& lf, const uint8_t* flags, int L, int M, int xsz, int ysz,
+                                          int pos, int act, int l)
+{
+    lf.act[pos] = act;
+    lf.lvl[pos] = (uint8_t)l;
+    int32_t id[4];
+    uint8_t lv[4];
+    leaf_neighbours(flags, L, M, xsz, ysz, act, l, id, lv);
+#pragma unroll
+    for (int d = 0; d < 4; ++d) { lf.nb[d][pos] = id[d]; lf.nbl[d][pos] = lv[d]; }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kTileThreads) k_tile_emit(Leaves<T> lf, const uint8_t* flags, const int32_t* offsets,
+                                                            int L, int D, int M, int xsz, int ysz)
+{
+    const int Tl = L - D;
+    const int tcode = blockIdx.x;
+    const int off = offsets[tcode];
+    __shared__ int s_k;
+    __shared__ uint32_t bits[32];      // leaf starts among the tile's 4^D (<= 1024) finest cells
+    __shared__ int32_t prefix[33];
+    if (threadIdx.x == 0) s_k = tile_leaf_level(flags, Tl, tcode);
+    if (threadIdx.x < 32) bits[threadIdx.x] = 0;
+    __syncthreads();
+    const int k = s_k;
+    if (k < Tl)
+    {
+        if (threadIdx.x == 0 && (tcode & ((1 << (2 * (Tl - k))) - 1)) == 0)
+            emit_leaf(lf, flags, L, M, xsz, ysz, off, lvl_idx(k) + (tcode >> (2 * (Tl - k))), k);
+        return;
+    }
+    const int root = lvl_idx(Tl) + tcode;
+    if (!(flags[root] & F_SIG))
+    {
+        if (threadIdx.x == 0) emit_leaf(lf, flags, L, M, xsz, ysz, off, root, Tl);
+        return;
+    }
+    // nodes of levels Tl+1 .. L below the tile root: 4 + 16 + ... + 4^D
+    const int nodes = ((1 << (2 * (D + 1))) - 1) / 3 - 1;
+    for (int pass = 0; pass < 2; ++pass)
+    {
+        for (int i = threadIdx.x; i < nodes; i += blockDim.x)
+        {
+            int j = 1, base = 0;
+            while (i >= base + (1 << (2 * j))) { base += 1 << (2 * j); ++j; }
+            const int lc = i - base;                       // local code at level Tl + j
+            const int lev = Tl + j;
+            const int parent = lvl_idx(lev - 1) + (tcode << (2 * (j - 1))) + (lc >> 2);
+            const int node = lvl_idx(lev) + (tcode << (2 * j)) + lc;
+            const bool leaf = (flags[parent] & F_SIG) && (lev == L || !(flags[node] & F_SIG));
+            if (!leaf) continue;
+            const int start = lc << (2 * (D - j));         // first finest cell, local to the tile
+            if (pass == 0)
+            {
+                atomicOr(&bits[start >> 5], 1u << (start & 31));
+            }
+            else
+            {
+                const int w = start >> 5;
+                const int rank = prefix[w] + __popc(bits[w] & ((1u << (start & 31)) - 1u));
+                emit_leaf(lf, flags, L, M, xsz, ysz, off + rank, node, lev);
+            }
+        }
+        __syncthreads();
+        if (pass == 0)
+        {
+            if (threadIdx.x < 32)
+            {
+                const int c = __popc(bits[threadIdx.x]);
+                int incl = c;
+                for (int o = 1; o < 32; o <<= 1)
+                {
+                    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                    if ((int)threadIdx.x >= o) incl += v;
+                }
+                prefix[threadIdx.x] = incl - c;
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// Initial leaf list: every finest cell, in Z order.
+template <typename T> __global__ void k_init_leaves(Leaves<T> lf, int L, int n)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        lf.act[i] = lvl_idx(L) + i;
+        lf.lvl[i] = (uint8_t)L;
+    }
+}
+
+} // namespace mw

@@ -1,0 +1,817 @@
+// Simulation object and C ABI (include/mwdg2.h).
+//
+// Host loop per step (mirrors source/run_simulation.cu:226-774 step by step):
+//   time update -> maxima + re-insertion -> point sources -> [encode+threshold+regularise
+//   -> decode+extra significance -> leaf topology] -> MWDG2 stage 1 -> re-insert ->
+//   scale re-encode -> stage 2 (or HWFV1 update) -> one 64-byte read-back (dt, leaves).
+// All per-step state stays on the device; the only host<->device traffic per step is the
+// point-source values (when there are sources) and the scalar read-back.
+#include "../../include/mwdg2.h"
+#include "case_io.hpp"
+#include "solver.cuh"
+
+#include <cerrno>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <sys/stat.h>
+#include <vector>
+
+namespace {
+
+thread_local std::string g_last_error = "";
+
+mwdg2_status set_err(mwdg2_status st, const std::string& msg)
+{
+    g_last_error = msg;
+    return st;
+}
+
+#define CU(call)                                                                                          \
+    do                                                                                                    \
+    {                                                                                                     \
+        cudaError_t e_ = (call);                                                                          \
+        if (e_ != cudaSuccess)                                                                            \
+            return set_err(MWDG2_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));           \
+    } while (0)
+
+struct SimBase
+{
+    virtual ~SimBase() = default;
+    virtual mwdg2_status init(const char* par, const mwdg2_opts& o) = 0;
+    virtual mwdg2_status step(double* dt, int64_t* n) = 0;
+    virtual mwdg2_status run(int64_t max_steps, int64_t* steps, int64_t* updates) = 0;
+    virtual mwdg2_status info(double* out, int n) = 0;
+    virtual mwdg2_status leaves(int32_t* a, int32_t* l, int32_t* ids, int32_t* lv, int64_t cap) = 0;
+    virtual mwdg2_status state(double* out, int64_t cap) = 0;
+    virtual mwdg2_status sig(uint8_t* out, int64_t cap) = 0;
+    virtual mwdg2_status hierarchy(int f, int m, double* out, int64_t cap) = 0;
+    virtual mwdg2_status stage(double* out, int n) = 0;
+    virtual mwdg2_status timing(double* out, int n) = 0;
+    virtual mwdg2_status counters(int64_t* out, int n) = 0;
+};
+
+template <typename T> class Sim final : public SimBase
+{
+public:
+    ~Sim() override { release(); }
+
+    mwdg2_status init(const char* par, const mwdg2_opts& o) override;
+    mwdg2_status step(double* dt_out, int64_t* n_out) override;
+    mwdg2_status run(int64_t max_steps, int64_t* steps, int64_t* updates) override;
+    mwdg2_status info(double* out, int n) override;
+    mwdg2_status leaves(int32_t* a, int32_t* l, int32_t* ids, int32_t* lv, int64_t cap) override;
+    mwdg2_status state(double* out, int64_t cap) override;
+    mwdg2_status sig(uint8_t* out, int64_t cap) override;
+    mwdg2_status hierarchy(int f, int m, double* out, int64_t cap) override;
+    mwdg2_status stage(double* out, int n) override;
+    mwdg2_status timing(double* out, int n) override;
+    mwdg2_status counters(int64_t* out, int n) override;
+
+private:
+    mwio::Case<T> cs_;
+    mwdg2_opts opts_{};
+    bool mw_ = true;
+    int L_ = 0, M_ = 0, n_det_ = 0, n_all_ = 0, D_ = 0, ntiles_ = 0;
+    int64_t F_ = 0;
+    T dt_ = T(0.001), time_ = T(0);
+    bool first_ = true, finished_ = false;
+    int timestep_ = 1;
+    int n_leaves_ = 0;
+    int solver_blocks_ = 0, red_blocks_ = 0;
+    int device_ = 0;
+    cudaStream_t st_ = nullptr;
+    std::vector<void*> allocs_;
+    mw::Hier<T> hr_{};
+    mw::Leaves<T> lf_{};
+    mw::Scalars<T>* sc_ = nullptr;      // device
+    mw::Scalars<T>* sc_host_ = nullptr; // pinned
+    int32_t* tile_counts_ = nullptr;
+    mw::Src<T>* d_src_ = nullptr;
+    mw::Src<T>* h_src_ = nullptr;       // pinned
+    int32_t* d_stage_codes_ = nullptr;
+    T* d_stage_out_ = nullptr;
+    double* d_state_scratch_ = nullptr;
+    mw::Params<T> P_{};
+    // timing
+    bool timed_ = false;
+    cudaEvent_t ev_[9] = {};
+    double last_ms_[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int64_t last_cnt_[6] = {0, 0, 0, 0, 0, 0};
+    int launches_ = 0;
+    // outputs
+    std::chrono::steady_clock::time_point t_start_;
+    double time_mra_ = 0, time_solver_ = 0;
+
+    template <typename P> mwdg2_status dalloc(P*& p, size_t count)
+    {
+        void* v = nullptr;
+        cudaError_t e = cudaMalloc(&v, count * sizeof(P) + 64);
+        if (e != cudaSuccess) return set_err(MWDG2_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        allocs_.push_back(v);
+        p = static_cast<P*>(v);
+        return MWDG2_OK;
+    }
+    void release();
+    mwdg2_status launch_step();
+    mwdg2_status write_outputs(bool first);
+    mwdg2_status sample_stage(std::vector<T>& vals);
+    mw::Bnd<T> bnd_now() const;
+    int grid_for(int64_t n, int threads, int cap) const
+    {
+        int64_t b = (n + threads - 1) / threads;
+        if (b > cap) b = cap;
+        return (int)(b < 1 ? 1 : b);
+    }
+};
+
+template <typename T> void Sim<T>::release()
+{
+    if (device_ >= 0) cudaSetDevice(device_);
+    for (auto& e : ev_) if (e) { cudaEventDestroy(e); e = nullptr; }
+    for (void* p : allocs_) cudaFree(p);
+    allocs_.clear();
+    if (sc_host_) { cudaFreeHost(sc_host_); sc_host_ = nullptr; }
+    if (h_src_) { cudaFreeHost(h_src_); h_src_ = nullptr; }
+    if (st_) { cudaStreamDestroy(st_); st_ = nullptr; }
+}
+
+template <typename T> mw::Bnd<T> Sim<T>::bnd_now() const
+{
+    mw::Bnd<T> b{};
+    for (int d = 0; d < 4; ++d)
+    {
+        b.start[d] = cs_.bnd[d].start;
+        b.end[d] = cs_.bnd[d].end;
+        b.type[d] = cs_.bnd[d].type;
+        b.inlet[d] = cs_.bnd[d].inlet;
+    }
+    return b;
+}
+
+template <typename T> mwdg2_status Sim<T>::init(const char* par, const mwdg2_opts& o)
+{
+    opts_ = o;
+    if (!cs_.read(par, o.epsilon, o.solver))
+        return set_err(cs_.error_kind == 1 ? MWDG2_ERR_IO : MWDG2_ERR_PARSE, cs_.error);
+    if (o.dirroot) cs_.dirroot = o.dirroot;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return set_err(MWDG2_ERR_CUDA, "no CUDA device available (this library has no CPU path)");
+    if (o.device >= 0) CU(cudaSetDevice(o.device));
+    CU(cudaGetDevice(&device_));
+    CU(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+    mw_ = (cs_.solver == 2);
+    L_ = cs_.L;
+    M_ = 1 << L_;
+    F_ = (int64_t)M_ * M_;
+    n_det_ = mw::lvl_idx(L_);
+    n_all_ = mw::lvl_idx(L_ + 1);
+    D_ = std::min(mw::kTileDepth, L_);
+    ntiles_ = 1 << (2 * (L_ - D_));
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_);
+    solver_blocks_ = sms * 8;
+    red_blocks_ = sms * 4;
+
+    // hierarchy, details, flags
+    const int modes = mw_ ? 3 : 1;
+    for (int f = 0; f < 4; ++f)
+        for (int m = 0; m < 3; ++m)
+        {
+            hr_.s[f][m] = nullptr;
+            if (m < modes) { mwdg2_status s = dalloc(hr_.s[f][m], n_all_); if (s) return s; }
+        }
+    for (int f = 0; f < 3; ++f)
+        for (int k = 0; k < 9; ++k)
+        {
+            hr_.det[f][k] = nullptr;
+            if (mw_ || k % 3 == 0) { mwdg2_status s = dalloc(hr_.det[f][k], n_det_); if (s) return s; }
+        }
+    if (mwdg2_status s = dalloc(hr_.norm, n_det_)) return s;
+    if (mwdg2_status s = dalloc(hr_.flags, n_det_)) return s;
+    // leaves (capacity: every finest cell)
+    if (mwdg2_status s = dalloc(lf_.act, F_)) return s;
+    if (mwdg2_status s = dalloc(lf_.lvl, F_)) return s;
+    for (int d = 0; d < 4; ++d)
+    {
+        if (mwdg2_status s = dalloc(lf_.nb[d], F_)) return s;
+        if (mwdg2_status s = dalloc(lf_.nbl[d], F_)) return s;
+    }
+    for (int k = 0; k < 9; ++k)
+    {
+        lf_.un[k] = lf_.us[k] = nullptr;
+        if (mw_ || k % 3 == 0)
+        {
+            if (mwdg2_status s = dalloc(lf_.un[k], F_)) return s;
+            if (mw_) { if (mwdg2_status s = dalloc(lf_.us[k], F_)) return s; }
+        }
+    }
+    if (mwdg2_status s = dalloc(sc_, 1)) return s;
+    if (mwdg2_status s = dalloc(tile_counts_, ntiles_)) return s;
+    CU(cudaMallocHost(&sc_host_, sizeof(mw::Scalars<T>)));
+    const int nsrc = (int)cs_.srcs.size();
+    if (nsrc > 0)
+    {
+        if (mwdg2_status s = dalloc(d_src_, nsrc)) return s;
+        CU(cudaMallocHost(&h_src_, sizeof(mw::Src<T>) * nsrc));
+    }
+    const int nst = (int)cs_.stage_codes.size();
+    if (nst > 0)
+    {
+        if (mwdg2_status s = dalloc(d_stage_codes_, nst)) return s;
+        if (mwdg2_status s = dalloc(d_stage_out_, 4 * nst)) return s;
+        CU(cudaMemcpyAsync(d_stage_codes_, cs_.stage_codes.data(), sizeof(int32_t) * nst, cudaMemcpyHostToDevice, st_));
+    }
+
+    // finest level of the hierarchy (zorder/copy_finest_coefficients.cu:3-35)
+    {
+        const int fin = mw::lvl_idx(L_);
+        std::vector<T> tmp(F_);
+        for (int m = 0; m < modes; ++m)
+        {
+            const std::vector<T>& h = cs_.fine[4 * m + 0];
+            const std::vector<T>& qx = cs_.fine[4 * m + 1];
+            const std::vector<T>& qy = cs_.fine[4 * m + 2];
+            const std::vector<T>& z = cs_.fine[4 * m + 3];
+            for (int64_t k = 0; k < F_; ++k) tmp[k] = h[k] + z[k];
+            CU(cudaMemcpy(hr_.s[0][m] + fin, tmp.data(), sizeof(T) * F_, cudaMemcpyHostToDevice));
+            CU(cudaMemcpy(hr_.s[1][m] + fin, qx.data(), sizeof(T) * F_, cudaMemcpyHostToDevice));
+            CU(cudaMemcpy(hr_.s[2][m] + fin, qy.data(), sizeof(T) * F_, cudaMemcpyHostToDevice));
+            CU(cudaMemcpy(hr_.s[3][m] + fin, z.data(), sizeof(T) * F_, cudaMemcpyHostToDevice));
+            // initial leaf state (all finest cells): h of mode 0 carries the initial
+            // point-source insertion, which only the first step's maxima see
+            const std::vector<T>& h_leaf = (m == 0) ? cs_.h0_for_maxes : h;
+            CU(cudaMemcpy(lf_.un[0 + m], h_leaf.data(), sizeof(T) * F_, cudaMemcpyHostToDevice));
+            CU(cudaMemcpy(lf_.un[3 + m], qx.data(), sizeof(T) * F_, cudaMemcpyHostToDevice));
+            CU(cudaMemcpy(lf_.un[6 + m], qy.data(), sizeof(T) * F_, cudaMemcpyHostToDevice));
+        }
+    }
+    // flags: all significant (mra/init_sig_details.cu) plus preflags
+    {
+        std::vector<uint8_t> fl(n_det_);
+        for (int i = 0; i < n_det_; ++i) fl[i] = mw::F_SIG | (cs_.preflag[i] ? mw::F_PRE : 0);
+        CU(cudaMemcpy(hr_.flags, fl.data(), n_det_, cudaMemcpyHostToDevice));
+    }
+    // release host copies of the initial grid
+    for (auto& v : cs_.fine) std::vector<T>().swap(v);
+    std::vector<T>().swap(cs_.h0_for_maxes);
+
+    P_.L = L_; P_.M = M_; P_.xsz = cs_.xsz; P_.ysz = cs_.ysz; P_.limit = cs_.limitslopes ? 1 : 0;
+    P_.dx = cs_.dx; P_.tol_h = cs_.tol_h; P_.tol_q = cs_.tol_q; P_.tol_s = cs_.tol_s; P_.g = cs_.g;
+    P_.manning = cs_.manning; P_.CFL = cs_.CFL; P_.initial_tstep = cs_.initial_tstep;
+    P_.wall_height = cs_.wall_height; P_.tol_Krivo = cs_.tol_Krivo; P_.eps = cs_.epsilon;
+
+    n_leaves_ = (int)F_;
+    mw::k_init_leaves<T><<<grid_for(F_, 256, 4096), 256, 0, st_>>>(lf_, L_, (int)F_);
+    // maxima of the initial state (run_simulation.cu:190) then bed encoding with preflags
+    // (mra/preflag_topo.cu:3-43)
+    mw::k_step_begin<T><<<1, 1, 0, st_>>>(sc_);
+    if (mw_) mw::k_maxes_reinsert<T, true><<<red_blocks_, 256, 0, st_>>>(lf_, hr_, sc_, (int)F_, false);
+    else mw::k_maxes_reinsert<T, false><<<red_blocks_, 256, 0, st_>>>(lf_, hr_, sc_, (int)F_, false);
+    for (int level = L_ - 1; level >= 0; --level)
+    {
+        const int nb = grid_for((int64_t)1 << (2 * level), 256, 1 << 24);
+        if (mw_) mw::k_topo_level<T, true><<<nb, 256, 0, st_>>>(hr_, sc_, L_, level, cs_.epsilon);
+        else mw::k_topo_level<T, false><<<nb, 256, 0, st_>>>(hr_, sc_, L_, level, cs_.epsilon);
+    }
+    CU(cudaGetLastError());
+    CU(cudaStreamSynchronize(st_));
+    {
+        int32_t nl = (int32_t)F_;
+        CU(cudaMemcpy(&sc_->n_leaves, &nl, sizeof(nl), cudaMemcpyHostToDevice));
+        int32_t zero = 0;
+        CU(cudaMemcpy(&sc_->status, &zero, sizeof(zero), cudaMemcpyHostToDevice));
+    }
+    timed_ = (o.verbose >= 2);
+    if (timed_) for (auto& e : ev_) CU(cudaEventCreate(&e));
+    t_start_ = std::chrono::steady_clock::now();
+    return MWDG2_OK;
+}
+
+template <typename T> mwdg2_status Sim<T>::launch_step()
+{
+    const bool mw = mw_;
+    const T eps = cs_.epsilon;
+    auto rec = [&](int k) { if (timed_) cudaEventRecord(ev_[k], st_); };
+    launches_ = 0;
+    rec(0);
+    mw::k_step_begin<T><<<1, 1, 0, st_>>>(sc_);
+    ++launches_;
+    const int nfix = first_ ? (int)F_ : -1;
+    if (mw) { mw::k_maxes_reinsert<T, true><<<red_blocks_, 256, 0, st_>>>(lf_, hr_, sc_, nfix, !first_); ++launches_; }
+    else { mw::k_maxes_reinsert<T, false><<<red_blocks_, 256, 0, st_>>>(lf_, hr_, sc_, nfix, !first_); ++launches_; }
+    // point sources (classes/PointSources.h:453-472 on the host, then the kernel)
+    const int nsrc = (int)cs_.srcs.size();
+    if (nsrc > 0)
+    {
+        for (int i = 0; i < nsrc; ++i)
+        {
+            auto& s = cs_.srcs[i];
+            if (s.varying) s.value = s.series.at(time_);
+            h_src_[i] = mw::Src<T>{s.code, s.type, s.value};
+        }
+        CU(cudaMemcpyAsync(d_src_, h_src_, sizeof(mw::Src<T>) * nsrc, cudaMemcpyHostToDevice, st_));
+        mw::k_point_sources<T><<<(nsrc + 127) / 128, 128, 0, st_>>>(hr_, d_src_, nsrc, dt_, cs_.dx, L_);
+        ++launches_;
+    }
+    rec(1);
+    const int top = std::min(4, L_ - 1);
+    const bool remesh = (eps > T(0) || first_);
+    if (remesh)
+    {
+        for (int level = L_ - 1; level > top; --level)
+        {
+            const int nb = grid_for((int64_t)1 << (2 * level), 256, 1 << 24);
+            if (mw) { mw::k_encode_level<T, true, true><<<nb, 256, 0, st_>>>(hr_, sc_, L_, level, eps); ++launches_; }
+            else { mw::k_encode_level<T, false, true><<<nb, 256, 0, st_>>>(hr_, sc_, L_, level, eps); ++launches_; }
+        }
+        if (mw) { mw::k_encode_top<T, true, true><<<1, 256, 0, st_>>>(hr_, sc_, L_, top, eps); ++launches_; }
+        else { mw::k_encode_top<T, false, true><<<1, 256, 0, st_>>>(hr_, sc_, L_, top, eps); ++launches_; }
+    }
+    rec(2);
+    if (remesh)
+    {
+        if (mw) { mw::k_decode_top<T, true><<<1, 256, 0, st_>>>(hr_, sc_, L_, top, eps); ++launches_; }
+        else { mw::k_decode_top<T, false><<<1, 256, 0, st_>>>(hr_, sc_, L_, top, eps); ++launches_; }
+        for (int level = top + 1; level < L_; ++level)
+        {
+            const int nb = grid_for((int64_t)1 << (2 * level), 256, 1 << 24);
+            if (mw) { mw::k_decode_level<T, true><<<nb, 256, 0, st_>>>(hr_, sc_, L_, level, eps); ++launches_; }
+            else { mw::k_decode_level<T, false><<<nb, 256, 0, st_>>>(hr_, sc_, L_, level, eps); ++launches_; }
+        }
+    }
+    rec(3);
+    if (remesh)
+    {
+        mw::k_tile_count<<<ntiles_, mw::kTileThreads, 0, st_>>>(hr_.flags, L_, D_, tile_counts_);
+        ++launches_;
+        mw::k_tile_scan<T><<<1, 1024, 0, st_>>>(tile_counts_, ntiles_, sc_);
+        ++launches_;
+        mw::k_tile_emit<T><<<ntiles_, mw::kTileThreads, 0, st_>>>(lf_, hr_.flags, tile_counts_, L_, D_, M_, cs_.xsz, cs_.ysz);
+        ++launches_;
+    }
+    rec(4);
+    // boundary inlets at the current time (classes/Boundaries.h:28-39)
+    for (int d = 0; d < 4; ++d)
+        if (cs_.bnd[d].varying) cs_.bnd[d].inlet = cs_.bnd[d].series.at(time_);
+    const mw::Bnd<T> B = bnd_now();
+    const bool fric = cs_.manning > T(0);
+    if (!mw)
+    {
+        mw::k_hwfv1<T><<<solver_blocks_, mw::kSolverThreads, 0, st_>>>(lf_, hr_, sc_, P_, B, dt_, fric);
+        ++launches_;
+        rec(5);
+        rec(6);
+        rec(7);
+    }
+    else
+    {
+        mw::k_mwdg2_stage<T, 1><<<solver_blocks_, mw::kSolverThreads, 0, st_>>>(lf_, hr_, sc_, P_, B, dt_, fric);
+        ++launches_;
+        rec(5);
+        mw::k_reinsert_us<T><<<red_blocks_, 256, 0, st_>>>(lf_, hr_, sc_);
+        ++launches_;
+        if (eps > T(0))
+        {
+            for (int level = L_ - 1; level > top; --level)
+            {
+                const int nb = grid_for((int64_t)1 << (2 * level), 256, 1 << 24);
+                mw::k_encode_level<T, true, false><<<nb, 256, 0, st_>>>(hr_, sc_, L_, level, eps);
+                ++launches_;
+            }
+            mw::k_encode_top<T, true, false><<<1, 256, 0, st_>>>(hr_, sc_, L_, top, eps);
+            ++launches_;
+        }
+        if (cs_.limitslopes) { mw::k_stage2_maxh<T><<<red_blocks_, 256, 0, st_>>>(lf_, hr_, sc_, P_, B, dt_); ++launches_; }
+        rec(6);
+        mw::k_mwdg2_stage<T, 2><<<solver_blocks_, mw::kSolverThreads, 0, st_>>>(lf_, hr_, sc_, P_, B, dt_, false);
+        ++launches_;
+        rec(7);
+    }
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(sc_host_, sc_, sizeof(mw::Scalars<T>), cudaMemcpyDeviceToHost, st_));
+    rec(8);
+    CU(cudaStreamSynchronize(st_));
+    if (timed_)
+    {
+        float ms = 0;
+        const int pairs[8][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 4}, {4, 5}, {5, 6}, {6, 7}, {0, 8}};
+        for (int k = 0; k < 8; ++k)
+        {
+            cudaEventElapsedTime(&ms, ev_[pairs[k][0]], ev_[pairs[k][1]]);
+            last_ms_[k] = ms;
+        }
+    }
+    last_cnt_[0] = (int64_t)sc_host_->enc;
+    last_cnt_[1] = (int64_t)sc_host_->enc2;
+    last_cnt_[2] = (int64_t)sc_host_->dec;
+    last_cnt_[3] = sc_host_->n_leaves;
+    last_cnt_[4] = n_det_ - 3;
+    last_cnt_[5] = launches_;
+    return MWDG2_OK;
+}
+
+template <typename T> mwdg2_status Sim<T>::step(double* dt_out, int64_t* n_out)
+{
+    if (finished_ || !(time_ < cs_.sim_time))
+    {
+        finished_ = true;
+        return MWDG2_DONE;
+    }
+    CU(cudaSetDevice(device_));
+    // run_simulation.cu:228-235
+    time_ += dt_;
+    if ((time_ - cs_.sim_time) > T(0))
+    {
+        time_ -= dt_;
+        dt_ = cs_.sim_time - time_;
+        time_ += dt_;
+    }
+    mwdg2_status s = launch_step();
+    if (s != MWDG2_OK) return s;
+    if (sc_host_->status & 1) return set_err(MWDG2_ERR_NUMERIC, "NaN in the leaf state");
+    n_leaves_ = sc_host_->n_leaves;
+    dt_ = sc_host_->dt_min;
+    first_ = false;
+    timestep_++;
+    if (dt_out) *dt_out = (double)dt_;
+    if (n_out) *n_out = n_leaves_;
+    return MWDG2_OK;
+}
+
+template <typename T> mwdg2_status Sim<T>::sample_stage(std::vector<T>& vals)
+{
+    const int np = (int)cs_.stage_codes.size();
+    vals.assign(4 * (size_t)np, T(0));
+    if (np == 0) return MWDG2_OK;
+    mw::k_sample_points<T><<<(np + 127) / 128, 128, 0, st_>>>(lf_, hr_, sc_, L_, d_stage_codes_, np, d_stage_out_);
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(vals.data(), d_stage_out_, sizeof(T) * 4 * np, cudaMemcpyDeviceToHost, st_));
+    CU(cudaStreamSynchronize(st_));
+    return MWDG2_OK;
+}
+
+// output/write_stage_point_data.cu:3-193 and output/write_cumulative_data.cpp:3-53
+template <typename T> mwdg2_status Sim<T>::write_outputs(bool first)
+{
+    const char* fmt = "%lf";  // NUM_FRMT: "%lf" and "%f" print alike
+    auto inv = [](int code, int& i, int& j) {
+        i = mw::compact(code);
+        j = mw::compact(code >> 1);
+    };
+    if (cs_.cumulative)
+    {
+        const std::string path = cs_.dirroot + "/" + cs_.resroot + ".cumu";
+        FILE* fp = fopen(path.c_str(), first ? "w" : "a");
+        if (!fp) return set_err(MWDG2_ERR_IO, "cannot write " + path);
+        if (first) fprintf(fp, "simtime,runtime_mra,runtime_solver,runtime_total,dt,reduction\n");
+        const double comp = (100.0 - 100.0 * n_leaves_ / ((double)cs_.xsz * cs_.ysz)) / 100.0;
+        fprintf(fp, "%lf,%lf,%lf,%lf,%lf,%lf\n", (double)time_, time_mra_, time_solver_, time_mra_ + time_solver_,
+                (double)dt_, comp);
+        fclose(fp);
+    }
+    const int np = (int)cs_.stage_codes.size();
+    if (np == 0) return MWDG2_OK;
+    std::vector<T> v;
+    if (mwdg2_status s = sample_stage(v)) return s;
+    const std::string base = cs_.dirroot + "/" + cs_.resroot;
+    FILE* fh = fopen((base + ".stage").c_str(), first ? "w" : "a");
+    FILE* fx = fopen((base + ".xvelocity").c_str(), first ? "w" : "a");
+    FILE* fy = fopen((base + ".yvelocity").c_str(), first ? "w" : "a");
+    if (!fh || !fx || !fy)
+    {
+        if (fh) fclose(fh);
+        if (fx) fclose(fx);
+        if (fy) fclose(fy);
+        return set_err(MWDG2_ERR_IO, "cannot write stage files under " + cs_.dirroot);
+    }
+    const T dx = cs_.dx;
+    auto header = [&](FILE* f, const char* title, const char* what) {
+        fprintf(f, "%s\n\n", title);
+        fprintf(f, "Stage information (stage,x,y,elev):\n");
+        for (int p = 0; p < np; ++p)
+        {
+            int i, j;
+            inv(cs_.stage_codes[p], i, j);
+            fprintf(f, "%d %lf %lf %lf\n", p + 1, (double)(i * dx + dx / T(2.0)), (double)(j * dx + dx / T(2.0)),
+                    (double)v[4 * p + 3]);
+        }
+        fprintf(f, "\nOutput, %s:\n", what);
+        fprintf(f, "Time; stages 1 to %d\n", np);
+    };
+    if (first)
+    {
+        header(fh, "Stage output, depth (m).", "depths");
+        if (cs_.voutput_stage)
+        {
+            header(fx, "Stage output, x velocity (m/s).", "x velocities");
+            header(fy, "Stage output, y velocity (m/s).", "y velocities");
+        }
+    }
+    fprintf(fh, "%lf ", (double)time_);
+    if (cs_.voutput_stage) { fprintf(fx, "%lf ", (double)time_); fprintf(fy, "%lf ", (double)time_); }
+    for (int p = 0; p < np; ++p)
+    {
+        const bool last = (p + 1 == np);
+        const T h = v[4 * p + 0];
+        fprintf(fh, last ? "%lf" : "%lf ", (double)h);
+        if (cs_.voutput_stage)
+        {
+            const T vx = (h < cs_.tol_h) ? T(0.0) : v[4 * p + 1] / h;
+            const T vy = (h < cs_.tol_h) ? T(0.0) : v[4 * p + 2] / h;
+            fprintf(fx, last ? "%lf" : "%lf ", (double)vx);
+            fprintf(fy, last ? "%lf" : "%lf ", (double)vy);
+        }
+    }
+    (void)fmt;
+    fprintf(fh, "\n");
+    if (cs_.voutput_stage) { fprintf(fx, "\n"); fprintf(fy, "\n"); }
+    fclose(fh);
+    fclose(fx);
+    fclose(fy);
+    return MWDG2_OK;
+}
+
+template <typename T> mwdg2_status Sim<T>::run(int64_t max_steps, int64_t* steps, int64_t* updates)
+{
+    int64_t done = 0, upd = 0;
+    if (opts_.write_outputs)
+    {
+        // classes/PlottingParams.h:55-60 (mkdir dirroot)
+        if (mkdir(cs_.dirroot.c_str(), 0755) != 0 && errno != EEXIST)
+            return set_err(MWDG2_ERR_IO, "cannot create output directory " + cs_.dirroot);
+    }
+    while (max_steps <= 0 || done < max_steps)
+    {
+        const bool first = first_;
+        double dt;
+        int64_t n;
+        const auto t0 = std::chrono::steady_clock::now();
+        mwdg2_status s = step(&dt, &n);
+        if (s == MWDG2_DONE) break;
+        if (s != MWDG2_OK) return s;
+        time_solver_ += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        ++done;
+        upd += n;
+        if (opts_.write_outputs)
+        {
+            // run_simulation.cu:656-751: saveint outputs (VTK/raster/c-prop) are not written;
+            // massint writes res.cumu (if `cumulative`) and the stage files
+            if (time_ >= cs_.saveint * cs_.saveint_count) cs_.saveint_count++;
+            if (time_ >= cs_.massint * cs_.massint_count)
+            {
+                cs_.massint_count++;
+                if (mwdg2_status so = write_outputs(first)) return so;
+            }
+        }
+        if (opts_.verbose && (timestep_ - 1) % 10000 == 1)
+        {
+            const double comp = 100.0 - 100.0 * n / ((double)cs_.xsz * cs_.ysz);
+            printf("Elements: %lld, compression: %f%%, time step: %f, timestep: %d, sim time: %f\n", (long long)n, comp,
+                   dt, timestep_ - 1, (double)time_);
+        }
+    }
+    if (steps) *steps = done;
+    if (updates) *updates = upd;
+    return MWDG2_OK;
+}
+
+template <typename T> mwdg2_status Sim<T>::info(double* out, int n)
+{
+    if (!out || n < 14) return set_err(MWDG2_ERR_ARG, "info: need 14 slots");
+    const double v[14] = {(double)time_, (double)dt_, (double)timestep_, (double)n_leaves_, (double)L_, (double)cs_.xsz,
+                          (double)cs_.ysz, (double)cs_.dx, (double)cs_.epsilon, (double)cs_.solver,
+                          (double)(sizeof(T) * 8), (double)cs_.sim_time, (double)n_det_, (double)n_all_};
+    for (int i = 0; i < 14; ++i) out[i] = v[i];
+    return MWDG2_OK;
+}
+
+template <typename T> mwdg2_status Sim<T>::leaves(int32_t* a, int32_t* l, int32_t* ids, int32_t* lv, int64_t cap)
+{
+    const int n = n_leaves_;
+    if (cap < n) return set_err(MWDG2_ERR_ARG, "get_leaves: capacity below the leaf count");
+    CU(cudaSetDevice(device_));
+    if (a) CU(cudaMemcpy(a, lf_.act, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
+    std::vector<uint8_t> tmp(n);
+    if (l)
+    {
+        CU(cudaMemcpy(tmp.data(), lf_.lvl, n, cudaMemcpyDeviceToHost));
+        for (int i = 0; i < n; ++i) l[i] = tmp[i];
+    }
+    for (int d = 0; d < 4; ++d)
+    {
+        if (ids) CU(cudaMemcpy(ids + (size_t)d * n, lf_.nb[d], sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
+        if (lv)
+        {
+            CU(cudaMemcpy(tmp.data(), lf_.nbl[d], n, cudaMemcpyDeviceToHost));
+            for (int i = 0; i < n; ++i) lv[(size_t)d * n + i] = tmp[i];
+        }
+    }
+    return MWDG2_OK;
+}
+
+template <typename T> mwdg2_status Sim<T>::state(double* out, int64_t cap)
+{
+    const int n = n_leaves_;
+    if (!out || cap < 12LL * n) return set_err(MWDG2_ERR_ARG, "get_state: need 12 x n_leaves doubles");
+    CU(cudaSetDevice(device_));
+    if (!d_state_scratch_) { if (mwdg2_status s = dalloc(d_state_scratch_, 12 * F_)) return s; }
+    mw::k_gather_state<T><<<grid_for(n, 256, 4096), 256, 0, st_>>>(lf_, hr_, sc_, mw_, d_state_scratch_);
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(out, d_state_scratch_, sizeof(double) * 12 * (size_t)n, cudaMemcpyDeviceToHost, st_));
+    CU(cudaStreamSynchronize(st_));
+    return MWDG2_OK;
+}
+
+template <typename T> mwdg2_status Sim<T>::sig(uint8_t* out, int64_t cap)
+{
+    if (!out || cap < n_det_) return set_err(MWDG2_ERR_ARG, "get_sig: need n_details bytes");
+    CU(cudaSetDevice(device_));
+    CU(cudaMemcpy(out, hr_.flags, n_det_, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < n_det_; ++i) out[i] = (out[i] & mw::F_SIG) ? 1 : 0;
+    return MWDG2_OK;
+}
+
+template <typename T> mwdg2_status Sim<T>::hierarchy(int f, int m, double* out, int64_t cap)
+{
+    if (f < 0 || f > 3 || m < 0 || m > 2 || !out || cap < n_all_) return set_err(MWDG2_ERR_ARG, "get_hierarchy: bad arguments");
+    if (!hr_.s[f][m]) return set_err(MWDG2_ERR_ARG, "get_hierarchy: HWFV1 holds mode 0 only");
+    CU(cudaSetDevice(device_));
+    std::vector<T> tmp(n_all_);
+    CU(cudaMemcpy(tmp.data(), hr_.s[f][m], sizeof(T) * n_all_, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < n_all_; ++i) out[i] = tmp[i];
+    return MWDG2_OK;
+}
+
+template <typename T> mwdg2_status Sim<T>::stage(double* out, int n)
+{
+    const int np = (int)cs_.stage_codes.size();
+    if (!out || n < np) return set_err(MWDG2_ERR_ARG, "read_stage: buffer smaller than the number of stage points");
+    CU(cudaSetDevice(device_));
+    std::vector<T> v;
+    if (mwdg2_status s = sample_stage(v)) return s;
+    for (int p = 0; p < np; ++p) out[p] = v[4 * p];
+    return MWDG2_OK;
+}
+
+template <typename T> mwdg2_status Sim<T>::timing(double* out, int n)
+{
+    for (int i = 0; i < n && i < 8; ++i) out[i] = last_ms_[i];
+    return MWDG2_OK;
+}
+
+template <typename T> mwdg2_status Sim<T>::counters(int64_t* out, int n)
+{
+    for (int i = 0; i < n && i < 6; ++i) out[i] = last_cnt_[i];
+    return MWDG2_OK;
+}
+
+} // namespace
+
+// ============================================================================ C ABI
+
+struct mwdg2_sim
+{
+    std::unique_ptr<SimBase> impl;
+};
+
+extern "C" {
+
+void mwdg2_default_opts(mwdg2_opts* o)
+{
+    if (!o) return;
+    o->precision = 64;
+    o->device = -1;
+    o->epsilon = -1.0;
+    o->solver = 0;
+    o->dirroot = nullptr;
+    o->write_outputs = 1;
+    o->verbose = 0;
+}
+
+const char* mwdg2_last_error(void) { return g_last_error.c_str(); }
+
+mwdg2_status mwdg2_create(const char* par_path, const mwdg2_opts* opts, mwdg2_sim** out)
+{
+    if (!par_path || !out) return set_err(MWDG2_ERR_ARG, "mwdg2_create: null argument");
+    *out = nullptr;
+    mwdg2_opts o;
+    mwdg2_default_opts(&o);
+    if (opts) o = *opts;
+    if (o.precision == 0) o.precision = 64;
+    if (o.precision != 32 && o.precision != 64) return set_err(MWDG2_ERR_ARG, "precision must be 32 or 64");
+    auto* s = new mwdg2_sim();
+    if (o.precision == 32) s->impl.reset(new Sim<float>());
+    else s->impl.reset(new Sim<double>());
+    mwdg2_status st = s->impl->init(par_path, o);
+    if (st != MWDG2_OK)
+    {
+        delete s;
+        return st;
+    }
+    *out = s;
+    return MWDG2_OK;
+}
+
+mwdg2_status mwdg2_step(mwdg2_sim* s, double* dt, int64_t* n)
+{
+    if (!s) return set_err(MWDG2_ERR_ARG, "null handle");
+    return s->impl->step(dt, n);
+}
+
+mwdg2_status mwdg2_run(mwdg2_sim* s, int64_t max_steps, int64_t* steps, int64_t* updates)
+{
+    if (!s) return set_err(MWDG2_ERR_ARG, "null handle");
+    return s->impl->run(max_steps, steps, updates);
+}
+
+mwdg2_status mwdg2_info(mwdg2_sim* s, double* out, int n)
+{
+    if (!s) return set_err(MWDG2_ERR_ARG, "null handle");
+    return s->impl->info(out, n);
+}
+
+mwdg2_status mwdg2_get_leaves(mwdg2_sim* s, int32_t* a, int32_t* l, int32_t* ids, int32_t* lv, int64_t cap)
+{
+    if (!s) return set_err(MWDG2_ERR_ARG, "null handle");
+    return s->impl->leaves(a, l, ids, lv, cap);
+}
+
+mwdg2_status mwdg2_get_state(mwdg2_sim* s, double* out, int64_t cap)
+{
+    if (!s) return set_err(MWDG2_ERR_ARG, "null handle");
+    return s->impl->state(out, cap);
+}
+
+mwdg2_status mwdg2_get_sig(mwdg2_sim* s, uint8_t* out, int64_t cap)
+{
+    if (!s) return set_err(MWDG2_ERR_ARG, "null handle");
+    return s->impl->sig(out, cap);
+}
+
+mwdg2_status mwdg2_get_hierarchy(mwdg2_sim* s, int f, int m, double* out, int64_t cap)
+{
+    if (!s) return set_err(MWDG2_ERR_ARG, "null handle");
+    return s->impl->hierarchy(f, m, out, cap);
+}
+
+mwdg2_status mwdg2_read_stage(mwdg2_sim* s, double* out, int n)
+{
+    if (!s) return set_err(MWDG2_ERR_ARG, "null handle");
+    return s->impl->stage(out, n);
+}
+
+mwdg2_status mwdg2_last_step_timing(mwdg2_sim* s, double* out, int n)
+{
+    if (!s || !out) return set_err(MWDG2_ERR_ARG, "null argument");
+    return s->impl->timing(out, n);
+}
+
+mwdg2_status mwdg2_last_step_counters(mwdg2_sim* s, int64_t* out, int n)
+{
+    if (!s || !out) return set_err(MWDG2_ERR_ARG, "null argument");
+    return s->impl->counters(out, n);
+}
+
+void mwdg2_destroy(mwdg2_sim* s) { delete s; }
+
+mwdg2_status mwdg2_run_simulation(int argc, char** argv)
+{
+    // input/read_command_line_params.cpp:12-47; the last argument is the .par file
+    if (argc < 2) return set_err(MWDG2_ERR_ARG, "usage: gpu-mwdg2 [-epsilon e] [-solver hwfv1|mwdg2] [-dirroot d] case.par");
+    mwdg2_opts o;
+    mwdg2_default_opts(&o);
+    o.verbose = 1;
+    std::string dirroot;
+    for (int i = 0; i < argc - 1; ++i)
+    {
+        const char* flag = argv[i];
+        const char* value = argv[i + 1];
+        if (!strncmp(flag, "-epsilon", 8)) o.epsilon = atof(value);
+        else if (!strncmp(flag, "-solver", 7))
+        {
+            if (!strncmp(value, "hwfv1", 5)) o.solver = 1;
+            else if (!strncmp(value, "mwdg2", 5)) o.solver = 2;
+            else return set_err(MWDG2_ERR_ARG, "invalid -solver (use hwfv1 or mwdg2)");
+        }
+        else if (!strncmp(flag, "-dirroot", 8)) dirroot = value;
+        else if (!strncmp(flag, "-precision", 10)) o.precision = atoi(value);
+    }
+    if (!dirroot.empty()) o.dirroot = dirroot.c_str();
+    mwdg2_sim* s = nullptr;
+    mwdg2_status st = mwdg2_create(argv[argc - 1], &o, &s);
+    if (st != MWDG2_OK) return st;
+    const auto t0 = std::chrono::steady_clock::now();
+    int64_t steps = 0, upd = 0;
+    st = mwdg2_run(s, 0, &steps, &upd);
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (st == MWDG2_OK) printf("Loop time: %f s (%lld steps, %.4e active-cell updates/s)\n", secs, (long long)steps, upd / secs);
+    mwdg2_destroy(s);
+    return st;
+}
+
+} // extern "C"

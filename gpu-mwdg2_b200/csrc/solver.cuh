@@ -1,0 +1,594 @@
+// Per-leaf solver kernels: one thread per leaf, grid-stride over the device-side leaf
+// count. Each kernel gathers the leaf and its four neighbours straight from the
+// hierarchy and keeps all per-neighbour work in registers, replacing the reference's
+// sequence load_soln_and_nghbr_coeffs -> add_ghost_cells -> friction_implicit ->
+// copy_to_buf_assem_sol -> limit_slopes -> dg2_update (or fv1_update) -> get_dt_CFL
+// and its five materialised neighbour copies.
+#pragma once
+
+#include "kernels.cuh"
+
+namespace mw {
+
+template <typename T> struct Cell { T h[3], qx[3], qy[3], z[3]; };
+
+// neighbours/load_soln_and_nghbr_coeffs.cu:3-104 (h = eta - z)
+template <typename T, bool MW> __device__ __forceinline__ void load_cell(const Hier<T>& hr, int a, Cell<T>& c)
+{
+#pragma unroll
+    for (int m = 0; m < (MW ? 3 : 1); ++m)
+    {
+        c.z[m] = hr.s[3][m][a];
+        c.h[m] = hr.s[0][m][a] - c.z[m];
+        c.qx[m] = hr.s[1][m][a];
+        c.qy[m] = hr.s[2][m][a];
+    }
+    if (!MW)
+    {
+        c.h[1] = c.h[2] = c.qx[1] = c.qx[2] = c.qy[1] = c.qy[2] = c.z[1] = c.z[2] = T(0.0);
+    }
+}
+
+// Ghost cells of a leaf at the domain border, raster cases
+// (neighbours/add_ghost_cells.cu:18-500): directions N, E, S, W in order; a fine
+// boundary cell of an HFIX/HVAR/QFIX/QVAR segment also resets the leaf's own depth.
+// gh/gq*: mode-0 values of the ghost in direction d (slopes are zero, bed = own bed).
+template <typename T>
+__device__ __forceinline__ void ghost_pass(T& own_h0, T own_qx0, T own_qy0, T own_z0, const int32_t (&nid)[4], int level,
+                                           int act, const Params<T>& P, const Bnd<T>& B, T dt, T (&gh)[4], T (&gqx)[4],
+                                           T (&gqy)[4])
+{
+    const int code = act - lvl_idx(level);
+    const int x = compact(code), y = compact(code >> 1);
+    const bool finest = (level == P.L);
+#pragma unroll
+    for (int d = 0; d < 4; ++d)
+    {
+        if (nid[d] != -1) continue;
+        gh[d] = own_h0;
+        gqx[d] = (d == 1 || d == 3) ? T(0.0) : own_qx0;
+        gqy[d] = (d == 0 || d == 2) ? T(0.0) : own_qy0;
+        const int c = (d == 0 || d == 2) ? x : y;
+        const bool bound = (c >= B.start[d] && c <= B.end[d]);
+        const bool border = (d == 0) ? (y == P.ysz - 1) : (d == 1) ? (x == P.xsz - 1) : (d == 2) ? (y == 0) : (x == 0);
+        if (!(finest && bound && border)) continue;
+        const int t = B.type[d];
+        if (t == FREE)
+        {
+            const T q = (d == 0 || d == 2) ? own_qy0 : own_qx0;
+            gh[d] = pow((q * q) / P.g, T(1.0) / T(3.0));
+            gqx[d] = own_qx0;
+            gqy[d] = own_qy0;
+        }
+        else if (t == HFIX || t == HVAR)
+        {
+            own_h0 = B.inlet[d] - own_z0;
+            gh[d] = own_h0;
+        }
+        else if (t == QFIX || t == QVAR)
+        {
+            own_h0 = B.inlet[d] * dt / P.dx;
+            gh[d] = own_h0;
+        }
+    }
+}
+
+// operators/friction_implicit.cu:155-264 -- implicit friction on the mode-0 value and,
+// for MWDG2, on the four Gauss-point values, whose differences rebuild the slopes.
+template <typename T, bool MW> __device__ __forceinline__ void friction_cell(Cell<T>& c, const Params<T>& P, T dt)
+{
+    if (!MW)
+    {
+        apply_friction(c.h[0], P.tol_h, P.tol_s, c.qx[0], c.qy[0], P.manning, P.g, dt);
+        return;
+    }
+    const T hlx = c.h[0] - c.h[1], hux = c.h[0] + c.h[1];
+    const T hly = c.h[0] - c.h[2], huy = c.h[0] + c.h[2];
+    T qxlx = c.qx[0] - c.qx[1], qxux = c.qx[0] + c.qx[1];
+    T qxly = c.qx[0] - c.qx[2], qxuy = c.qx[0] + c.qx[2];
+    T qylx = c.qy[0] - c.qy[1], qyux = c.qy[0] + c.qy[1];
+    T qyly = c.qy[0] - c.qy[2], qyuy = c.qy[0] + c.qy[2];
+    apply_friction(c.h[0], P.tol_h, P.tol_s, c.qx[0], c.qy[0], P.manning, P.g, dt);
+    apply_friction(hlx, P.tol_h, P.tol_s, qxlx, qylx, P.manning, P.g, dt);
+    apply_friction(hux, P.tol_h, P.tol_s, qxux, qyux, P.manning, P.g, dt);
+    apply_friction(hly, P.tol_h, P.tol_s, qxly, qyly, P.manning, P.g, dt);
+    apply_friction(huy, P.tol_h, P.tol_s, qxuy, qyuy, P.manning, P.g, dt);
+    c.qx[1] = T(0.5) * (qxux - qxlx);
+    c.qx[2] = T(0.5) * (qxuy - qxly);
+    c.qy[1] = T(0.5) * (qyux - qylx);
+    c.qy[2] = T(0.5) * (qyuy - qyly);
+}
+
+// What the limiter and the flux of a face need from one neighbour.
+template <typename T> struct NbFace
+{
+    T h0, eta0, qx0, qy0;   // mode-0 values
+    T hf, qxf, qyf, zf;     // values at the shared face (neighbour's Legendre basis)
+    T etaf;                 // face value of eta = z + h (limiter)
+};
+
+template <typename T> __device__ __forceinline__ NbFace<T> nb_face(const Cell<T>& c, const P3<T>& b)
+{
+    NbFace<T> r;
+    r.h0 = c.h[0];
+    r.qx0 = c.qx[0];
+    r.qy0 = c.qy[0];
+    r.eta0 = c.z[0] + c.h[0];
+    r.hf = face(P3<T>{c.h[0], c.h[1], c.h[2]}, b);
+    r.qxf = face(P3<T>{c.qx[0], c.qx[1], c.qx[2]}, b);
+    r.qyf = face(P3<T>{c.qy[0], c.qy[1], c.qy[2]}, b);
+    r.zf = face(P3<T>{c.z[0], c.z[1], c.z[2]}, b);
+    r.etaf = face(P3<T>{c.z[0] + c.h[0], c.z[1] + c.h[1], c.z[2] + c.h[2]}, b);
+    return r;
+}
+
+// operators/get_limited_slopes.cuh:10-78 for one field u (own planar coefficients),
+// given the neighbours' face values and mode-0 values of that field.
+template <typename T>
+__device__ __forceinline__ void limited_slopes(const P3<T>& u, T un_pos, T ue_pos, T us_neg, T uw_neg, T un0, T ue0, T us0,
+                                               T uw0, T dxf, T tolK, T& o1x, T& o1y)
+{
+    const T s3 = sqrt(T(3.0));
+    const T u_n_neg = face(u, P3<T>{T(1.0), T(0.0), s3});
+    const T u_e_neg = face(u, P3<T>{T(1.0), s3, T(0.0)});
+    const T u_s_pos = face(u, P3<T>{T(1.0), T(0.0), -s3});
+    const T u_w_pos = face(u, P3<T>{T(1.0), -s3, T(0.0)});
+    const T jn = fabs(un_pos - u_n_neg);
+    const T je = fabs(ue_pos - u_e_neg);
+    const T js = fabs(u_s_pos - us_neg);
+    const T jw = fabs(u_w_pos - uw_neg);
+    const T norm_x = fmax(fabs(u._0 - u._1x), fabs(u._0 + u._1x));
+    const T norm_y = fmax(fabs(u._0 - u._1y), fabs(u._0 + u._1y));
+    const T DS_e = (norm_x > T(1e-12)) ? je / (T(0.5) * dxf * norm_x) : T(0.0);
+    const T DS_w = (norm_x > T(1e-12)) ? jw / (T(0.5) * dxf * norm_x) : T(0.0);
+    const T DS_n = (norm_y > T(1e-12)) ? jn / (T(0.5) * dxf * norm_y) : T(0.0);
+    const T DS_s = (norm_y > T(1e-12)) ? js / (T(0.5) * dxf * norm_y) : T(0.0);
+    o1x = (fmax(DS_e, DS_w) < tolK) ? u._1x : minmod(u._1x, (u._0 - uw0) / s3, (ue0 - u._0) / s3);
+    o1y = (fmax(DS_n, DS_s) < tolK) ? u._1y : minmod(u._1y, (u._0 - us0), (un0 - u._0));
+}
+
+template <typename T> struct Geo { T x, y, dxl; bool in_extent; };
+
+template <typename T> __device__ __forceinline__ Geo<T> leaf_geo(int act, int level, const Params<T>& P)
+{
+    Geo<T> g;
+    g.dxl = P.dx * (1 << (P.L - level));
+    const int code = act - lvl_idx(level);
+    g.x = cell_centre(compact(code), g.dxl);
+    g.y = cell_centre(compact(code >> 1), g.dxl);
+    g.in_extent = !((g.x >= P.xsz * P.dx) || (g.y >= P.ysz * P.dx));
+    return g;
+}
+
+// Legendre basis of the neighbour in direction D evaluated at the shared face.
+template <typename T, int DIR>
+__device__ __forceinline__ P3<T> nb_basis(const Geo<T>& g, int nid, int nlvl, const Params<T>& P)
+{
+    if (nid == -1) return leg_basis<T, DIR>(true, g.x, g.y, g.dxl, g.dxl, T(0), T(0), T(1), T(1));
+    const T dn = P.dx * (1 << (P.L - nlvl));
+    const int code = nid - lvl_idx(nlvl);
+    const T xn = cell_centre(compact(code), dn);
+    const T yn = cell_centre(compact(code >> 1), dn);
+    return leg_basis<T, DIR>(false, g.x, g.y, g.dxl, g.dxl, xn, yn, dn, dn);
+}
+
+// operators/dg2_update.cu:160-334 -- the DG2 right-hand side applied to the own
+// coefficients c (h, qx, qy planar; z planar) with the neighbours' face values.
+template <typename T>
+__device__ __forceinline__ void dg2_rhs_update(const P3<T>& ch, const P3<T>& cqx, const P3<T>& cqy, const P3<T>& zp,
+                                               const NbFace<T> (&nf)[4], T dxl, const Params<T>& P, T dt, T (&out)[9])
+{
+    const T s3 = sqrt(T(3.0));
+    const T g = P.g, tol_h = P.tol_h;
+    const P3<T> bn = {T(1.0), T(0.0), s3}, be = {T(1.0), s3, T(0.0)};
+    const P3<T> bs = {T(1.0), T(0.0), -s3}, bw = {T(1.0), -s3, T(0.0)};
+    const T z_n_pos = nf[0].zf, z_e_pos = nf[1].zf, z_s_neg = nf[2].zf, z_w_neg = nf[3].zf;
+    const T z_n_neg = face(zp, bn), z_e_neg = face(zp, be), z_s_pos = face(zp, bs), z_w_pos = face(zp, bw);
+    const T zi_n = fmax(z_n_neg, z_n_pos), zi_e = fmax(z_e_neg, z_e_pos);
+    const T zi_s = fmax(z_s_neg, z_s_pos), zi_w = fmax(z_w_neg, z_w_pos);
+    const V3<T> Us_n_pos = star(V3<T>{nf[0].hf, nf[0].qxf, nf[0].qyf}, z_n_pos, zi_n, tol_h);
+    const V3<T> Us_e_pos = star(V3<T>{nf[1].hf, nf[1].qxf, nf[1].qyf}, z_e_pos, zi_e, tol_h);
+    const V3<T> Us_s_neg = star(V3<T>{nf[2].hf, nf[2].qxf, nf[2].qyf}, z_s_neg, zi_s, tol_h);
+    const V3<T> Us_w_neg = star(V3<T>{nf[3].hf, nf[3].qxf, nf[3].qyf}, z_w_neg, zi_w, tol_h);
+    const T hfn = face(ch, bn), hfe = face(ch, be), hfs = face(ch, bs), hfw = face(ch, bw);
+    const V3<T> Us_n_neg = star(V3<T>{hfn, face(cqx, bn), face(cqy, bn)}, z_n_neg, zi_n, tol_h);
+    const V3<T> Us_e_neg = star(V3<T>{hfe, face(cqx, be), face(cqy, be)}, z_e_neg, zi_e, tol_h);
+    const V3<T> Us_s_pos = star(V3<T>{hfs, face(cqx, bs), face(cqy, bs)}, z_s_pos, zi_s, tol_h);
+    const V3<T> Us_w_pos = star(V3<T>{hfw, face(cqx, bw), face(cqy, bw)}, z_w_pos, zi_w, tol_h);
+    const V3<T> F_n = flux_hll_y(Us_n_neg, Us_n_pos, tol_h, g);
+    const V3<T> F_e = flux_hll_x(Us_e_neg, Us_e_pos, tol_h, g);
+    const V3<T> F_s = flux_hll_y(Us_s_neg, Us_s_pos, tol_h, g);
+    const V3<T> F_w = flux_hll_x(Us_w_neg, Us_w_pos, tol_h, g);
+    // x direction: modes 0 and 1x (operators/get_bed_src.cuh:46-72 for the bed slope)
+    const V3<T> U0x = (Us_e_neg + Us_w_pos) / T(2.0);
+    const V3<T> U1x = (Us_e_neg - Us_w_pos) / (T(2.0) * s3);
+    V3<T> Lx0 = (-T(1.0) * (F_e - F_w)) / dxl;
+    V3<T> Lx1 = (-s3 / dxl) * (F_e + F_w - phys_flux_x(U0x - U1x, tol_h, g) - phys_flux_x(U0x + U1x, tol_h, g));
+    {
+        const T eta_e_neg = hfe + z_e_neg, eta_w_pos = hfw + z_w_pos;
+        const T zse = zi_e - fmax(T(0.0), -(eta_e_neg - zi_e));
+        const T zsw = zi_w - fmax(T(0.0), -(eta_w_pos - zi_w));
+        const T z1 = (zse - zsw) / (T(2.0) * s3);
+        Lx0.qx = Lx0.qx + -T(2.0) * s3 * g * U0x.h * z1 / dxl;
+        Lx1.qx = Lx1.qx + -T(2.0) * s3 * g * U1x.h * z1 / dxl;
+        Lx0.h = Lx0.h + T(0.0); Lx0.qy = Lx0.qy + T(0.0);
+        Lx1.h = Lx1.h + T(0.0); Lx1.qy = Lx1.qy + T(0.0);
+    }
+    // y direction: modes 0 and 1y
+    const V3<T> U0y = (Us_n_neg + Us_s_pos) / T(2.0);
+    const V3<T> U1y = (Us_n_neg - Us_s_pos) / (T(2.0) * s3);
+    V3<T> Ly0 = (-T(1.0) * (F_n - F_s)) / dxl;
+    V3<T> Ly1 = (-s3 / dxl) * (F_s + F_n - phys_flux_y(U0y - U1y, tol_h, g) - phys_flux_y(U0y + U1y, tol_h, g));
+    {
+        const T eta_n_neg = hfn + z_n_neg, eta_s_pos = hfs + z_s_pos;
+        const T zsn = zi_n - fmax(T(0.0), -(eta_n_neg - zi_n));
+        const T zss = zi_s - fmax(T(0.0), -(eta_s_pos - zi_s));
+        const T z1 = (zsn - zss) / (T(2.0) * s3);
+        Ly0.qy = Ly0.qy + -T(2.0) * s3 * g * U0y.h * z1 / dxl;
+        Ly1.qy = Ly1.qy + -T(2.0) * s3 * g * U1y.h * z1 / dxl;
+        Ly0.h = Ly0.h + T(0.0); Ly0.qx = Ly0.qx + T(0.0);
+        Ly1.h = Ly1.h + T(0.0); Ly1.qx = Ly1.qx + T(0.0);
+    }
+    // coeffs += dt * (Lx + Ly): Lx has modes (0, 1x, 0), Ly has (0, 0, 1y)
+    const T zero = T(0.0);
+    out[0] = ch._0 + dt * (Lx0.h + Ly0.h);
+    out[1] = ch._1x + dt * (Lx1.h + zero);
+    out[2] = ch._1y + dt * (zero + Ly1.h);
+    out[3] = cqx._0 + dt * (Lx0.qx + Ly0.qx);
+    out[4] = cqx._1x + dt * (Lx1.qx + zero);
+    out[5] = cqx._1y + dt * (zero + Ly1.qx);
+    out[6] = cqy._0 + dt * (Lx0.qy + Ly0.qy);
+    out[7] = cqy._1x + dt * (Lx1.qy + zero);
+    out[8] = cqy._1y + dt * (zero + Ly1.qy);
+}
+
+// One RK2 stage of MWDG2 for every leaf. STAGE 1: friction (once per step), limiter with
+// the step's max depth, U* -> us, U^n (after friction and limiter) -> un.
+// STAGE 2: limiter with the stage's max depth, U^{n+1} = (U** + U^n)/2 -> un, CFL dt.
+template <typename T, int STAGE>
+__global__ void __launch_bounds__(kSolverThreads) k_mwdg2_stage(Leaves<T> lf, Hier<T> hr, Scalars<T>* sc, Params<T> P,
+                                                                Bnd<T> B, T dt, bool friction)
+{
+    const int n = sc->n_leaves;
+    T dt_loc = (sizeof(T) == 8) ? T(1.0e308) : T(3.0e38);
+    bool nan_seen = false;
+    const T max_h = (STAGE == 1) ? fmax(T(1.0), sc->max_h) : sc->max_h2;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        const int a = lf.act[i];
+        const int level = lf.lvl[i];
+        int32_t nid[4];
+        int nl[4];
+#pragma unroll
+        for (int d = 0; d < 4; ++d) { nid[d] = lf.nb[d][i]; nl[d] = lf.nbl[d][i]; }
+        Cell<T> own;
+        load_cell<T, true>(hr, a, own);
+        T gh[4], gqx[4], gqy[4];
+        ghost_pass(own.h[0], own.qx[0], own.qy[0], own.z[0], nid, level, a, P, B, dt, gh, gqx, gqy);
+        // friction_implicit.cu:24-48: shallow or slow leaves lose their discharge and
+        // skip friction (their neighbours' copies are then left untouched too)
+        bool fric = false;
+        if (STAGE == 1 && friction)
+        {
+            const T h = own.h[0];
+            const bool below_depth = (h < P.tol_h);
+            const T ux = below_depth ? T(0.0) : own.qx[0] / h;
+            const T uy = below_depth ? T(0.0) : own.qy[0] / h;
+            const bool below_speed = (fabs(ux) < P.tol_s && fabs(uy) < P.tol_s);
+            if (below_depth || below_speed) { own.qx[0] = T(0.0); own.qy[0] = T(0.0); }
+            fric = !(below_depth || below_speed);
+            if (fric) friction_cell<T, true>(own, P, dt);
+        }
+        const Geo<T> geo = leaf_geo<T>(a, level, P);
+        NbFace<T> nf[4];
+#pragma unroll
+        for (int d = 0; d < 4; ++d)
+        {
+            Cell<T> c;
+            if (nid[d] != -1) load_cell<T, true>(hr, nid[d], c);
+            else
+            {
+                c.h[0] = gh[d]; c.qx[0] = gqx[d]; c.qy[0] = gqy[d]; c.z[0] = own.z[0];
+                c.h[1] = c.h[2] = c.qx[1] = c.qx[2] = c.qy[1] = c.qy[2] = c.z[1] = c.z[2] = T(0.0);
+            }
+            if (fric) friction_cell<T, true>(c, P, dt);
+            P3<T> b;
+            if (d == 0) b = nb_basis<T, NORTH>(geo, nid[d], nl[d], P);
+            else if (d == 1) b = nb_basis<T, EAST>(geo, nid[d], nl[d], P);
+            else if (d == 2) b = nb_basis<T, SOUTH>(geo, nid[d], nl[d], P);
+            else b = nb_basis<T, WEST>(geo, nid[d], nl[d], P);
+            nf[d] = nb_face(c, b);
+        }
+        // operators/copy_to_buf_assem_sol.cu: the stage-1 result of a leaf that is not
+        // updated is its state before limiting
+        T pre[9];
+        if (STAGE == 1)
+        {
+#pragma unroll
+            for (int m = 0; m < 3; ++m) { pre[m] = own.h[m]; pre[3 + m] = own.qx[m]; pre[6 + m] = own.qy[m]; }
+        }
+        // operators/limit_slopes.cu:3-238 (finest-level leaves inside the DEM only)
+        if (P.limit && level == P.L && geo.in_extent)
+        {
+            const P3<T> eta = {own.z[0] + own.h[0], own.z[1] + own.h[1], own.z[2] + own.h[2]};
+            const P3<T> qx = {own.qx[0], own.qx[1], own.qx[2]}, qy = {own.qy[0], own.qy[1], own.qy[2]};
+            T e1x, e1y, q1x, q1y, r1x, r1y;
+            limited_slopes(eta, nf[0].etaf, nf[1].etaf, nf[2].etaf, nf[3].etaf, nf[0].eta0, nf[1].eta0, nf[2].eta0,
+                           nf[3].eta0, P.dx, P.tol_Krivo, e1x, e1y);
+            limited_slopes(qx, nf[0].qxf, nf[1].qxf, nf[2].qxf, nf[3].qxf, nf[0].qx0, nf[1].qx0, nf[2].qx0, nf[3].qx0,
+                           P.dx, P.tol_Krivo, q1x, q1y);
+            limited_slopes(qy, nf[0].qyf, nf[1].qyf, nf[2].qyf, nf[3].qyf, nf[0].qy0, nf[1].qy0, nf[2].qy0, nf[3].qy0,
+                           P.dx, P.tol_Krivo, r1x, r1y);
+            const bool ax = (T(0.05) * max_h < fmin(own.h[0], fmin(nf[1].h0, nf[3].h0)));
+            const bool ay = (T(0.05) * max_h < fmin(own.h[0], fmin(nf[0].h0, nf[2].h0)));
+            if (ax) { own.h[1] = e1x - own.z[1]; own.qx[1] = q1x; own.qy[1] = r1x; }
+            if (ay) { own.h[2] = e1y - own.z[2]; own.qx[2] = q1y; own.qy[2] = r1y; }
+        }
+        if (STAGE == 1)
+        {
+#pragma unroll
+            for (int m = 0; m < 3; ++m) { lf.un[m][i] = own.h[m]; lf.un[3 + m][i] = own.qx[m]; lf.un[6 + m][i] = own.qy[m]; }
+        }
+        // operators/dg2_update.cu:31-79 (wet leaves, not high wall, inside the DEM)
+        const bool highwall = (fabs(own.z[0] - P.wall_height) < T(1e-10));
+        const bool wet = (own.h[0] >= P.tol_h || nf[0].h0 >= P.tol_h || nf[1].h0 >= P.tol_h || nf[2].h0 >= P.tol_h ||
+                          nf[3].h0 >= P.tol_h) && !highwall;
+        T leaf_dt = P.initial_tstep;
+        if (wet && geo.in_extent)
+        {
+            T u[9];
+            dg2_rhs_update(P3<T>{own.h[0], own.h[1], own.h[2]}, P3<T>{own.qx[0], own.qx[1], own.qx[2]},
+                           P3<T>{own.qy[0], own.qy[1], own.qy[2]}, P3<T>{own.z[0], own.z[1], own.z[2]}, nf, geo.dxl, P, dt, u);
+            if (STAGE == 2)
+            {
+#pragma unroll
+                for (int k = 0; k < 9; ++k) u[k] = T(0.5) * (u[k] + lf.un[k][i]);
+            }
+            if (u[0] < P.tol_h)
+            {
+                u[3] = u[4] = u[5] = u[6] = u[7] = u[8] = T(0.0);
+            }
+            else if (STAGE == 2)
+            {
+                const T ux = u[3] / u[0], uy = u[6] / u[0];
+                const T dtx = P.CFL * geo.dxl / (fabs(ux) + sqrt(P.g * u[0]));
+                const T dty = P.CFL * geo.dxl / (fabs(uy) + sqrt(P.g * u[0]));
+                leaf_dt = fmin(dtx, dty);
+            }
+            if (STAGE == 1)
+            {
+#pragma unroll
+                for (int k = 0; k < 9; ++k) lf.us[k][i] = u[k];
+            }
+            else
+            {
+#pragma unroll
+                for (int k = 0; k < 9; ++k) lf.un[k][i] = u[k];
+                nan_seen |= (u[0] != u[0]);
+            }
+        }
+        else if (STAGE == 1)
+        {
+#pragma unroll
+            for (int k = 0; k < 9; ++k) lf.us[k][i] = pre[k];
+        }
+        dt_loc = fmin(dt_loc, leaf_dt);
+    }
+    if (STAGE == 2)
+    {
+        dt_loc = warp_min(dt_loc);
+        __shared__ T red[kSolverThreads / 32];
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        if (lane == 0) red[w] = dt_loc;
+        __syncthreads();
+        if (threadIdx.x == 0)
+        {
+            T m = red[0];
+            for (int k = 1; k < (int)(blockDim.x >> 5); ++k) m = fmin(m, red[k]);
+            atomic_min_nn(&sc->dt_min, m);
+        }
+        if (__syncthreads_or(nan_seen) && threadIdx.x == 0) atomicOr(&sc->status, 1);
+    }
+}
+
+// Stage-1 result into the hierarchy (mra/reinsert_assem_sol.cu on d_buf_assem_sol).
+template <typename T> __global__ void __launch_bounds__(256) k_reinsert_us(Leaves<T> lf, Hier<T> hr, Scalars<T>* sc)
+{
+    const int n = sc->n_leaves;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        const int a = lf.act[i];
+        hr.s[0][0][a] = lf.us[0][i] + hr.s[3][0][a];
+        hr.s[1][0][a] = lf.us[3][i];
+        hr.s[2][0][a] = lf.us[6][i];
+        hr.s[0][1][a] = lf.us[1][i] + hr.s[3][1][a];
+        hr.s[1][1][a] = lf.us[4][i];
+        hr.s[2][1][a] = lf.us[7][i];
+        hr.s[0][2][a] = lf.us[2][i] + hr.s[3][2][a];
+        hr.s[1][2][a] = lf.us[5][i];
+        hr.s[2][2][a] = lf.us[8][i];
+    }
+}
+
+// max |h0| of the stage-2 leaf state after ghost cells (run_simulation.cu:613-620).
+template <typename T>
+__global__ void __launch_bounds__(256) k_stage2_maxh(Leaves<T> lf, Hier<T> hr, Scalars<T>* sc, Params<T> P, Bnd<T> B, T dt)
+{
+    const int n = sc->n_leaves;
+    T mh = T(0);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        const int a = lf.act[i];
+        const T z0 = hr.s[3][0][a];
+        T h0 = hr.s[0][0][a] - z0;
+        int32_t nid[4];
+        bool border = false;
+#pragma unroll
+        for (int d = 0; d < 4; ++d) { nid[d] = lf.nb[d][i]; border |= (nid[d] == -1); }
+        if (border)
+        {
+            T gh[4], gqx[4], gqy[4];
+            ghost_pass(h0, hr.s[1][0][a], hr.s[2][0][a], z0, nid, (int)lf.lvl[i], a, P, B, dt, gh, gqx, gqy);
+        }
+        mh = fmax(mh, fabs(h0));
+    }
+    T v[1] = {mh};
+    T* const dst[1] = {&sc->max_h2};
+    block_max_atomic<T, 1>(v, dst);
+}
+
+// operators/fv1_update.cu:3-243 with friction and ghost cells fused; in-place update.
+template <typename T>
+__global__ void __launch_bounds__(kSolverThreads) k_hwfv1(Leaves<T> lf, Hier<T> hr, Scalars<T>* sc, Params<T> P, Bnd<T> B,
+                                                          T dt, bool friction)
+{
+    const int n = sc->n_leaves;
+    T dt_loc = (sizeof(T) == 8) ? T(1.0e308) : T(3.0e38);
+    bool nan_seen = false;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        const int a = lf.act[i];
+        const int level = lf.lvl[i];
+        int32_t nid[4];
+#pragma unroll
+        for (int d = 0; d < 4; ++d) nid[d] = lf.nb[d][i];
+        Cell<T> own;
+        load_cell<T, false>(hr, a, own);
+        T gh[4], gqx[4], gqy[4];
+        ghost_pass(own.h[0], own.qx[0], own.qy[0], own.z[0], nid, level, a, P, B, dt, gh, gqx, gqy);
+        bool fric = false;
+        if (friction)
+        {
+            const T h = own.h[0];
+            const bool below_depth = (h < P.tol_h);
+            const T ux = below_depth ? T(0.0) : own.qx[0] / h;
+            const T uy = below_depth ? T(0.0) : own.qy[0] / h;
+            const bool below_speed = (fabs(ux) < P.tol_s && fabs(uy) < P.tol_s);
+            if (below_depth || below_speed) { own.qx[0] = T(0.0); own.qy[0] = T(0.0); }
+            fric = !(below_depth || below_speed);
+            if (fric) friction_cell<T, false>(own, P, dt);
+        }
+        V3<T> U[4];
+        T zn[4];
+#pragma unroll
+        for (int d = 0; d < 4; ++d)
+        {
+            Cell<T> c;
+            if (nid[d] != -1) load_cell<T, false>(hr, nid[d], c);
+            else { c.h[0] = gh[d]; c.qx[0] = gqx[d]; c.qy[0] = gqy[d]; c.z[0] = own.z[0]; }
+            if (fric) friction_cell<T, false>(c, P, dt);
+            U[d] = V3<T>{c.h[0], c.qx[0], c.qy[0]};
+            zn[d] = c.z[0];
+        }
+        T h = own.h[0], qx = own.qx[0], qy = own.qy[0];
+        const bool wet = (h >= P.tol_h || U[0].h >= P.tol_h || U[1].h >= P.tol_h || U[2].h >= P.tol_h || U[3].h >= P.tol_h);
+        T leaf_dt = P.initial_tstep;
+        if (wet)
+        {
+            const T dxl = P.dx * (1 << (P.L - level));
+            const T z = own.z[0];
+            const T eta_loc = h + z;
+            const T zin = fmax(z, zn[0]), zie = fmax(z, zn[1]), zis = fmax(z, zn[2]), ziw = fmax(z, zn[3]);
+            const V3<T> Uc = {h, qx, qy};
+            const V3<T> Usnn = star(Uc, z, zin, P.tol_h), Usnp = star(U[0], zn[0], zin, P.tol_h);
+            const V3<T> F_n = flux_hll_y(Usnn, Usnp, P.tol_h, P.g);
+            const V3<T> Usen = star(Uc, z, zie, P.tol_h), Usep = star(U[1], zn[1], zie, P.tol_h);
+            const V3<T> F_e = flux_hll_x(Usen, Usep, P.tol_h, P.g);
+            const V3<T> Ussn = star(U[2], zn[2], zis, P.tol_h), Ussp = star(Uc, z, zis, P.tol_h);
+            const V3<T> F_s = flux_hll_y(Ussn, Ussp, P.tol_h, P.g);
+            const V3<T> Uswn = star(U[3], zn[3], ziw, P.tol_h), Uswp = star(Uc, z, ziw, P.tol_h);
+            const V3<T> F_w = flux_hll_x(Uswn, Uswp, P.tol_h, P.g);
+            // operators/get_bed_src.cuh:7-44
+            const T zsw = ziw - fmax(T(0.0), -(eta_loc - ziw));
+            const T zse = zie - fmax(T(0.0), -(eta_loc - zie));
+            const T bx = P.g * T(0.5) * (Uswp.h + Usen.h) * (zse - zsw) / dxl;
+            const T zss = zis - fmax(T(0.0), -(eta_loc - zis));
+            const T zsn = zin - fmax(T(0.0), -(eta_loc - zin));
+            const T by = P.g * T(0.5) * (Ussp.h + Usnn.h) * (zsn - zss) / dxl;
+            h = h - dt * (F_e.h - F_w.h) / dxl;
+            qx = qx - dt * ((F_e.qx - F_w.qx) / dxl + bx);
+            qy = qy - dt * (F_e.qy - F_w.qy) / dxl;
+            h = h - dt * (F_n.h - F_s.h) / dxl;
+            qx = qx - dt * (F_n.qx - F_s.qx) / dxl;
+            qy = qy - dt * ((F_n.qy - F_s.qy) / dxl + by);
+            const bool below_depth = (h < P.tol_h);
+            const bool below_disch = (fabs(qx) < P.tol_q && fabs(qy) < P.tol_q);
+            if (below_depth || below_disch) { qx = T(0.0); qy = T(0.0); }
+            if (!below_depth)
+            {
+                const T ux = qx / h, uy = qy / h;
+                const T dtx = P.CFL * dxl / (fabs(ux) + sqrt(P.g * h));
+                const T dty = P.CFL * dxl / (fabs(uy) + sqrt(P.g * h));
+                leaf_dt = fmin(dtx, dty);
+            }
+            nan_seen |= (h != h);
+        }
+        lf.un[0][i] = h;
+        lf.un[3][i] = qx;
+        lf.un[6][i] = qy;
+        dt_loc = fmin(dt_loc, leaf_dt);
+    }
+    dt_loc = warp_min(dt_loc);
+    __shared__ T red[kSolverThreads / 32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) red[w] = dt_loc;
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        T m = red[0];
+        for (int k = 1; k < (int)(blockDim.x >> 5); ++k) m = fmin(m, red[k]);
+        atomic_min_nn(&sc->dt_min, m);
+    }
+    if (__syncthreads_or(nan_seen) && threadIdx.x == 0) atomicOr(&sc->status, 1);
+}
+
+// Leaf containing each finest cell code (binary search over the leaves' Z-order starts)
+// and its depth eta0 - z0, discharges and bed (output/project_assem_sol.cu:3-77).
+template <typename T>
+__global__ void k_sample_points(Leaves<T> lf, Hier<T> hr, Scalars<T>* sc, int L, const int32_t* codes, int np, T* out)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= np) return;
+    const int n = sc->n_leaves;
+    const int c = codes[k];
+    int lo = 0, hi = n - 1;
+    while (lo < hi)
+    {
+        const int mid = (lo + hi + 1) >> 1;
+        const int l = lf.lvl[mid];
+        const int start = (lf.act[mid] - lvl_idx(l)) << (2 * (L - l));
+        if (start <= c) lo = mid; else hi = mid - 1;
+    }
+    const int a = lf.act[lo];
+    const T z0 = hr.s[3][0][a];
+    const T eta = lf.un[0][lo] + z0;
+    out[4 * k + 0] = eta - z0;
+    out[4 * k + 1] = lf.un[3][lo];
+    out[4 * k + 2] = lf.un[6][lo];
+    out[4 * k + 3] = z0;
+}
+
+// Leaf state with the bed coefficients gathered from the hierarchy, 12 rows of n values.
+template <typename T> __global__ void k_gather_state(Leaves<T> lf, Hier<T> hr, Scalars<T>* sc, bool mw, double* out)
+{
+    const int n = sc->n_leaves;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        const int a = lf.act[i];
+        const size_t N = (size_t)n;
+        out[0 * N + i] = lf.un[0][i];
+        out[1 * N + i] = lf.un[3][i];
+        out[2 * N + i] = lf.un[6][i];
+        out[3 * N + i] = hr.s[3][0][a];
+        out[4 * N + i] = mw ? (double)lf.un[1][i] : 0.0;
+        out[5 * N + i] = mw ? (double)lf.un[4][i] : 0.0;
+        out[6 * N + i] = mw ? (double)lf.un[7][i] : 0.0;
+        out[7 * N + i] = mw ? (double)hr.s[3][1][a] : 0.0;
+        out[8 * N + i] = mw ? (double)lf.un[2][i] : 0.0;
+        out[9 * N + i] = mw ? (double)lf.un[5][i] : 0.0;
+        out[10 * N + i] = mw ? (double)lf.un[8][i] : 0.0;
+        out[11 * N + i] = mw ? (double)hr.s[3][2][a] : 0.0;
+    }
+}
+
+} // namespace mw

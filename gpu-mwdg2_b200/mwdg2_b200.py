@@ -1,0 +1,227 @@
+"""Python binding (ctypes) of the C ABI in include/mwdg2.h.
+
+`Simulation` is the host-side mirror of the reference's run_simulation
+(al0vya/gpu-mwdg2 source/run_simulation.cu): it reads the same .par/.dem/.start/.bci/
+.bdy/.stage inputs, advances adaptive time steps on the GPU and exposes the leaf grid,
+neighbours, significance flags and state for comparison with the reference.
+
+There is no CPU path: constructing a Simulation without the built library or without a
+CUDA device raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from contextlib import contextmanager
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmwdg2_b200.so")
+EXE_PATH = os.path.join(HERE, "gpu-mwdg2")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "mwdg2.h")
+
+STATUS = {0: "OK", 1: "ERR_IO", 2: "ERR_PARSE", 3: "ERR_CUDA", 4: "ERR_NUMERIC", 5: "ERR_TIMEOUT",
+          6: "ERR_ARG", 7: "ERR_STATE", 8: "DONE"}
+STATE_ROWS = ("h0", "qx0", "qy0", "z0", "h1x", "qx1x", "qy1x", "z1x", "h1y", "qx1y", "qy1y", "z1y")
+
+
+class MWDG2Error(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class Opts(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int), ("device", ctypes.c_int), ("epsilon", ctypes.c_double),
+                ("solver", ctypes.c_int), ("dirroot", ctypes.c_char_p), ("write_outputs", ctypes.c_int),
+                ("verbose", ctypes.c_int)]
+
+
+_lib = None
+
+
+def build() -> None:
+    """Compile the library and the gpu-mwdg2 executable for sm_100a."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def exported_symbols() -> list[str]:
+    """Names of the functions declared in include/mwdg2.h."""
+    import re
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"\b(mwdg2_[a-z_]+)\s*\(", text)))
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is not built; run build() (make -C gpu-mwdg2_b200)")
+        L = ctypes.CDLL(LIB_PATH)
+        vp = ctypes.c_void_p
+        i32p = ctypes.POINTER(ctypes.c_int32)
+        i64p = ctypes.POINTER(ctypes.c_int64)
+        dp = ctypes.POINTER(ctypes.c_double)
+        u8p = ctypes.POINTER(ctypes.c_uint8)
+        L.mwdg2_default_opts.argtypes = [ctypes.POINTER(Opts)]
+        L.mwdg2_last_error.restype = ctypes.c_char_p
+        L.mwdg2_create.argtypes = [ctypes.c_char_p, ctypes.POINTER(Opts), ctypes.POINTER(vp)]
+        L.mwdg2_step.argtypes = [vp, dp, i64p]
+        L.mwdg2_run.argtypes = [vp, ctypes.c_int64, i64p, i64p]
+        L.mwdg2_run_simulation.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p)]
+        L.mwdg2_info.argtypes = [vp, dp, ctypes.c_int]
+        L.mwdg2_get_leaves.argtypes = [vp, i32p, i32p, i32p, i32p, ctypes.c_int64]
+        L.mwdg2_get_state.argtypes = [vp, dp, ctypes.c_int64]
+        L.mwdg2_get_sig.argtypes = [vp, u8p, ctypes.c_int64]
+        L.mwdg2_get_hierarchy.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp, ctypes.c_int64]
+        L.mwdg2_read_stage.argtypes = [vp, dp, ctypes.c_int]
+        L.mwdg2_last_step_timing.argtypes = [vp, dp, ctypes.c_int]
+        L.mwdg2_last_step_counters.argtypes = [vp, i64p, ctypes.c_int]
+        L.mwdg2_destroy.argtypes = [vp]
+        for name in ("mwdg2_create", "mwdg2_step", "mwdg2_run", "mwdg2_run_simulation", "mwdg2_info",
+                     "mwdg2_get_leaves", "mwdg2_get_state", "mwdg2_get_sig", "mwdg2_get_hierarchy",
+                     "mwdg2_read_stage", "mwdg2_last_step_timing", "mwdg2_last_step_counters"):
+            getattr(L, name).restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def _check(st: int) -> int:
+    if st not in (0, 8):
+        raise MWDG2Error(st, lib().mwdg2_last_error().decode())
+    return st
+
+
+def _p(a, t):
+    return a.ctypes.data_as(ctypes.POINTER(t))
+
+
+@contextmanager
+def _cwd(path):
+    old = os.getcwd()
+    os.chdir(path)
+    try:
+        yield
+    finally:
+        os.chdir(old)
+
+
+class Simulation:
+    """One adaptive shallow-water simulation on the GPU.
+
+    Relative file names in the .par resolve against the .par's directory (the reference
+    resolves them against the working directory; this wrapper changes into the .par's
+    directory while reading and while writing outputs)."""
+
+    def __init__(self, par: str, precision: int = 64, epsilon: float | None = None,
+                 solver: str | None = None, dirroot: str | None = None, write_outputs: bool = False,
+                 device: int = -1, timing: bool = False):
+        self.par = os.path.abspath(par)
+        self.dir = os.path.dirname(self.par)
+        o = Opts()
+        lib().mwdg2_default_opts(ctypes.byref(o))
+        o.precision = precision
+        o.device = device
+        o.epsilon = -1.0 if epsilon is None else float(epsilon)
+        o.solver = {None: 0, "hwfv1": 1, "mwdg2": 2}[solver]
+        self._dirroot = dirroot.encode() if dirroot else None
+        o.dirroot = self._dirroot
+        o.write_outputs = 1 if write_outputs else 0
+        o.verbose = 2 if timing else 0
+        h = ctypes.c_void_p()
+        with _cwd(self.dir):
+            _check(lib().mwdg2_create(self.par.encode(), ctypes.byref(o), ctypes.byref(h)))
+        self._h = h
+        self.precision = precision
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().mwdg2_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self) -> dict:
+        a = np.zeros(14)
+        _check(lib().mwdg2_info(self._h, _p(a, ctypes.c_double), 14))
+        keys = ("time", "dt", "timestep", "n_leaves", "L", "xsz", "ysz", "dx", "epsilon", "solver",
+                "precision", "sim_time", "n_det", "n_all")
+        d = dict(zip(keys, a.tolist()))
+        for k in ("timestep", "n_leaves", "L", "xsz", "ysz", "solver", "precision", "n_det", "n_all"):
+            d[k] = int(d[k])
+        return d
+
+    def step(self) -> tuple[bool, float, int]:
+        dt = ctypes.c_double()
+        n = ctypes.c_int64()
+        st = _check(lib().mwdg2_step(self._h, ctypes.byref(dt), ctypes.byref(n)))
+        return st == 0, dt.value, n.value
+
+    def run(self, max_steps: int = 0) -> tuple[int, int]:
+        steps = ctypes.c_int64()
+        upd = ctypes.c_int64()
+        with _cwd(self.dir):
+            _check(lib().mwdg2_run(self._h, max_steps, ctypes.byref(steps), ctypes.byref(upd)))
+        return steps.value, upd.value
+
+    def leaves(self) -> dict:
+        n = self.info()["n_leaves"]
+        act = np.zeros(n, np.int32)
+        lvl = np.zeros(n, np.int32)
+        ids = np.zeros(4 * n, np.int32)
+        lvls = np.zeros(4 * n, np.int32)
+        _check(lib().mwdg2_get_leaves(self._h, _p(act, ctypes.c_int32), _p(lvl, ctypes.c_int32),
+                                      _p(ids, ctypes.c_int32), _p(lvls, ctypes.c_int32), n))
+        return {"act": act, "lvl": lvl, "nb_ids": ids.reshape(4, n), "nb_lvls": lvls.reshape(4, n)}
+
+    def state(self) -> dict:
+        n = self.info()["n_leaves"]
+        out = np.zeros(12 * n)
+        _check(lib().mwdg2_get_state(self._h, _p(out, ctypes.c_double), 12 * n))
+        out = out.reshape(12, n)
+        return {k: out[i] for i, k in enumerate(STATE_ROWS)}
+
+    def sig(self) -> np.ndarray:
+        n = self.info()["n_det"]
+        out = np.zeros(n, np.uint8)
+        _check(lib().mwdg2_get_sig(self._h, _p(out, ctypes.c_uint8), n))
+        return out
+
+    def hierarchy(self, field: int, mode: int) -> np.ndarray:
+        n = self.info()["n_all"]
+        out = np.zeros(n)
+        _check(lib().mwdg2_get_hierarchy(self._h, field, mode, _p(out, ctypes.c_double), n))
+        return out
+
+    def stage(self, n_points: int) -> np.ndarray:
+        out = np.zeros(max(1, n_points))
+        _check(lib().mwdg2_read_stage(self._h, _p(out, ctypes.c_double), n_points))
+        return out[:n_points]
+
+    def last_step_timing(self) -> np.ndarray:
+        out = np.zeros(8)
+        _check(lib().mwdg2_last_step_timing(self._h, _p(out, ctypes.c_double), 8))
+        return out
+
+    def last_step_counters(self) -> dict:
+        out = np.zeros(6, np.int64)
+        _check(lib().mwdg2_last_step_counters(self._h, _p(out, ctypes.c_int64), 6))
+        return dict(zip(("encoded", "reencoded", "decoded", "leaves", "detail_slots", "launches"), out.tolist()))
+
+
+def run_simulation(argv: list[str]) -> int:
+    """In-process equivalent of the reference's run_simulation(argc, argv)."""
+    arr = (ctypes.c_char_p * len(argv))(*[a.encode() for a in argv])
+    return lib().mwdg2_run_simulation(len(argv), arr)

@@ -107,14 +107,17 @@ mwdg2_status mwdg2_get_hierarchy(mwdg2_sim* sim, int field, int mode, double* ou
 mwdg2_status mwdg2_read_stage(mwdg2_sim* sim, double* out, int n);
 
 /* Device timing of the last step's kernels, in milliseconds, by phase:
- * [0] maxes+reinsert, [1] encode+regularise, [2] decode+extra significance,
- * [3] leaf topology, [4] solver stage 1 (or FV1), [5] stage-2 (re-encode, gather, update),
- * [6] whole step. Requires opts.verbose >= 2 at create (adds events); else zeros. */
+ * [0] maxima + re-insertion + point sources, [1] encode + threshold + regularisation,
+ * [2] decode + extra significance, [3] leaf topology (leaf list and neighbours),
+ * [4] MWDG2 stage 1 (or the HWFV1 update), [5] stage-1 re-insertion + scale re-encode +
+ * stage-2 maximum depth, [6] MWDG2 stage 2, [7] whole step including the scalar read-back.
+ * Requires opts.verbose >= 2 at create (CUDA events per phase); otherwise zeros. n <= 8. */
 mwdg2_status mwdg2_last_step_timing(mwdg2_sim* sim, double* out, int n);
 
 /* Counters of the last step used for the algorithmic-bytes roofline:
  * [0] parents encoded (E), [1] parents re-encoded scale-only (E2), [2] parents decoded (D),
- * [3] leaves (N_a), [4] detail slots (T = get_lvl_idx(L) - 3). n >= 5. */
+ * [3] leaves (N_a), [4] detail slots (T = get_lvl_idx(L) - 3), [5] kernels launched in the
+ * step. n <= 6. */
 mwdg2_status mwdg2_last_step_counters(mwdg2_sim* sim, int64_t* out, int n);
 
 void mwdg2_destroy(mwdg2_sim* sim);

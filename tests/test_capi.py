@@ -1,0 +1,53 @@
+"""The C-ABI library loads and exports every entry point declared in include/mwdg2.h,
+and rejects bad input without touching a GPU."""
+import ctypes
+import os
+
+import pytest
+
+import mwdg2_b200
+
+
+def test_header_lists_entry_points():
+    names = mwdg2_b200.exported_symbols()
+    for must in ("mwdg2_create", "mwdg2_step", "mwdg2_run", "mwdg2_run_simulation", "mwdg2_get_leaves",
+                 "mwdg2_get_state", "mwdg2_get_sig", "mwdg2_read_stage", "mwdg2_destroy"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = mwdg2_b200.lib()
+    for name in mwdg2_b200.exported_symbols():
+        assert hasattr(lib, name), name
+
+
+def test_default_opts():
+    o = mwdg2_b200.Opts()
+    mwdg2_b200.lib().mwdg2_default_opts(ctypes.byref(o))
+    assert o.precision == 64 and o.device == -1 and o.epsilon < 0 and o.solver == 0 and o.write_outputs == 1
+
+
+def test_missing_par_is_io_error(tmp_path):
+    with pytest.raises(mwdg2_b200.MWDG2Error) as e:
+        mwdg2_b200.Simulation(str(tmp_path / "nope.par"))
+    assert e.value.status == 1
+
+
+def test_bad_precision_is_arg_error(tmp_path):
+    with pytest.raises(mwdg2_b200.MWDG2Error) as e:
+        mwdg2_b200.Simulation(str(tmp_path / "nope.par"), precision=16)
+    assert e.value.status == 6
+
+
+def test_unsupported_solver_keyword_is_parse_error(tmp_path):
+    p = tmp_path / "x.par"
+    p.write_text("max_ref_lvl 7\nDEMfile a.dem\n")
+    with pytest.raises(mwdg2_b200.MWDG2Error) as e:
+        mwdg2_b200.Simulation(str(p))
+    assert e.value.status == 2
+
+
+def test_null_handle_calls_are_rejected():
+    lib = mwdg2_b200.lib()
+    assert lib.mwdg2_step(None, None, None) == 6
+    assert lib.mwdg2_info(None, None, 0) == 6
