@@ -443,7 +443,8 @@ __device__ __forceinline__ int tile_leaf_level(const uint8_t* flags, int Tl, int
     return Tl;
 }
 
-__global__ void __launch_bounds__(kTileThreads) k_tile_count(const uint8_t* flags, int L, int D, int32_t* counts)
+// static: the header is included by more than one translation unit of the library
+static __global__ void __launch_bounds__(kTileThreads) k_tile_count(const uint8_t* flags, int L, int D, int32_t* counts)
 {
     const int Tl = L - D;
     const int tcode = blockIdx.x;

@@ -672,6 +672,9 @@ template <typename T> mwdg2_status Sim<T>::counters(int64_t* out, int n)
 
 } // namespace
 
+// Internal: lets other translation units of the library set the mwdg2_last_error text.
+void mwdg2_detail_set_last_error(const char* msg) { g_last_error = msg ? msg : ""; }
+
 // ============================================================================ C ABI
 
 struct mwdg2_sim

@@ -122,6 +122,36 @@ mwdg2_status mwdg2_last_step_counters(mwdg2_sim* sim, int64_t* out, int n);
 
 void mwdg2_destroy(mwdg2_sim* sim);
 
+/* Leaf topology from significance flags, allocating no device memory. No counterpart in
+ * the reference: it is for callers that cannot call cudaMalloc -- code running under a
+ * memory manager that owns all device memory (a framework that reserves the device heap
+ * up front) and real-time loops that must not enter the CUDA allocator, which may
+ * synchronise the device and take driver locks. It computes what mwdg2_step computes
+ * after remeshing: the leaves of the tree given by d_sig in Z order, their levels and
+ * their four neighbours (north, east, south, west; -1 at the border), exactly as
+ * mwdg2_get_leaves reports them.
+ *
+ *   d_sig        device, get_lvl_idx(max_ref_lvl) bytes, 1 = significant (as returned
+ *                by mwdg2_get_sig); every significant node's parent must be significant
+ *   max_ref_lvl  5..13: the kernels' scratch is a file-scope device array of 65536 tile
+ *                counts (about 256 KiB per device, held until the process exits); larger
+ *                levels are rejected with MWDG2_ERR_ARG
+ *   xsz, ysz     DEM size in cells (1..2^max_ref_lvl)
+ *   d_act        device int32[cap]; d_levels device uint8[cap]
+ *   d_nb_ids     device int32[4*cap]; d_nb_levels device uint8[4*cap] ([4][cap] layout)
+ *   cap          at least 4^max_ref_lvl (every finest cell a leaf)
+ *   n_leaves_out host; number of leaves written
+ *   stream       cudaStream_t to run on (NULL: the default stream); the call returns
+ *                after the outputs are complete
+ * The first call on a device looks up the scratch array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call before any
+ * stream capture. Every call on a device shares the one scratch array, so calls whose
+ * work overlaps on the GPU (different host threads or streams) race: serialise them. */
+mwdg2_status mwdg2_leaf_topology_static(const uint8_t* d_sig, int max_ref_lvl, int xsz, int ysz,
+                                        int32_t* d_act, uint8_t* d_levels, int32_t* d_nb_ids,
+                                        uint8_t* d_nb_levels, int64_t cap, int64_t* n_leaves_out,
+                                        void* stream);
+
 #ifdef __cplusplus
 }
 #endif
