@@ -564,6 +564,12 @@ __device__ __forceinline__ void emit_leaf(const Leaves<T>& lf, const uint8_t* fl
     for (int d = 0; d < 4; ++d) { lf.nb[d][pos] = id[d]; lf.nbl[d][pos] = lv[d]; }
 }
 
+// Leaves of one tile in Z order with their neighbours. The tile's subtree flags are
+// copied to shared memory; every finest cell of the tile gets the level of the leaf that
+// contains it (walk down the shared flags); leaf starts are ranked with popcounts; then
+// thread r writes the leaf of rank r (coalesced), looking its neighbours up in the
+// per-cell level map when the neighbouring cell lies in the tile and descending the
+// global flags otherwise.
 template <typename T>
 __global__ void __launch_bounds__(kTileThreads) k_tile_emit(Leaves<T> lf, const uint8_t* flags, const int32_t* offsets,
                                                             int L, int D, int M, int xsz, int ysz)
@@ -571,9 +577,12 @@ __global__ void __launch_bounds__(kTileThreads) k_tile_emit(Leaves<T> lf, const 
     const int Tl = L - D;
     const int tcode = blockIdx.x;
     const int off = offsets[tcode];
-    __shared__ int s_k;
-    __shared__ uint32_t bits[32];      // leaf starts among the tile's 4^D (<= 1024) finest cells
-    __shared__ int32_t prefix[33];
+    __shared__ int s_k, s_total;
+    __shared__ uint8_t sflag[344];      // flags of levels Tl .. L-1 below the tile root (<= 341)
+    __shared__ uint8_t cell_lvl[1024];  // leaf level of each finest cell, tile-local Morton order
+    __shared__ uint16_t start_of[1024]; // tile-local start cell of the leaf of each rank
+    __shared__ uint32_t bits[32];       // leaf starts
+    __shared__ int32_t prefix[32];
     if (threadIdx.x == 0) s_k = tile_leaf_level(flags, Tl, tcode);
     if (threadIdx.x < 32) bits[threadIdx.x] = 0;
     __syncthreads();
@@ -590,48 +599,86 @@ __global__ void __launch_bounds__(kTileThreads) k_tile_emit(Leaves<T> lf, const 
         if (threadIdx.x == 0) emit_leaf(lf, flags, L, M, xsz, ysz, off, root, Tl);
         return;
     }
-    // nodes of levels Tl+1 .. L below the tile root: 4 + 16 + ... + 4^D
-    const int nodes = ((1 << (2 * (D + 1))) - 1) / 3 - 1;
-    for (int pass = 0; pass < 2; ++pass)
+    const int nodes = ((1 << (2 * D)) - 1) / 3;
+    for (int i = threadIdx.x; i < nodes; i += blockDim.x)
     {
-        for (int i = threadIdx.x; i < nodes; i += blockDim.x)
+        int j = 0, base = 0;
+        while (i >= base + (1 << (2 * j))) { base += 1 << (2 * j); ++j; }
+        sflag[i] = flags[lvl_idx(Tl + j) + (tcode << (2 * j)) + (i - base)] & F_SIG;
+    }
+    __syncthreads();
+    const int ncell = 1 << (2 * D);
+    for (int c = threadIdx.x; c < ncell; c += blockDim.x)
+    {
+        int lev = L, base = 0;
+        for (int j = 0; j < D; ++j)
         {
-            int j = 1, base = 0;
-            while (i >= base + (1 << (2 * j))) { base += 1 << (2 * j); ++j; }
-            const int lc = i - base;                       // local code at level Tl + j
-            const int lev = Tl + j;
-            const int parent = lvl_idx(lev - 1) + (tcode << (2 * (j - 1))) + (lc >> 2);
-            const int node = lvl_idx(lev) + (tcode << (2 * j)) + lc;
-            const bool leaf = (flags[parent] & F_SIG) && (lev == L || !(flags[node] & F_SIG));
-            if (!leaf) continue;
-            const int start = lc << (2 * (D - j));         // first finest cell, local to the tile
-            if (pass == 0)
+            if (!sflag[base + (c >> (2 * (D - j)))]) { lev = Tl + j; break; }
+            base += 1 << (2 * j);
+        }
+        cell_lvl[c] = (uint8_t)lev;
+        if ((c & ((1 << (2 * (L - lev))) - 1)) == 0) atomicOr(&bits[c >> 5], 1u << (c & 31));
+    }
+    __syncthreads();
+    if (threadIdx.x < 32)
+    {
+        const int cnt = __popc(bits[threadIdx.x]);
+        int incl = cnt;
+        for (int o = 1; o < 32; o <<= 1)
+        {
+            const int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if ((int)threadIdx.x >= o) incl += v;
+        }
+        prefix[threadIdx.x] = incl - cnt;
+        if (threadIdx.x == 31) s_total = incl;
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < ncell; c += blockDim.x)
+    {
+        const int w = c >> 5;
+        const uint32_t b = bits[w];
+        if (b & (1u << (c & 31))) start_of[prefix[w] + __popc(b & ((1u << (c & 31)) - 1u))] = (uint16_t)c;
+    }
+    __syncthreads();
+    const int total = s_total;
+    const int tbase = tcode << (2 * D);              // finest Morton code of the tile's first cell
+    const int tx0 = compact(tbase), ty0 = compact(tbase >> 1), tw = 1 << D;
+    for (int r = threadIdx.x; r < total; r += blockDim.x)
+    {
+        const int c = start_of[r];
+        const int lev = cell_lvl[c];
+        const int gc = tbase + c;                     // finest code of the leaf's south-west cell
+        const int pos = off + r;
+        lf.act[pos] = lvl_idx(lev) + (gc >> (2 * (L - lev)));
+        lf.lvl[pos] = (uint8_t)lev;
+        const int s = 1 << (L - lev);
+        const int x0 = compact(gc), y0 = compact(gc >> 1), xe = x0 + s - 1, ye = y0 + s - 1;
+        int32_t id[4];
+        uint8_t lv[4];
+        // target finest cell of each direction, -1 border rule of neighbours/find_neighbours.cu
+        const bool nb_border[4] = {(ye == M - 1 || ye == ysz - 1) && ye != 0, (xe == M - 1 || xe == xsz - 1) && xe != 0,
+                                   y0 == 0, x0 == 0};
+        const int txs[4] = {xe, xe + 1, x0, x0 - 1};
+        const int tys[4] = {ye + 1, ye, y0 - 1, y0};
+#pragma unroll
+        for (int d = 0; d < 4; ++d)
+        {
+            if (nb_border[d]) { id[d] = -1; lv[d] = (uint8_t)lev; continue; }
+            const int tx = txs[d], ty = tys[d];
+            if (tx >= tx0 && tx < tx0 + tw && ty >= ty0 && ty < ty0 + tw)
             {
-                atomicOr(&bits[start >> 5], 1u << (start & 31));
+                const int lt = cell_lvl[morton(tx - tx0, ty - ty0)];
+                const int m = lev < lt ? lev : lt;
+                id[d] = lvl_idx(m) + (morton(tx, ty) >> (2 * (L - m)));
+                lv[d] = (uint8_t)m;
             }
             else
             {
-                const int w = start >> 5;
-                const int rank = prefix[w] + __popc(bits[w] & ((1u << (start & 31)) - 1u));
-                emit_leaf(lf, flags, L, M, xsz, ysz, off + rank, node, lev);
+                descend(flags, L, lev, gc, tx, ty, id[d], lv[d]);
             }
         }
-        __syncthreads();
-        if (pass == 0)
-        {
-            if (threadIdx.x < 32)
-            {
-                const int c = __popc(bits[threadIdx.x]);
-                int incl = c;
-                for (int o = 1; o < 32; o <<= 1)
-                {
-                    const int v = __shfl_up_sync(0xffffffffu, incl, o);
-                    if ((int)threadIdx.x >= o) incl += v;
-                }
-                prefix[threadIdx.x] = incl - c;
-            }
-            __syncthreads();
-        }
+#pragma unroll
+        for (int d = 0; d < 4; ++d) { lf.nb[d][pos] = id[d]; lf.nbl[d][pos] = lv[d]; }
     }
 }
 

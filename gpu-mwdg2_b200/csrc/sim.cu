@@ -302,8 +302,14 @@ template <typename T> mwdg2_status Sim<T>::launch_step()
     mw::k_step_begin<T><<<1, 1, 0, st_>>>(sc_);
     ++launches_;
     const int nfix = first_ ? (int)F_ : -1;
-    if (mw) { mw::k_maxes_reinsert<T, true><<<red_blocks_, 256, 0, st_>>>(lf_, hr_, sc_, nfix, !first_); ++launches_; }
-    else { mw::k_maxes_reinsert<T, false><<<red_blocks_, 256, 0, st_>>>(lf_, hr_, sc_, nfix, !first_); ++launches_; }
+    // leaf count before remeshing is known exactly; after remeshing it is near the previous
+    // step's, so per-leaf grids are sized from it (grid-stride loops cover any growth)
+    const int g_prev = grid_for(n_leaves_, 256, 1 << 20);
+    const int64_t n_hint = std::min<int64_t>(F_, (int64_t)n_leaves_ + n_leaves_ / 4 + 1024);
+    const int g_leaf = grid_for(n_hint, 256, 1 << 20);
+    const int g_solver = grid_for(n_hint, mw::kSolverThreads, 1 << 20);
+    if (mw) { mw::k_maxes_reinsert<T, true><<<g_prev, 256, 0, st_>>>(lf_, hr_, sc_, nfix, !first_); ++launches_; }
+    else { mw::k_maxes_reinsert<T, false><<<g_prev, 256, 0, st_>>>(lf_, hr_, sc_, nfix, !first_); ++launches_; }
     // point sources (classes/PointSources.h:453-472 on the host, then the kernel)
     const int nsrc = (int)cs_.srcs.size();
     if (nsrc > 0)
@@ -362,7 +368,7 @@ template <typename T> mwdg2_status Sim<T>::launch_step()
     const bool fric = cs_.manning > T(0);
     if (!mw)
     {
-        mw::k_hwfv1<T><<<solver_blocks_, mw::kSolverThreads, 0, st_>>>(lf_, hr_, sc_, P_, B, dt_, fric);
+        mw::k_hwfv1<T><<<g_solver, mw::kSolverThreads, 0, st_>>>(lf_, hr_, sc_, P_, B, dt_, fric);
         ++launches_;
         rec(5);
         rec(6);
@@ -370,10 +376,10 @@ template <typename T> mwdg2_status Sim<T>::launch_step()
     }
     else
     {
-        mw::k_mwdg2_stage<T, 1><<<solver_blocks_, mw::kSolverThreads, 0, st_>>>(lf_, hr_, sc_, P_, B, dt_, fric);
+        mw::k_mwdg2_stage<T, 1><<<g_solver, mw::kSolverThreads, 0, st_>>>(lf_, hr_, sc_, P_, B, dt_, fric);
         ++launches_;
         rec(5);
-        mw::k_reinsert_us<T><<<red_blocks_, 256, 0, st_>>>(lf_, hr_, sc_);
+        mw::k_reinsert_us<T><<<g_leaf, 256, 0, st_>>>(lf_, hr_, sc_);
         ++launches_;
         if (eps > T(0))
         {
@@ -386,9 +392,9 @@ template <typename T> mwdg2_status Sim<T>::launch_step()
             mw::k_encode_top<T, true, false><<<1, 256, 0, st_>>>(hr_, sc_, L_, top, eps);
             ++launches_;
         }
-        if (cs_.limitslopes) { mw::k_stage2_maxh<T><<<red_blocks_, 256, 0, st_>>>(lf_, hr_, sc_, P_, B, dt_); ++launches_; }
+        if (cs_.limitslopes) { mw::k_stage2_maxh<T><<<g_leaf, 256, 0, st_>>>(lf_, hr_, sc_, P_, B, dt_); ++launches_; }
         rec(6);
-        mw::k_mwdg2_stage<T, 2><<<solver_blocks_, mw::kSolverThreads, 0, st_>>>(lf_, hr_, sc_, P_, B, dt_, false);
+        mw::k_mwdg2_stage<T, 2><<<g_solver, mw::kSolverThreads, 0, st_>>>(lf_, hr_, sc_, P_, B, dt_, false);
         ++launches_;
         rec(7);
     }

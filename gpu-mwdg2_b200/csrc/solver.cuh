@@ -265,6 +265,15 @@ __global__ void __launch_bounds__(kSolverThreads) k_mwdg2_stage(Leaves<T> lf, Hi
         load_cell<T, true>(hr, a, own);
         T gh[4], gqx[4], gqy[4];
         ghost_pass(own.h[0], own.qx[0], own.qy[0], own.z[0], nid, level, a, P, B, dt, gh, gqx, gqy);
+        // Depths of the four neighbours (after ghost cells). A leaf whose own depth and
+        // neighbour depths are all below tol_h is not updated (dg2_update.cu:36-50), is not
+        // limited (the limiter needs a depth above 0.05 max_h) and, being below tol_h, gets
+        // no friction: it needs none of the neighbours' other coefficients.
+        T nbh[4];
+#pragma unroll
+        for (int d = 0; d < 4; ++d) nbh[d] = (nid[d] != -1) ? hr.s[0][0][nid[d]] - hr.s[3][0][nid[d]] : gh[d];
+        const bool dry = own.h[0] < P.tol_h && nbh[0] < P.tol_h && nbh[1] < P.tol_h && nbh[2] < P.tol_h &&
+                         nbh[3] < P.tol_h;
         // friction_implicit.cu:24-48: shallow or slow leaves lose their discharge and
         // skip friction (their neighbours' copies are then left untouched too)
         bool fric = false;
@@ -278,6 +287,20 @@ __global__ void __launch_bounds__(kSolverThreads) k_mwdg2_stage(Leaves<T> lf, Hi
             if (below_depth || below_speed) { own.qx[0] = T(0.0); own.qy[0] = T(0.0); }
             fric = !(below_depth || below_speed);
             if (fric) friction_cell<T, true>(own, P, dt);
+        }
+        if (dry)
+        {
+            if (STAGE == 1)
+            {
+#pragma unroll
+                for (int m = 0; m < 3; ++m)
+                {
+                    lf.un[m][i] = own.h[m]; lf.un[3 + m][i] = own.qx[m]; lf.un[6 + m][i] = own.qy[m];
+                    lf.us[m][i] = own.h[m]; lf.us[3 + m][i] = own.qx[m]; lf.us[6 + m][i] = own.qy[m];
+                }
+            }
+            dt_loc = fmin(dt_loc, P.initial_tstep);
+            continue;
         }
         const Geo<T> geo = leaf_geo<T>(a, level, P);
         NbFace<T> nf[4];
@@ -467,6 +490,18 @@ __global__ void __launch_bounds__(kSolverThreads) k_hwfv1(Leaves<T> lf, Hier<T> 
             if (below_depth || below_speed) { own.qx[0] = T(0.0); own.qy[0] = T(0.0); }
             fric = !(below_depth || below_speed);
             if (fric) friction_cell<T, false>(own, P, dt);
+        }
+        T nbh[4];
+#pragma unroll
+        for (int d = 0; d < 4; ++d) nbh[d] = (nid[d] != -1) ? hr.s[0][0][nid[d]] - hr.s[3][0][nid[d]] : gh[d];
+        if (own.h[0] < P.tol_h && nbh[0] < P.tol_h && nbh[1] < P.tol_h && nbh[2] < P.tol_h && nbh[3] < P.tol_h)
+        {
+            // dry leaf: not updated (fv1_update.cu:27-46), discharge zeroed by friction if enabled
+            lf.un[0][i] = own.h[0];
+            lf.un[3][i] = own.qx[0];
+            lf.un[6][i] = own.qy[0];
+            dt_loc = fmin(dt_loc, P.initial_tstep);
+            continue;
         }
         V3<T> U[4];
         T zn[4];
