@@ -278,8 +278,8 @@ def main():
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": int(sum(cc["launches"] for cc in counters)),
             "clocks": clk.summary(),
-            "phase_ms_mean": dict(zip(("maxes_reinsert_srcs", "encode", "decode", "topology", "stage1",
-                                       "reinsert_reencode", "stage2", "step"), [round(x, 4) for x in mean_ph])),
+            "phase_ms_mean": dict(zip(("step_begin_srcs", "encode", "decode", "topology", "stage1",
+                                       "reencode", "stage2", "step"), [round(x, 4) for x in mean_ph])),
             "leaves_mean": n_mean}
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(par, a, a.cpu_steps)

@@ -2,12 +2,14 @@
 //
 // Data layout in HBM (one simulation):
 //   hierarchy  s[field][mode][h]   field eta,qx,qy,z; mode 0,1x,1y; h = get_lvl_idx(level)+Morton
-//   details    det[field][t*3+m][p] field eta,qx,qy; t alpha,beta,gamma; parents only
-//   norm[p], flags[p]              parents only (levels 0..L-1); flag bits F_SIG/F_ENC/F_PRE
-//   leaves     act, lvl, nb[4], nbl[4], un[9] (state), us[9] (RK stage-1 result), in Z order
+//   flags[p]                       parents only (levels 0..L-1); flag bits F_SIG/F_ENC/F_PRE
+//   stage      s[field<3][mode][h] of the RK stage-1 result (leaves and significant parents;
+//              the bed is shared with the hierarchy)
+//   leaves     act, lvl, nb[4], nbl[4], un[9] (state), in Z order
 //
-// Work per step touches the significant part of the tree and the leaves only; no array
-// is cleared per step (the F_ENC bit marks which parents hold fresh details).
+// Work per step touches the significant part of the tree and the leaves only. Details are
+// never stored: the decode recomputes them from the children (F_ENC marks the parents
+// whose details are non-zero this step), so no detail or norm array is written or cleared.
 #pragma once
 
 #include "mw_math.cuh"
@@ -21,8 +23,6 @@ constexpr int kSolverThreads = 128;
 template <typename T> struct Hier
 {
     T* s[4][3];
-    T* det[3][9];
-    T* norm;
     uint8_t* flags;
 };
 
@@ -33,7 +33,6 @@ template <typename T> struct Leaves
     int32_t* nb[4];
     uint8_t* nbl[4];
     T* un[9];   // [field*3 + mode], field h, qx, qy
-    T* us[9];
 };
 
 template <typename T> struct Scalars
@@ -44,6 +43,8 @@ template <typename T> struct Scalars
     int32_t n_leaves;
     int32_t status;                   // bit 0: NaN seen in the state
     unsigned long long enc, enc2, dec;
+    int32_t wet[2];                   // leaves not dry in RK stage 1 / stage 2 (wet-list lengths)
+    T next_max[4];                    // maxima of the state at the end of the step (eta, h, qx, z)
 };
 
 template <typename T> struct Params
@@ -117,12 +118,20 @@ __device__ __forceinline__ void block_max_atomic(T (&v)[N], T* const (&dst)[N])
 }
 
 // ---------------------------------------------------------------- step bookkeeping
-template <typename T> __global__ void k_step_begin(Scalars<T>* sc)
+// carry: the maxima come from the previous step's final RK stage (MWDG2 after its first
+// step); otherwise k_maxes_reinsert computes them.
+template <typename T> __global__ void k_step_begin(Scalars<T>* sc, bool carry)
 {
-    sc->max_eta = T(0); sc->max_h = T(0); sc->max_qx = T(0); sc->max_z = T(0);
+    sc->max_eta = carry ? sc->next_max[0] : T(0);
+    sc->max_h = carry ? sc->next_max[1] : T(0);
+    sc->max_qx = carry ? sc->next_max[2] : T(0);
+    sc->max_z = carry ? sc->next_max[3] : T(0);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) sc->next_max[k] = T(0);
     sc->max_h2 = T(0);
     sc->dt_min = (sizeof(T) == 8) ? T(1.0e308) : T(3.0e38);
     sc->enc = 0; sc->enc2 = 0; sc->dec = 0;
+    sc->wet[0] = 0; sc->wet[1] = 0;
 }
 
 // Maxima of the leaf state (mra/get_max_scale_coeffs.cu:3-27, with the reference's
@@ -266,10 +275,6 @@ __device__ __forceinline__ void encode_parent(const Hier<T>& hr, const Scalars<T
                 hr.s[fld][0][p] = s[0]; hr.s[fld][1][p] = s[1]; hr.s[fld][2][p] = s[2];
                 T d[3][3];
                 mw_encode_details(k, d);
-#pragma unroll
-                for (int t = 0; t < 3; ++t)
-#pragma unroll
-                    for (int m = 0; m < 3; ++m) hr.det[fld][t * 3 + m][p] = d[t][m];
                 nd = fmax(nd, mw_detail_max(d) / mx[fld]);
             }
             else
@@ -278,13 +283,11 @@ __device__ __forceinline__ void encode_parent(const Hier<T>& hr, const Scalars<T
                 load4(hr.s[fld][0] + c, k);
                 hr.s[fld][0][p] = hw_scale(k);
                 const T a = hw_alpha(k), b = hw_beta(k), g = hw_gamma(k);
-                hr.det[fld][0][p] = a; hr.det[fld][3][p] = b; hr.det[fld][6][p] = g;
                 T m1 = fmax(fabs(a), fabs(b));
                 m1 = fmax(fabs(g), m1);
                 nd = fmax(nd, m1 / mx[fld]);
             }
         }
-        hr.norm[p] = nd;
         if (nd >= encode_eps(eps, L, level) || (f & F_PRE)) nf |= F_SIG;
         if (!(nf & F_SIG) && level <= L - 2)
         {
@@ -324,14 +327,23 @@ __global__ void __launch_bounds__(256) k_encode_top(Hier<T> hr, Scalars<T>* sc, 
 // Decode one significant parent into its four children (mra/decoding_kernel_{mw,hw}.cu)
 // and apply extra significance (mra/extra_significance_kernel.cu: parents whose norm
 // reaches eps_l * 2^(M_BAR+1) make all four children significant).
+// The details of a parent encoded this step are recomputed here from its children,
+// which no kernel has changed since the encode read them (encode runs bottom-up and
+// decode top-down, so a level's children are overwritten only by this very decode);
+// the result is bit-identical to the encode's and no detail arrays are stored. Parents
+// made significant without being encoded have zero details and zero norm, as in the
+// reference (mra/zero_details.cu).
 template <typename T, bool MW>
-__device__ __forceinline__ void decode_parent(const Hier<T>& hr, int L, int level, int idx, T eps, unsigned& n_done)
+__device__ __forceinline__ void decode_parent(const Hier<T>& hr, const Scalars<T>* sc, int L, int level, int idx, T eps,
+                                              unsigned& n_done)
 {
     const int p = lvl_idx(level) + idx;
     const uint8_t f = hr.flags[p];
     if (!(f & F_SIG)) return;
     const bool enc = (f & F_ENC) != 0;
     const int c = lvl_idx(level + 1) + 4 * idx;
+    const T mx[3] = {fmax(T(1.0), sc->max_eta), fmax(T(1.0), sc->max_qx), fmax(T(1.0), sc->max_qx)};
+    T nd = T(0.0);
 #pragma unroll
     for (int fld = 0; fld < 3; ++fld)
     {
@@ -339,10 +351,20 @@ __device__ __forceinline__ void decode_parent(const Hier<T>& hr, int L, int leve
         {
             const T s[3] = {hr.s[fld][0][p], hr.s[fld][1][p], hr.s[fld][2][p]};
             T d[3][3];
+            if (enc)
+            {
+                T k[3][4];
+                load4(hr.s[fld][0] + c, k[0]); load4(hr.s[fld][1] + c, k[1]); load4(hr.s[fld][2] + c, k[2]);
+                mw_encode_details(k, d);
+                nd = fmax(nd, mw_detail_max(d) / mx[fld]);
+            }
+            else
+            {
 #pragma unroll
-            for (int t = 0; t < 3; ++t)
+                for (int t = 0; t < 3; ++t)
 #pragma unroll
-                for (int m = 0; m < 3; ++m) d[t][m] = enc ? hr.det[fld][t * 3 + m][p] : T(0.0);
+                    for (int m = 0; m < 3; ++m) d[t][m] = T(0.0);
+            }
             T k[3][4];
             mw_decode(s, d, k);
             store4(hr.s[fld][0] + c, k[0]); store4(hr.s[fld][1] + c, k[1]); store4(hr.s[fld][2] + c, k[2]);
@@ -350,9 +372,16 @@ __device__ __forceinline__ void decode_parent(const Hier<T>& hr, int L, int leve
         else
         {
             const T u = hr.s[fld][0][p];
-            const T a = enc ? hr.det[fld][0][p] : T(0.0);
-            const T b = enc ? hr.det[fld][3][p] : T(0.0);
-            const T g = enc ? hr.det[fld][6][p] : T(0.0);
+            T a = T(0.0), b = T(0.0), g = T(0.0);
+            if (enc)
+            {
+                T k[4];
+                load4(hr.s[fld][0] + c, k);
+                a = hw_alpha(k); b = hw_beta(k); g = hw_gamma(k);
+                T m1 = fmax(fabs(a), fabs(b));
+                m1 = fmax(fabs(g), m1);
+                nd = fmax(nd, m1 / mx[fld]);
+            }
             T k[4];
             hw_decode(u, a, b, g, k);
             store4(hr.s[fld][0] + c, k);
@@ -363,8 +392,7 @@ __device__ __forceinline__ void decode_parent(const Hier<T>& hr, int L, int leve
     {
         const T eps_local = eps / (1 << (L - level));
         const T eps_extra = eps_local * pow(T(2.0), T(1.5) + 1);
-        const T nrm = enc ? hr.norm[p] : T(0.0);
-        if (nrm >= eps_extra) *reinterpret_cast<uint32_t*>(hr.flags + c) |= 0x01010101u;
+        if (nd >= eps_extra) *reinterpret_cast<uint32_t*>(hr.flags + c) |= 0x01010101u;
     }
 }
 
@@ -373,7 +401,7 @@ __global__ void __launch_bounds__(256) k_decode_level(Hier<T> hr, Scalars<T>* sc
 {
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned done = 0;
-    if (idx < (1 << (2 * level))) decode_parent<T, MW>(hr, L, level, idx, eps, done);
+    if (idx < (1 << (2 * level))) decode_parent<T, MW>(hr, sc, L, level, idx, eps, done);
     const unsigned tot = __reduce_add_sync(0xffffffffu, done);
     if ((threadIdx.x & 31) == 0 && tot) atomicAdd(&sc->dec, (unsigned long long)tot);
 }
@@ -385,7 +413,7 @@ __global__ void __launch_bounds__(256) k_decode_top(Hier<T> hr, Scalars<T>* sc, 
     for (int level = 0; level <= top; ++level)
     {
         for (int idx = threadIdx.x; idx < (1 << (2 * level)); idx += blockDim.x)
-            decode_parent<T, MW>(hr, L, level, idx, eps, done);
+            decode_parent<T, MW>(hr, sc, L, level, idx, eps, done);
         __syncthreads();
     }
     const unsigned tot = __reduce_add_sync(0xffffffffu, done);
@@ -436,44 +464,73 @@ __global__ void __launch_bounds__(256) k_topo_level(Hier<T> hr, Scalars<T>* sc, 
 // neighbours/compaction.cu).
 
 // First level on the root -> tile path whose node is not significant; Tl if none.
-__device__ __forceinline__ int tile_leaf_level(const uint8_t* flags, int Tl, int tcode)
+// Called by a whole warp: lane j loads level j's flag, so the Tl (<= 10) loads are
+// independent instead of a chain of dependent loads.
+__device__ __forceinline__ int tile_leaf_level_warp(const uint8_t* flags, int Tl, int tcode)
 {
-    for (int j = 0; j < Tl; ++j)
-        if (!(flags[lvl_idx(j) + (tcode >> (2 * (Tl - j)))] & F_SIG)) return j;
-    return Tl;
+    const int lane = threadIdx.x & 31;
+    const bool nonsig = lane < Tl && !(flags[lvl_idx(lane) + (tcode >> (2 * (Tl - lane)))] & F_SIG);
+    const unsigned m = __ballot_sync(0xffffffffu, nonsig);
+    return m ? __ffs(m) - 1 : Tl;
+}
+
+// First level j in [j0, lim) whose node on the path to finest cell `tc` is not
+// significant; lim if none. The (at most 16) flag loads are issued independently.
+__device__ __forceinline__ int first_nonsig_level(const uint8_t* flags, int L, int tc, int j0, int lim)
+{
+    unsigned nonsig = 0;
+#pragma unroll
+    for (int t = 0; t < 16; ++t)
+    {
+        const int j = j0 + t;
+        if (j < lim && !(flags[lvl_idx(j) + (tc >> (2 * (L - j)))] & F_SIG)) nonsig |= 1u << t;
+    }
+    return nonsig ? j0 + __ffs(nonsig) - 1 : lim;
+}
+
+// Morton codes hold x in the even bits and y in the odd bits. Arithmetic on one
+// coordinate of a code ("dilated integers") needs no de-interleaving: with m the mask of
+// that coordinate's bits, (a | ~m) + b carries through the other coordinate's bits.
+constexpr unsigned kXBits = 0x55555555u, kYBits = 0xAAAAAAAAu;
+__device__ __forceinline__ unsigned dil_add(unsigned a, unsigned b, unsigned m) { return ((a | ~m) + b) & m; }
+__device__ __forceinline__ unsigned dil_sub(unsigned a, unsigned b, unsigned m) { return (a - b) & m; }
+
+// Word w (0..84) of the flags of levels Tl+1 .. Tl+4 below tile root `tcode` (levels
+// Tl+1..Tl+4 hold 1, 4, 16, 64 words): its level offset j (1..4) and global byte index.
+// lvl_idx(l) is a multiple of 4 for l >= 1, so every word is aligned.
+__device__ __forceinline__ int tile_flag_word(int Tl, int tcode, int w, int& j)
+{
+    j = 1 + (w >= 1) + (w >= 5) + (w >= 21);
+    const int wbase = (j == 1) ? 0 : (j == 2) ? 1 : (j == 3) ? 5 : 21;
+    return lvl_idx(Tl + j) + (tcode << (2 * j)) + 4 * (w - wbase);
 }
 
 // static: the header is included by more than one translation unit of the library
-static __global__ void __launch_bounds__(kTileThreads) k_tile_count(const uint8_t* flags, int L, int D, int32_t* counts)
+static __global__ void __launch_bounds__(kTileThreads) k_tile_count(const uint8_t* flags, int L, int32_t* counts)
 {
-    const int Tl = L - D;
+    static_assert(kTileDepth == 5, "the word layout of tile_flag_word assumes 4^5-cell tiles");
+    const int Tl = L - kTileDepth;
     const int tcode = blockIdx.x;
-    __shared__ int s_k;
-    if (threadIdx.x == 0) s_k = tile_leaf_level(flags, Tl, tcode);
-    __syncthreads();
-    const int k = s_k;
-    if (k < Tl)
+    const int k = tile_leaf_level_warp(flags, Tl + 1, tcode << 2);  // levels 0..Tl, every warp finds it
+    if (k <= Tl)
     {
-        if (threadIdx.x == 0) counts[tcode] = ((tcode & ((1 << (2 * (Tl - k))) - 1)) == 0) ? 1 : 0;
+        // a coarser leaf starts in its first tile only; a non-significant root is one leaf
+        if (threadIdx.x == 0) counts[tcode] = (k == Tl || (tcode & ((1 << (2 * (Tl - k))) - 1)) == 0) ? 1 : 0;
         return;
     }
-    // significant nodes of the subtree, levels Tl .. L-1 (1 + 4 + ... + 4^(D-1) nodes)
-    const int nodes = ((1 << (2 * D)) - 1) / 3;
+    // significant nodes of the subtree: the root plus levels Tl+1 .. L-1 (85 flag words)
     int cnt = 0;
-    for (int i = threadIdx.x; i < nodes; i += blockDim.x)
+    if (threadIdx.x < 85)
     {
-        int j = 0, base = 0;
-        while (i >= base + (1 << (2 * j))) { base += 1 << (2 * j); ++j; }
-        const int node = lvl_idx(Tl + j) + (tcode << (2 * j)) + (i - base);
-        cnt += (flags[node] & F_SIG) ? 1 : 0;
+        int j;
+        const uint32_t w = *reinterpret_cast<const uint32_t*>(flags + tile_flag_word(Tl, tcode, threadIdx.x, j));
+        cnt = __popc(w & (0x01010101u * F_SIG));
     }
-    __shared__ int s_cnt;
-    if (threadIdx.x == 0) s_cnt = 0;
-    __syncthreads();
     cnt = __reduce_add_sync(0xffffffffu, cnt);
-    if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(&s_cnt, cnt);
+    __shared__ int s_cnt[kTileThreads / 32];
+    if ((threadIdx.x & 31) == 0) s_cnt[threadIdx.x >> 5] = cnt;
     __syncthreads();
-    if (threadIdx.x == 0) counts[tcode] = 1 + 3 * s_cnt;
+    if (threadIdx.x == 0) counts[tcode] = 1 + 3 * (1 + s_cnt[0] + s_cnt[1] + s_cnt[2]);
 }
 
 // Exclusive scan of n tile counts in one block; total -> sc->n_leaves.
@@ -504,120 +561,128 @@ template <typename T> __global__ void __launch_bounds__(1024) k_tile_scan(int32_
 }
 
 // Neighbour of a leaf (level l, finest reference cell code `ref`) across the finest cell
-// (tx, ty): the ancestor of the leaf containing that cell at min(l, its level)
-// (neighbours/find_neighbours.cu:100-108). Descends from the first level where the
-// two cells' paths differ, since all shared ancestors of a leaf are significant.
-__device__ __forceinline__ void descend(const uint8_t* flags, int L, int l, int ref, int tx, int ty, int32_t& id, uint8_t& lv)
-{
-    const int tc = morton(tx, ty);
-    const int b = 31 - __clz(tc ^ ref);
-    int j = L - (b >> 1);
-    if (j < 0) j = 0;
-    while (true)
-    {
-        const int node = lvl_idx(j) + (tc >> (2 * (L - j)));
-        if (j >= l) { id = node; lv = (uint8_t)l; return; }
-        if (!(flags[node] & F_SIG)) { id = node; lv = (uint8_t)j; return; }
-        ++j;
-    }
-}
-
-// Four neighbours of a leaf (north/east from its north-east finest cell, south/west from
-// its south-west finest cell; -1 and the leaf's level at the DEM or mesh border:
-// neighbours/find_neighbours.cu:51-428, neighbours/compaction.cu:109-151).
-__device__ __forceinline__ void leaf_neighbours(const uint8_t* flags, int L, int M, int xsz, int ysz, int act, int l,
-                                                int32_t (&id)[4], uint8_t (&lv)[4])
+// (tx, ty), direction d (N, E, S, W): the ancestor of the leaf containing that cell at
+// min(l, its level) (neighbours/find_neighbours.cu:100-108); -1 and level l across the
+// DEM or mesh border (north/east from the leaf's north-east finest cell, south/west from
+// its south-west one: neighbours/find_neighbours.cu:51-428, neighbours/compaction.cu:109-151).
+// All shared ancestors of the leaf and that cell are significant, so the search starts
+// at the first level where their paths differ.
+__device__ __forceinline__ void leaf_neighbour(const uint8_t* flags, int L, int M, int xsz, int ysz, int act, int l,
+                                               int d, int32_t& id, uint8_t& lv)
 {
     const int code = act - lvl_idx(l);
     const int x = compact(code), y = compact(code >> 1);
     const int s = 1 << (L - l);
     const int x0 = x * s, y0 = y * s, xe = x0 + s - 1, ye = y0 + s - 1;
-    const int ref = morton(x0, y0);
-    // north-east cell
-    {
-        const bool northern = (ye == M - 1 || ye == ysz - 1), southern = (ye == 0);
-        const bool eastern = (xe == M - 1 || xe == xsz - 1), western = (xe == 0);
-        if (northern && !southern) { id[0] = -1; lv[0] = (uint8_t)l; }
-        else descend(flags, L, l, ref, xe, ye + 1, id[0], lv[0]);
-        if (eastern && !western) { id[1] = -1; lv[1] = (uint8_t)l; }
-        else descend(flags, L, l, ref, xe + 1, ye, id[1], lv[1]);
-    }
-    // south-west cell
-    {
-        if (y0 == 0) { id[2] = -1; lv[2] = (uint8_t)l; }
-        else descend(flags, L, l, ref, x0, y0 - 1, id[2], lv[2]);
-        if (x0 == 0) { id[3] = -1; lv[3] = (uint8_t)l; }
-        else descend(flags, L, l, ref, x0 - 1, y0, id[3], lv[3]);
-    }
+    const bool border = (d == 0) ? ((ye == M - 1 || ye == ysz - 1) && ye != 0)
+                      : (d == 1) ? ((xe == M - 1 || xe == xsz - 1) && xe != 0)
+                      : (d == 2) ? (y0 == 0) : (x0 == 0);
+    if (border) { id = -1; lv = (uint8_t)l; return; }
+    const int tx = (d == 0) ? xe : (d == 1) ? xe + 1 : (d == 2) ? x0 : x0 - 1;
+    const int ty = (d == 0) ? ye + 1 : (d == 1) ? ye : (d == 2) ? y0 - 1 : y0;
+    const int tc = morton(tx, ty);
+    const int b = 31 - __clz(tc ^ morton(x0, y0));
+    const int j0 = max(0, L - (b >> 1));
+    const int m = first_nonsig_level(flags, L, tc, j0, l);
+    id = lvl_idx(m) + (tc >> (2 * (L - m)));
+    lv = (uint8_t)m;
 }
 
-template <typename T>
-__device__ __forceinline__ void emit_leaf(const Leaves<T>& lf, const uint8_t* flags, int L, int M, int xsz, int ysz,
-                                          int pos, int act, int l)
+// Level of the leaf containing finest cell (tx, ty), searching from the first level where
+// its path leaves that of `ref` (a cell of a tile whose root is significant, so every
+// shared ancestor is significant).
+__device__ __forceinline__ int cell_leaf_level(const uint8_t* flags, int L, int ref, int tx, int ty)
 {
-    lf.act[pos] = act;
-    lf.lvl[pos] = (uint8_t)l;
-    int32_t id[4];
-    uint8_t lv[4];
-    leaf_neighbours(flags, L, M, xsz, ysz, act, l, id, lv);
-#pragma unroll
-    for (int d = 0; d < 4; ++d) { lf.nb[d][pos] = id[d]; lf.nbl[d][pos] = lv[d]; }
+    const int tc = morton(tx, ty);
+    const int b = 31 - __clz(tc ^ ref);
+    return first_nonsig_level(flags, L, tc, max(0, L - (b >> 1)), L);
+}
+
+// A tile holding one leaf (the tile's root or the first tile of a coarser leaf): threads
+// 0..3 of the block find one neighbour each.
+template <typename T>
+__device__ __forceinline__ void emit_single_leaf(const Leaves<T>& lf, const uint8_t* flags, int L, int M, int xsz,
+                                                 int ysz, int pos, int act, int l)
+{
+    const int d = threadIdx.x;
+    if (d >= 4) return;
+    if (d == 0) { lf.act[pos] = act; lf.lvl[pos] = (uint8_t)l; }
+    int32_t id;
+    uint8_t lv;
+    leaf_neighbour(flags, L, M, xsz, ysz, act, l, d, id, lv);
+    lf.nb[d][pos] = id;
+    lf.nbl[d][pos] = lv;
 }
 
 // Leaves of one tile in Z order with their neighbours. The tile's subtree flags are
 // copied to shared memory; every finest cell of the tile gets the level of the leaf that
-// contains it (walk down the shared flags); leaf starts are ranked with popcounts; then
-// thread r writes the leaf of rank r (coalesced), looking its neighbours up in the
-// per-cell level map when the neighbouring cell lies in the tile and descending the
-// global flags otherwise.
+// contains it, and so does the ring of cells just outside the tile (searches in the
+// global flags); leaf starts are ranked with popcounts; then thread r writes the leaf of
+// rank r (coalesced): the neighbour across a face is the ancestor of the neighbouring
+// finest cell at min(own level, that cell's leaf level) (neighbours/find_neighbours.cu:
+// 100-108), -1 across the DEM or mesh border (neighbours/find_neighbours.cu:51-428).
+// Neighbouring cells are found by dilated-integer steps on the leaf's Morton code.
 template <typename T>
 __global__ void __launch_bounds__(kTileThreads) k_tile_emit(Leaves<T> lf, const uint8_t* flags, const int32_t* offsets,
-                                                            int L, int D, int M, int xsz, int ysz)
+                                                            int L, int M, int xsz, int ysz)
 {
+    constexpr int D = kTileDepth, kCells = 1 << (2 * D);
     const int Tl = L - D;
     const int tcode = blockIdx.x;
     const int off = offsets[tcode];
-    __shared__ int s_k, s_total;
-    __shared__ uint8_t sflag[344];      // flags of levels Tl .. L-1 below the tile root (<= 341)
-    __shared__ uint8_t cell_lvl[1024];  // leaf level of each finest cell, tile-local Morton order
-    __shared__ uint16_t start_of[1024]; // tile-local start cell of the leaf of each rank
-    __shared__ uint32_t bits[32];       // leaf starts
-    __shared__ int32_t prefix[32];
-    if (threadIdx.x == 0) s_k = tile_leaf_level(flags, Tl, tcode);
-    if (threadIdx.x < 32) bits[threadIdx.x] = 0;
-    __syncthreads();
-    const int k = s_k;
+    // subtree flags at lvl_idx(j) + local index (j = 1..4); lvl_idx(D) bytes
+    __shared__ __align__(4) uint8_t sflag[((1 << (2 * D)) - 1) / 3 + 3];
+    __shared__ uint8_t cell_lvl[kCells];              // leaf level of each finest cell, tile-local Morton order
+    __shared__ uint16_t start_of[kCells];             // tile-local start cell of the leaf of each rank
+    __shared__ uint32_t bits[kCells / 32];            // leaf starts
+    __shared__ int32_t prefix[kCells / 32];
+    __shared__ int s_total;
+    // leaf levels of the cells just outside the tile (N, E, S, W), indexed by the dilated
+    // tile-local coordinate along the side (x bits for N/S, y bits shifted down for E/W)
+    __shared__ uint8_t halo[4][(kXBits & (kCells - 1)) + 1];
+    const int k = tile_leaf_level_warp(flags, Tl + 1, tcode << 2);  // levels 0..Tl, every warp
     if (k < Tl)
     {
-        if (threadIdx.x == 0 && (tcode & ((1 << (2 * (Tl - k))) - 1)) == 0)
-            emit_leaf(lf, flags, L, M, xsz, ysz, off, lvl_idx(k) + (tcode >> (2 * (Tl - k))), k);
+        if ((tcode & ((1 << (2 * (Tl - k))) - 1)) == 0)
+            emit_single_leaf(lf, flags, L, M, xsz, ysz, off, lvl_idx(k) + (tcode >> (2 * (Tl - k))), k);
         return;
     }
-    const int root = lvl_idx(Tl) + tcode;
-    if (!(flags[root] & F_SIG))
+    if (k == Tl)
     {
-        if (threadIdx.x == 0) emit_leaf(lf, flags, L, M, xsz, ysz, off, root, Tl);
+        emit_single_leaf(lf, flags, L, M, xsz, ysz, off, lvl_idx(Tl) + tcode, Tl);
         return;
     }
-    const int nodes = ((1 << (2 * D)) - 1) / 3;
-    for (int i = threadIdx.x; i < nodes; i += blockDim.x)
+    if (threadIdx.x < 85)
     {
-        int j = 0, base = 0;
-        while (i >= base + (1 << (2 * j))) { base += 1 << (2 * j); ++j; }
-        sflag[i] = flags[lvl_idx(Tl + j) + (tcode << (2 * j)) + (i - base)] & F_SIG;
+        int j;
+        const int g = tile_flag_word(Tl, tcode, threadIdx.x, j);
+        const int local = g - lvl_idx(Tl + j) - (tcode << (2 * j));
+        *reinterpret_cast<uint32_t*>(sflag + lvl_idx(j) + local) =
+            *reinterpret_cast<const uint32_t*>(flags + g) & (0x01010101u * F_SIG);
+    }
+    const unsigned tbase = (unsigned)tcode << (2 * D);   // finest Morton code of the tile's first cell
+    const int tw = 1 << D;
+    if (threadIdx.x < 4 * tw)
+    {
+        const int side = threadIdx.x / tw, i = threadIdx.x % tw;
+        const int tx0 = compact((int)tbase), ty0 = compact((int)(tbase >> 1));
+        const int hx = (side == 0 || side == 2) ? tx0 + i : (side == 1 ? tx0 + tw : tx0 - 1);
+        const int hy = (side == 1 || side == 3) ? ty0 + i : (side == 0 ? ty0 + tw : ty0 - 1);
+        halo[side][dilate(i)] =
+            (hx >= 0 && hx < M && hy >= 0 && hy < M) ? (uint8_t)cell_leaf_level(flags, L, (int)tbase, hx, hy) : 0;
     }
     __syncthreads();
-    const int ncell = 1 << (2 * D);
-    for (int c = threadIdx.x; c < ncell; c += blockDim.x)
+    // leaf level of every cell: the first level below the (significant) root whose node
+    // on the cell's path is not significant
+    for (int c = threadIdx.x; c < kCells; c += blockDim.x)
     {
-        int lev = L, base = 0;
-        for (int j = 0; j < D; ++j)
-        {
-            if (!sflag[base + (c >> (2 * (D - j)))]) { lev = Tl + j; break; }
-            base += 1 << (2 * j);
-        }
+        int lev = L;
+#pragma unroll
+        for (int j = D - 1; j >= 1; --j)
+            if (!sflag[lvl_idx(j) + (c >> (2 * (D - j)))]) lev = Tl + j;
         cell_lvl[c] = (uint8_t)lev;
-        if ((c & ((1 << (2 * (L - lev))) - 1)) == 0) atomicOr(&bits[c >> 5], 1u << (c & 31));
+        const unsigned start = __ballot_sync(0xffffffffu, (c & ((1 << (2 * (L - lev))) - 1)) == 0);
+        if ((threadIdx.x & 31) == 0) bits[c >> 5] = start;
     }
     __syncthreads();
     if (threadIdx.x < 32)
@@ -633,7 +698,7 @@ __global__ void __launch_bounds__(kTileThreads) k_tile_emit(Leaves<T> lf, const 
         if (threadIdx.x == 31) s_total = incl;
     }
     __syncthreads();
-    for (int c = threadIdx.x; c < ncell; c += blockDim.x)
+    for (int c = threadIdx.x; c < kCells; c += blockDim.x)
     {
         const int w = c >> 5;
         const uint32_t b = bits[w];
@@ -641,44 +706,45 @@ __global__ void __launch_bounds__(kTileThreads) k_tile_emit(Leaves<T> lf, const 
     }
     __syncthreads();
     const int total = s_total;
-    const int tbase = tcode << (2 * D);              // finest Morton code of the tile's first cell
-    const int tx0 = compact(tbase), ty0 = compact(tbase >> 1), tw = 1 << D;
+    const unsigned lmask = kCells - 1;
+    // dilated coordinates of the mesh's last row/column and of the DEM's
+    const unsigned mesh_x = kXBits & ((1u << (2 * L)) - 1u), mesh_y = mesh_x << 1;
+    const unsigned dem_x = (unsigned)dilate(xsz - 1), dem_y = (unsigned)dilate(ysz - 1) << 1;
     for (int r = threadIdx.x; r < total; r += blockDim.x)
     {
         const int c = start_of[r];
         const int lev = cell_lvl[c];
-        const int gc = tbase + c;                     // finest code of the leaf's south-west cell
+        const int sh = 2 * (L - lev);
+        const unsigned gc = tbase + (unsigned)c;       // finest code of the leaf's south-west cell
         const int pos = off + r;
-        lf.act[pos] = lvl_idx(lev) + (gc >> (2 * (L - lev)));
+        lf.act[pos] = lvl_idx(lev) + (int)(gc >> sh);
         lf.lvl[pos] = (uint8_t)lev;
-        const int s = 1 << (L - lev);
-        const int x0 = compact(gc), y0 = compact(gc >> 1), xe = x0 + s - 1, ye = y0 + s - 1;
-        int32_t id[4];
-        uint8_t lv[4];
-        // target finest cell of each direction, -1 border rule of neighbours/find_neighbours.cu
-        const bool nb_border[4] = {(ye == M - 1 || ye == ysz - 1) && ye != 0, (xe == M - 1 || xe == xsz - 1) && xe != 0,
-                                   y0 == 0, x0 == 0};
-        const int txs[4] = {xe, xe + 1, x0, x0 - 1};
-        const int tys[4] = {ye + 1, ye, y0 - 1, y0};
+        const unsigned X0 = gc & kXBits, Y0 = gc & kYBits;            // dilated x0, y0
+        const unsigned span = (1u << sh) - 1u;                         // dilated (size - 1) in both
+        const unsigned Xe = X0 | (span & kXBits), Ye = Y0 | (span & kYBits);
+        // target finest cell per direction: N (xe, ye+1), E (xe+1, ye), S (x0, y0-1), W (x0-1, y0)
+        const bool border[4] = {(Ye == mesh_y || Ye == dem_y) && Ye != 0, (Xe == mesh_x || Xe == dem_x) && Xe != 0,
+                                Y0 == 0, X0 == 0};
+        const unsigned tc[4] = {Xe | dil_add(Ye, 2u, kYBits), dil_add(Xe, 1u, kXBits) | Ye, X0 | dil_sub(Y0, 2u, kYBits),
+                                dil_sub(X0, 1u, kXBits) | Y0};
 #pragma unroll
         for (int d = 0; d < 4; ++d)
         {
-            if (nb_border[d]) { id[d] = -1; lv[d] = (uint8_t)lev; continue; }
-            const int tx = txs[d], ty = tys[d];
-            if (tx >= tx0 && tx < tx0 + tw && ty >= ty0 && ty < ty0 + tw)
+            int32_t id = -1;
+            int lv = lev;
+            if (!border[d])
             {
-                const int lt = cell_lvl[morton(tx - tx0, ty - ty0)];
-                const int m = lev < lt ? lev : lt;
-                id[d] = lvl_idx(m) + (morton(tx, ty) >> (2 * (L - m)));
-                lv[d] = (uint8_t)m;
+                const unsigned t = tc[d];
+                int lt;
+                if ((t >> (2 * D)) == (unsigned)tcode) lt = cell_lvl[t & lmask];
+                else if (d == 0 || d == 2) lt = halo[d][t & lmask & kXBits];
+                else lt = halo[d][(t & lmask & kYBits) >> 1];
+                lv = lev < lt ? lev : lt;
+                id = lvl_idx(lv) + (int)(t >> (2 * (L - lv)));
             }
-            else
-            {
-                descend(flags, L, lev, gc, tx, ty, id[d], lv[d]);
-            }
+            lf.nb[d][pos] = id;
+            lf.nbl[d][pos] = (uint8_t)lv;
         }
-#pragma unroll
-        for (int d = 0; d < 4; ++d) { lf.nb[d][pos] = id[d]; lf.nbl[d][pos] = lv[d]; }
     }
 }
 

@@ -76,6 +76,9 @@ extern "C" mwdg2_status mwdg2_leaf_topology_static(const uint8_t* d_sig, int max
     if (max_ref_lvl < mw::kTileDepth || max_ref_lvl > kStaticMaxLevel)
         return fail(MWDG2_ERR_ARG, "mwdg2_leaf_topology_static: max_ref_lvl must be between 5 and 13 "
                                    "(the static scratch holds 65536 tile counts)");
+    // the kernels read the flags four at a time
+    if (reinterpret_cast<uintptr_t>(d_sig) % 4 != 0)
+        return fail(MWDG2_ERR_ARG, "mwdg2_leaf_topology_static: d_sig must be 4-byte aligned");
     const int M = 1 << max_ref_lvl;
     if (xsz < 1 || ysz < 1 || xsz > M || ysz > M)
         return fail(MWDG2_ERR_ARG, "mwdg2_leaf_topology_static: xsz and ysz must be within 1..2^max_ref_lvl");
@@ -89,7 +92,7 @@ extern "C" mwdg2_status mwdg2_leaf_topology_static(const uint8_t* d_sig, int max
     const int ntiles = 1 << (2 * (max_ref_lvl - D));
     // Every tile count and the total are written before they are read, so nothing in the
     // scratch has to start at zero.
-    mw::k_tile_count<<<ntiles, mw::kTileThreads, 0, st>>>(d_sig, max_ref_lvl, D, scratch->tile_counts);
+    mw::k_tile_count<<<ntiles, mw::kTileThreads, 0, st>>>(d_sig, max_ref_lvl, scratch->tile_counts);
     mw::k_tile_scan<float><<<1, 1024, 0, st>>>(scratch->tile_counts, ntiles, &scratch->scalars);
     mw::Leaves<float> lf{};
     lf.act = d_act;
@@ -99,8 +102,8 @@ extern "C" mwdg2_status mwdg2_leaf_topology_static(const uint8_t* d_sig, int max
         lf.nb[d] = d_nb_ids + (size_t)d * cap;
         lf.nbl[d] = d_nb_levels + (size_t)d * cap;
     }
-    mw::k_tile_emit<float><<<ntiles, mw::kTileThreads, 0, st>>>(lf, d_sig, scratch->tile_counts, max_ref_lvl, D, M,
-                                                                xsz, ysz);
+    mw::k_tile_emit<float><<<ntiles, mw::kTileThreads, 0, st>>>(lf, d_sig, scratch->tile_counts, max_ref_lvl, M, xsz,
+                                                                ysz);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(MWDG2_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
     int32_t n = 0;

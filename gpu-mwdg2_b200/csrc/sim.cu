@@ -3,7 +3,11 @@
 // Host loop per step (mirrors source/run_simulation.cu:226-774 step by step):
 //   time update -> maxima + re-insertion -> point sources -> [encode+threshold+regularise
 //   -> decode+extra significance -> leaf topology] -> MWDG2 stage 1 -> re-insert ->
-//   scale re-encode -> stage 2 (or HWFV1 update) -> one 64-byte read-back (dt, leaves).
+//   scale re-encode -> stage 2 (or HWFV1 update) -> one small read-back (dt, leaves).
+// MWDG2 folds both re-insertions into the RK stages: stage 1 writes U* straight into a
+// second (stage) hierarchy, stage 2 writes U^{n+1} into the hierarchy and reduces the
+// maxima the next step starts from, so after the first step the step begins with the
+// point sources.
 // All per-step state stays on the device; the only host<->device traffic per step is the
 // point-source values (when there are sources) and the scalar read-back.
 #include "../../include/mwdg2.h"
@@ -86,10 +90,13 @@ private:
     cudaStream_t st_ = nullptr;
     std::vector<void*> allocs_;
     mw::Hier<T> hr_{};
+    mw::Hier<T> hs_{};                  // MWDG2 stage hierarchy (U*), bed and flags shared with hr_
     mw::Leaves<T> lf_{};
     mw::Scalars<T>* sc_ = nullptr;      // device
     mw::Scalars<T>* sc_host_ = nullptr; // pinned
     int32_t* tile_counts_ = nullptr;
+    int32_t* wet_list_ = nullptr;       // leaves that are not dry in an RK stage
+    int64_t wet_prev_[2] = {-1, -1};    // previous step's wet-leaf count per RK stage
     mw::Src<T>* d_src_ = nullptr;
     mw::Src<T>* h_src_ = nullptr;       // pinned
     int32_t* d_stage_codes_ = nullptr;
@@ -100,7 +107,7 @@ private:
     bool timed_ = false;
     cudaEvent_t ev_[9] = {};
     double last_ms_[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    int64_t last_cnt_[6] = {0, 0, 0, 0, 0, 0};
+    int64_t last_cnt_[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     int launches_ = 0;
     // outputs
     std::chrono::steady_clock::time_point t_start_;
@@ -117,6 +124,28 @@ private:
     }
     void release();
     mwdg2_status launch_step();
+    // One MWDG2 RK stage. When fewer than half of the leaves were wet in this stage last
+    // step, a light pass finishes the dry leaves and lists the others for the full kernel
+    // (whose grid is sized from last step's wet count); otherwise one sweep over all leaves.
+    template <int STAGE>
+    void stage(const mw::Hier<T>& hin, const mw::Hier<T>& hout, const mw::Bnd<T>& B, bool fric, int g_leaf, int g_solver)
+    {
+        const int64_t w = wet_prev_[STAGE - 1];
+        if (w >= 0 && 2 * w < n_leaves_)
+        {
+            mw::k_stage_classify<T, STAGE><<<g_leaf, 256, 0, st_>>>(lf_, hin, hout, sc_, P_, B, dt_, fric, wet_list_);
+            const int64_t hint = std::min<int64_t>(F_, w + w / 4 + 4096);
+            mw::k_mwdg2_stage<T, STAGE, true><<<grid_for(hint, mw::kSolverThreads, 1 << 20), mw::kSolverThreads, 0,
+                                                st_>>>(lf_, hin, hout, sc_, P_, B, dt_, fric, wet_list_);
+            launches_ += 2;
+        }
+        else
+        {
+            mw::k_mwdg2_stage<T, STAGE, false><<<g_solver, mw::kSolverThreads, 0, st_>>>(lf_, hin, hout, sc_, P_, B, dt_,
+                                                                                         fric, nullptr);
+            launches_ += 1;
+        }
+    }
     mwdg2_status write_outputs(bool first);
     mwdg2_status sample_stage(std::vector<T>& vals);
     mw::Bnd<T> bnd_now() const;
@@ -177,22 +206,18 @@ template <typename T> mwdg2_status Sim<T>::init(const char* par, const mwdg2_opt
     solver_blocks_ = sms * 8;
     red_blocks_ = sms * 4;
 
-    // hierarchy, details, flags
+    // hierarchy, stage hierarchy, flags
     const int modes = mw_ ? 3 : 1;
     for (int f = 0; f < 4; ++f)
         for (int m = 0; m < 3; ++m)
         {
-            hr_.s[f][m] = nullptr;
+            hr_.s[f][m] = hs_.s[f][m] = nullptr;
             if (m < modes) { mwdg2_status s = dalloc(hr_.s[f][m], n_all_); if (s) return s; }
+            if (mw_ && f < 3) { mwdg2_status s = dalloc(hs_.s[f][m], n_all_); if (s) return s; }
         }
-    for (int f = 0; f < 3; ++f)
-        for (int k = 0; k < 9; ++k)
-        {
-            hr_.det[f][k] = nullptr;
-            if (mw_ || k % 3 == 0) { mwdg2_status s = dalloc(hr_.det[f][k], n_det_); if (s) return s; }
-        }
-    if (mwdg2_status s = dalloc(hr_.norm, n_det_)) return s;
     if (mwdg2_status s = dalloc(hr_.flags, n_det_)) return s;
+    for (int m = 0; m < 3; ++m) hs_.s[3][m] = hr_.s[3][m];
+    hs_.flags = hr_.flags;
     // leaves (capacity: every finest cell)
     if (mwdg2_status s = dalloc(lf_.act, F_)) return s;
     if (mwdg2_status s = dalloc(lf_.lvl, F_)) return s;
@@ -203,15 +228,12 @@ template <typename T> mwdg2_status Sim<T>::init(const char* par, const mwdg2_opt
     }
     for (int k = 0; k < 9; ++k)
     {
-        lf_.un[k] = lf_.us[k] = nullptr;
-        if (mw_ || k % 3 == 0)
-        {
-            if (mwdg2_status s = dalloc(lf_.un[k], F_)) return s;
-            if (mw_) { if (mwdg2_status s = dalloc(lf_.us[k], F_)) return s; }
-        }
+        lf_.un[k] = nullptr;
+        if (mw_ || k % 3 == 0) { if (mwdg2_status s = dalloc(lf_.un[k], F_)) return s; }
     }
     if (mwdg2_status s = dalloc(sc_, 1)) return s;
     if (mwdg2_status s = dalloc(tile_counts_, ntiles_)) return s;
+    if (mw_) { if (mwdg2_status s = dalloc(wet_list_, F_)) return s; }
     CU(cudaMallocHost(&sc_host_, sizeof(mw::Scalars<T>)));
     const int nsrc = (int)cs_.srcs.size();
     if (nsrc > 0)
@@ -269,7 +291,7 @@ template <typename T> mwdg2_status Sim<T>::init(const char* par, const mwdg2_opt
     mw::k_init_leaves<T><<<grid_for(F_, 256, 4096), 256, 0, st_>>>(lf_, L_, (int)F_);
     // maxima of the initial state (run_simulation.cu:190) then bed encoding with preflags
     // (mra/preflag_topo.cu:3-43)
-    mw::k_step_begin<T><<<1, 1, 0, st_>>>(sc_);
+    mw::k_step_begin<T><<<1, 1, 0, st_>>>(sc_, false);
     if (mw_) mw::k_maxes_reinsert<T, true><<<red_blocks_, 256, 0, st_>>>(lf_, hr_, sc_, (int)F_, false);
     else mw::k_maxes_reinsert<T, false><<<red_blocks_, 256, 0, st_>>>(lf_, hr_, sc_, (int)F_, false);
     for (int level = L_ - 1; level >= 0; --level)
@@ -299,7 +321,10 @@ template <typename T> mwdg2_status Sim<T>::launch_step()
     auto rec = [&](int k) { if (timed_) cudaEventRecord(ev_[k], st_); };
     launches_ = 0;
     rec(0);
-    mw::k_step_begin<T><<<1, 1, 0, st_>>>(sc_);
+    // MWDG2 after its first step: the previous step's stage 2 re-inserted the state into
+    // the hierarchy and reduced its maxima, so only the point sources remain here
+    const bool carry = mw && !first_;
+    mw::k_step_begin<T><<<1, 1, 0, st_>>>(sc_, carry);
     ++launches_;
     const int nfix = first_ ? (int)F_ : -1;
     // leaf count before remeshing is known exactly; after remeshing it is near the previous
@@ -308,7 +333,7 @@ template <typename T> mwdg2_status Sim<T>::launch_step()
     const int64_t n_hint = std::min<int64_t>(F_, (int64_t)n_leaves_ + n_leaves_ / 4 + 1024);
     const int g_leaf = grid_for(n_hint, 256, 1 << 20);
     const int g_solver = grid_for(n_hint, mw::kSolverThreads, 1 << 20);
-    if (mw) { mw::k_maxes_reinsert<T, true><<<g_prev, 256, 0, st_>>>(lf_, hr_, sc_, nfix, !first_); ++launches_; }
+    if (mw) { if (!carry) { mw::k_maxes_reinsert<T, true><<<g_prev, 256, 0, st_>>>(lf_, hr_, sc_, nfix, false); ++launches_; } }
     else { mw::k_maxes_reinsert<T, false><<<g_prev, 256, 0, st_>>>(lf_, hr_, sc_, nfix, !first_); ++launches_; }
     // point sources (classes/PointSources.h:453-472 on the host, then the kernel)
     const int nsrc = (int)cs_.srcs.size();
@@ -353,11 +378,11 @@ template <typename T> mwdg2_status Sim<T>::launch_step()
     rec(3);
     if (remesh)
     {
-        mw::k_tile_count<<<ntiles_, mw::kTileThreads, 0, st_>>>(hr_.flags, L_, D_, tile_counts_);
+        mw::k_tile_count<<<ntiles_, mw::kTileThreads, 0, st_>>>(hr_.flags, L_, tile_counts_);
         ++launches_;
         mw::k_tile_scan<T><<<1, 1024, 0, st_>>>(tile_counts_, ntiles_, sc_);
         ++launches_;
-        mw::k_tile_emit<T><<<ntiles_, mw::kTileThreads, 0, st_>>>(lf_, hr_.flags, tile_counts_, L_, D_, M_, cs_.xsz, cs_.ysz);
+        mw::k_tile_emit<T><<<ntiles_, mw::kTileThreads, 0, st_>>>(lf_, hr_.flags, tile_counts_, L_, M_, cs_.xsz, cs_.ysz);
         ++launches_;
     }
     rec(4);
@@ -376,26 +401,22 @@ template <typename T> mwdg2_status Sim<T>::launch_step()
     }
     else
     {
-        mw::k_mwdg2_stage<T, 1><<<g_solver, mw::kSolverThreads, 0, st_>>>(lf_, hr_, sc_, P_, B, dt_, fric);
-        ++launches_;
+        stage<1>(hr_, hs_, B, fric, g_leaf, g_solver);
         rec(5);
-        mw::k_reinsert_us<T><<<g_leaf, 256, 0, st_>>>(lf_, hr_, sc_);
-        ++launches_;
         if (eps > T(0))
         {
             for (int level = L_ - 1; level > top; --level)
             {
                 const int nb = grid_for((int64_t)1 << (2 * level), 256, 1 << 24);
-                mw::k_encode_level<T, true, false><<<nb, 256, 0, st_>>>(hr_, sc_, L_, level, eps);
+                mw::k_encode_level<T, true, false><<<nb, 256, 0, st_>>>(hs_, sc_, L_, level, eps);
                 ++launches_;
             }
-            mw::k_encode_top<T, true, false><<<1, 256, 0, st_>>>(hr_, sc_, L_, top, eps);
+            mw::k_encode_top<T, true, false><<<1, 256, 0, st_>>>(hs_, sc_, L_, top, eps);
             ++launches_;
         }
-        if (cs_.limitslopes) { mw::k_stage2_maxh<T><<<g_leaf, 256, 0, st_>>>(lf_, hr_, sc_, P_, B, dt_); ++launches_; }
+        if (cs_.limitslopes) { mw::k_stage2_maxh<T><<<g_leaf, 256, 0, st_>>>(lf_, hs_, sc_, P_, B, dt_); ++launches_; }
         rec(6);
-        mw::k_mwdg2_stage<T, 2><<<g_solver, mw::kSolverThreads, 0, st_>>>(lf_, hr_, sc_, P_, B, dt_, false);
-        ++launches_;
+        stage<2>(hs_, hr_, B, false, g_leaf, g_solver);
         rec(7);
     }
     CU(cudaGetLastError());
@@ -412,12 +433,16 @@ template <typename T> mwdg2_status Sim<T>::launch_step()
             last_ms_[k] = ms;
         }
     }
+    if (mw)
+        for (int s = 0; s < 2; ++s) wet_prev_[s] = sc_host_->wet[s];
     last_cnt_[0] = (int64_t)sc_host_->enc;
     last_cnt_[1] = (int64_t)sc_host_->enc2;
     last_cnt_[2] = (int64_t)sc_host_->dec;
     last_cnt_[3] = sc_host_->n_leaves;
     last_cnt_[4] = n_det_ - 3;
     last_cnt_[5] = launches_;
+    last_cnt_[6] = mw ? sc_host_->wet[0] : 0;
+    last_cnt_[7] = mw ? sc_host_->wet[1] : 0;
     return MWDG2_OK;
 }
 
@@ -672,7 +697,7 @@ template <typename T> mwdg2_status Sim<T>::timing(double* out, int n)
 
 template <typename T> mwdg2_status Sim<T>::counters(int64_t* out, int n)
 {
-    for (int i = 0; i < n && i < 6; ++i) out[i] = last_cnt_[i];
+    for (int i = 0; i < n && i < 8; ++i) out[i] = last_cnt_[i];
     return MWDG2_OK;
 }
 

@@ -242,19 +242,154 @@ __device__ __forceinline__ void dg2_rhs_update(const P3<T>& ch, const P3<T>& cqx
     out[8] = cqy._1y + dt * (zero + Ly1.qy);
 }
 
-// One RK2 stage of MWDG2 for every leaf. STAGE 1: friction (once per step), limiter with
-// the step's max depth, U* -> us, U^n (after friction and limiter) -> un.
-// STAGE 2: limiter with the stage's max depth, U^{n+1} = (U** + U^n)/2 -> un, CFL dt.
+// Depth after ghost cells of the own leaf and its four neighbours; a leaf is dry when all
+// five are below tol_h: it is not updated (dg2_update.cu:36-50), not limited (the limiter
+// needs a depth above 0.05 max_h) and, being below tol_h, gets no friction, so it needs
+// none of its neighbours' other coefficients.
+template <typename T>
+__device__ __forceinline__ bool leaf_is_dry(const Hier<T>& hr, T own_h0, const int32_t (&nid)[4], const T (&gh)[4], T tol_h)
+{
+    if (!(own_h0 < tol_h)) return false;
+#pragma unroll
+    for (int d = 0; d < 4; ++d)
+    {
+        const T h = (nid[d] != -1) ? hr.s[0][0][nid[d]] - hr.s[3][0][nid[d]] : gh[d];
+        if (!(h < tol_h)) return false;
+    }
+    return true;
+}
+
+// Leaf state u (h, qx, qy by mode, the layout of Leaves::un) into the hierarchy at `a`,
+// depths as surface elevations eta = h + z (mra/reinsert_assem_sol.cu:3-32).
+template <typename T>
+__device__ __forceinline__ void put_leaf(const Hier<T>& hr, int a, const T (&u)[9], const T (&z)[3])
+{
+#pragma unroll
+    for (int m = 0; m < 3; ++m)
+    {
+        hr.s[0][m][a] = u[m] + z[m];
+        hr.s[1][m][a] = u[3 + m];
+        hr.s[2][m][a] = u[6 + m];
+    }
+}
+
+// Running maxima of the state at the end of a step, as the next step's
+// mra/get_max_scale_coeffs.cu:3-27 reads them (|eta|, |h0|, |qx0|, |z0|; the reference
+// also uses qx0 for the qy maximum).
+template <typename T> struct StateMax
+{
+    T eta = T(0), h = T(0), qx = T(0), z = T(0);
+    __device__ __forceinline__ void add(const T (&u)[9], T z0)
+    {
+        const T e = u[0] + z0;
+        eta = fmax(eta, fabs(e));
+        h = fmax(h, fabs(u[0]));
+        qx = fmax(qx, fabs(u[3]));
+        z = fmax(z, fabs(z0));
+    }
+    __device__ __forceinline__ void flush(Scalars<T>* sc)
+    {
+        T v[4] = {eta, h, qx, z};
+        T* const dst[4] = {&sc->next_max[0], &sc->next_max[1], &sc->next_max[2], &sc->next_max[3]};
+        block_max_atomic<T, 4>(v, dst);
+    }
+};
+
+// Wet-list construction for one RK stage: dry leaves are finished here, the others are
+// appended to `wet` for k_mwdg2_stage<.., LIST=true>. Stage 1 gives a dry leaf's state,
+// with the discharge cleared by friction, to U^n (un) and to the stage hierarchy `hout`;
+// stage 2 leaves it unchanged and re-inserts U^n into the hierarchy `hout`.
 template <typename T, int STAGE>
-__global__ void __launch_bounds__(kSolverThreads) k_mwdg2_stage(Leaves<T> lf, Hier<T> hr, Scalars<T>* sc, Params<T> P,
-                                                                Bnd<T> B, T dt, bool friction)
+__global__ void __launch_bounds__(256) k_stage_classify(Leaves<T> lf, Hier<T> hin, Hier<T> hout, Scalars<T>* sc,
+                                                        Params<T> P, Bnd<T> B, T dt, bool friction, int32_t* wet)
 {
     const int n = sc->n_leaves;
+    bool any_dry = false;
+    StateMax<T> mx;
+    for (int i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x)
+    {
+        const int i = i0 + threadIdx.x;
+        bool is_wet = false;
+        if (i < n)
+        {
+            const int a = lf.act[i];
+            const int level = lf.lvl[i];
+            int32_t nid[4];
+#pragma unroll
+            for (int d = 0; d < 4; ++d) nid[d] = lf.nb[d][i];
+            T h0 = hin.s[0][0][a] - hin.s[3][0][a];
+            T qx0 = hin.s[1][0][a], qy0 = hin.s[2][0][a];
+            const T z0 = hin.s[3][0][a];
+            T gh[4], gqx[4], gqy[4];
+            ghost_pass(h0, qx0, qy0, z0, nid, level, a, P, B, dt, gh, gqx, gqy);
+            is_wet = !leaf_is_dry(hin, h0, nid, gh, P.tol_h);
+            any_dry |= !is_wet;
+            if (!is_wet)
+            {
+                const T z[3] = {z0, hin.s[3][1][a], hin.s[3][2][a]};
+                T u[9];
+                if (STAGE == 1)
+                {
+                    if (friction) { qx0 = T(0.0); qy0 = T(0.0); }
+                    u[0] = h0; u[3] = qx0; u[6] = qy0;
+#pragma unroll
+                    for (int m = 1; m < 3; ++m)
+                    {
+                        u[m] = hin.s[0][m][a] - z[m];
+                        u[3 + m] = hin.s[1][m][a];
+                        u[6 + m] = hin.s[2][m][a];
+                    }
+#pragma unroll
+                    for (int k = 0; k < 9; ++k) lf.un[k][i] = u[k];
+                }
+                else
+                {
+#pragma unroll
+                    for (int k = 0; k < 9; ++k) u[k] = lf.un[k][i];
+                    mx.add(u, z0);
+                }
+                put_leaf(hout, a, u, z);
+            }
+        }
+        // warp-aggregated append
+        const unsigned mask = __ballot_sync(0xffffffffu, is_wet);
+        const int lane = threadIdx.x & 31;
+        int base = 0;
+        if (lane == 0 && mask) base = atomicAdd(&sc->wet[STAGE - 1], __popc(mask));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (is_wet) wet[base + __popc(mask & ((1u << lane) - 1u))] = i;
+    }
+    if (STAGE == 2)
+    {
+        mx.flush(sc);
+        // dry leaves report initial_tstep as their CFL step (dg2_update.cu:61)
+        if (__syncthreads_or(any_dry) && threadIdx.x == 0) atomic_min_nn(&sc->dt_min, P.initial_tstep);
+    }
+}
+
+// One RK2 stage of MWDG2, reading the hierarchy `hin` and writing each leaf's result into
+// the hierarchy `hout` at the leaf's own index (which no leaf reads in this stage).
+// STAGE 1 (hin: hierarchy, hout: stage hierarchy): friction (once per step), limiter with
+// the step's max depth, U* -> hout, U^n (after friction and limiter) -> un.
+// STAGE 2 (hin: stage hierarchy, hout: hierarchy): limiter with the stage's max depth,
+// U^{n+1} = (U** + U^n)/2 -> un and hout (the next step's re-insertion,
+// mra/reinsert_assem_sol.cu), the next step's maxima, CFL dt. LIST: only the leaves in
+// the wet list built by k_stage_classify; otherwise every leaf.
+template <typename T, int STAGE, bool LIST>
+__global__ void __launch_bounds__(kSolverThreads) k_mwdg2_stage(Leaves<T> lf, Hier<T> hin, Hier<T> hout, Scalars<T>* sc,
+                                                                Params<T> P, Bnd<T> B, T dt, bool friction,
+                                                                const int32_t* wet)
+{
+    const Hier<T>& hr = hin;
+    StateMax<T> mx;
+    const int n = LIST ? sc->wet[STAGE - 1] : sc->n_leaves;
     T dt_loc = (sizeof(T) == 8) ? T(1.0e308) : T(3.0e38);
     bool nan_seen = false;
+    unsigned n_wet = 0;
     const T max_h = (STAGE == 1) ? fmax(T(1.0), sc->max_h) : sc->max_h2;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
     {
+        const int i = LIST ? wet[k] : k;
         const int a = lf.act[i];
         const int level = lf.lvl[i];
         int32_t nid[4];
@@ -269,11 +404,8 @@ __global__ void __launch_bounds__(kSolverThreads) k_mwdg2_stage(Leaves<T> lf, Hi
         // neighbour depths are all below tol_h is not updated (dg2_update.cu:36-50), is not
         // limited (the limiter needs a depth above 0.05 max_h) and, being below tol_h, gets
         // no friction: it needs none of the neighbours' other coefficients.
-        T nbh[4];
-#pragma unroll
-        for (int d = 0; d < 4; ++d) nbh[d] = (nid[d] != -1) ? hr.s[0][0][nid[d]] - hr.s[3][0][nid[d]] : gh[d];
-        const bool dry = own.h[0] < P.tol_h && nbh[0] < P.tol_h && nbh[1] < P.tol_h && nbh[2] < P.tol_h &&
-                         nbh[3] < P.tol_h;
+        const bool dry = !LIST && leaf_is_dry(hr, own.h[0], nid, gh, P.tol_h);
+        n_wet += dry ? 0 : 1;
         // friction_implicit.cu:24-48: shallow or slow leaves lose their discharge and
         // skip friction (their neighbours' copies are then left untouched too)
         bool fric = false;
@@ -290,15 +422,21 @@ __global__ void __launch_bounds__(kSolverThreads) k_mwdg2_stage(Leaves<T> lf, Hi
         }
         if (dry)
         {
+            T u[9];
             if (STAGE == 1)
             {
 #pragma unroll
-                for (int m = 0; m < 3; ++m)
-                {
-                    lf.un[m][i] = own.h[m]; lf.un[3 + m][i] = own.qx[m]; lf.un[6 + m][i] = own.qy[m];
-                    lf.us[m][i] = own.h[m]; lf.us[3 + m][i] = own.qx[m]; lf.us[6 + m][i] = own.qy[m];
-                }
+                for (int m = 0; m < 3; ++m) { u[m] = own.h[m]; u[3 + m] = own.qx[m]; u[6 + m] = own.qy[m]; }
+#pragma unroll
+                for (int k = 0; k < 9; ++k) lf.un[k][i] = u[k];
             }
+            else
+            {
+#pragma unroll
+                for (int k = 0; k < 9; ++k) u[k] = lf.un[k][i];
+                mx.add(u, own.z[0]);
+            }
+            put_leaf(hout, a, u, own.z);
             dt_loc = fmin(dt_loc, P.initial_tstep);
             continue;
         }
@@ -378,27 +516,34 @@ __global__ void __launch_bounds__(kSolverThreads) k_mwdg2_stage(Leaves<T> lf, Hi
                 const T dty = P.CFL * geo.dxl / (fabs(uy) + sqrt(P.g * u[0]));
                 leaf_dt = fmin(dtx, dty);
             }
-            if (STAGE == 1)
-            {
-#pragma unroll
-                for (int k = 0; k < 9; ++k) lf.us[k][i] = u[k];
-            }
-            else
+            if (STAGE == 2)
             {
 #pragma unroll
                 for (int k = 0; k < 9; ++k) lf.un[k][i] = u[k];
                 nan_seen |= (u[0] != u[0]);
+                mx.add(u, own.z[0]);
             }
+            put_leaf(hout, a, u, own.z);
         }
-        else if (STAGE == 1)
+        else if (STAGE == 1) put_leaf(hout, a, pre, own.z);
+        else
         {
+            T u[9];
 #pragma unroll
-            for (int k = 0; k < 9; ++k) lf.us[k][i] = pre[k];
+            for (int k = 0; k < 9; ++k) u[k] = lf.un[k][i];
+            mx.add(u, own.z[0]);
+            put_leaf(hout, a, u, own.z);
         }
         dt_loc = fmin(dt_loc, leaf_dt);
     }
+    if (!LIST)
+    {
+        const unsigned tot = __reduce_add_sync(0xffffffffu, n_wet);
+        if ((threadIdx.x & 31) == 0 && tot) atomicAdd(&sc->wet[STAGE - 1], (int)tot);
+    }
     if (STAGE == 2)
     {
+        mx.flush(sc);
         dt_loc = warp_min(dt_loc);
         __shared__ T red[kSolverThreads / 32];
         const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -411,25 +556,6 @@ __global__ void __launch_bounds__(kSolverThreads) k_mwdg2_stage(Leaves<T> lf, Hi
             atomic_min_nn(&sc->dt_min, m);
         }
         if (__syncthreads_or(nan_seen) && threadIdx.x == 0) atomicOr(&sc->status, 1);
-    }
-}
-
-// Stage-1 result into the hierarchy (mra/reinsert_assem_sol.cu on d_buf_assem_sol).
-template <typename T> __global__ void __launch_bounds__(256) k_reinsert_us(Leaves<T> lf, Hier<T> hr, Scalars<T>* sc)
-{
-    const int n = sc->n_leaves;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    {
-        const int a = lf.act[i];
-        hr.s[0][0][a] = lf.us[0][i] + hr.s[3][0][a];
-        hr.s[1][0][a] = lf.us[3][i];
-        hr.s[2][0][a] = lf.us[6][i];
-        hr.s[0][1][a] = lf.us[1][i] + hr.s[3][1][a];
-        hr.s[1][1][a] = lf.us[4][i];
-        hr.s[2][1][a] = lf.us[7][i];
-        hr.s[0][2][a] = lf.us[2][i] + hr.s[3][2][a];
-        hr.s[1][2][a] = lf.us[5][i];
-        hr.s[2][2][a] = lf.us[8][i];
     }
 }
 

@@ -216,9 +216,10 @@ class Simulation:
         return out
 
     def last_step_counters(self) -> dict:
-        out = np.zeros(6, np.int64)
-        _check(lib().mwdg2_last_step_counters(self._h, _p(out, ctypes.c_int64), 6))
-        return dict(zip(("encoded", "reencoded", "decoded", "leaves", "detail_slots", "launches"), out.tolist()))
+        out = np.zeros(8, np.int64)
+        _check(lib().mwdg2_last_step_counters(self._h, _p(out, ctypes.c_int64), 8))
+        return dict(zip(("encoded", "reencoded", "decoded", "leaves", "detail_slots", "launches", "wet_stage1",
+                         "wet_stage2"), out.tolist()))
 
 
 def run_simulation(argv: list[str]) -> int:

@@ -99,7 +99,8 @@ mwdg2_status mwdg2_get_state(mwdg2_sim* sim, double* out, int64_t cap);
 mwdg2_status mwdg2_get_sig(mwdg2_sim* sim, uint8_t* out, int64_t cap);
 
 /* One hierarchy array: field 0 eta, 1 qx, 2 qy, 3 z; mode 0, 1 (1x), 2 (1y);
- * n_hierarchy values. */
+ * n_hierarchy values. After an MWDG2 step the leaves' entries hold the new state and the
+ * significant parents the scale coefficients encoded at the start of that step. */
 mwdg2_status mwdg2_get_hierarchy(mwdg2_sim* sim, int field, int mode, double* out, int64_t cap);
 
 /* Depth h = eta - z of the leaf containing each stage point, in .stage file order
@@ -107,9 +108,10 @@ mwdg2_status mwdg2_get_hierarchy(mwdg2_sim* sim, int field, int mode, double* ou
 mwdg2_status mwdg2_read_stage(mwdg2_sim* sim, double* out, int n);
 
 /* Device timing of the last step's kernels, in milliseconds, by phase:
- * [0] maxima + re-insertion + point sources, [1] encode + threshold + regularisation,
+ * [0] maxima + re-insertion (HWFV1, and MWDG2's first step; later MWDG2 steps take both
+ * from the previous stage 2) + point sources, [1] encode + threshold + regularisation,
  * [2] decode + extra significance, [3] leaf topology (leaf list and neighbours),
- * [4] MWDG2 stage 1 (or the HWFV1 update), [5] stage-1 re-insertion + scale re-encode +
+ * [4] MWDG2 stage 1 (or the HWFV1 update), [5] scale re-encode of the stage-1 result +
  * stage-2 maximum depth, [6] MWDG2 stage 2, [7] whole step including the scalar read-back.
  * Requires opts.verbose >= 2 at create (CUDA events per phase); otherwise zeros. n <= 8. */
 mwdg2_status mwdg2_last_step_timing(mwdg2_sim* sim, double* out, int n);
@@ -117,7 +119,7 @@ mwdg2_status mwdg2_last_step_timing(mwdg2_sim* sim, double* out, int n);
 /* Counters of the last step used for the algorithmic-bytes roofline:
  * [0] parents encoded (E), [1] parents re-encoded scale-only (E2), [2] parents decoded (D),
  * [3] leaves (N_a), [4] detail slots (T = get_lvl_idx(L) - 3), [5] kernels launched in the
- * step. n <= 6. */
+ * step, [6] / [7] MWDG2 leaves not dry in RK stage 1 / stage 2 (0 for HWFV1). n <= 8. */
 mwdg2_status mwdg2_last_step_counters(mwdg2_sim* sim, int64_t* out, int n);
 
 void mwdg2_destroy(mwdg2_sim* sim);
@@ -132,7 +134,8 @@ void mwdg2_destroy(mwdg2_sim* sim);
  * mwdg2_get_leaves reports them.
  *
  *   d_sig        device, get_lvl_idx(max_ref_lvl) bytes, 1 = significant (as returned
- *                by mwdg2_get_sig); every significant node's parent must be significant
+ *                by mwdg2_get_sig); every significant node's parent must be significant;
+ *                4-byte aligned (cudaMalloc pointers are), else MWDG2_ERR_ARG
  *   max_ref_lvl  5..13: the kernels' scratch is a file-scope device array of 65536 tile
  *                counts (about 256 KiB per device, held until the process exits); larger
  *                levels are rejected with MWDG2_ERR_ARG

@@ -51,3 +51,28 @@ def test_null_handle_calls_are_rejected():
     lib = mwdg2_b200.lib()
     assert lib.mwdg2_step(None, None, None) == 6
     assert lib.mwdg2_info(None, None, 0) == 6
+
+
+def _static_topology():
+    f = mwdg2_b200.lib().mwdg2_leaf_topology_static
+    f.restype = ctypes.c_int
+    f.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64), ctypes.c_void_p]
+    return f
+
+
+@pytest.mark.parametrize("sig_addr, level, cap, needle", [
+    (16, 14, 4 ** 14, "max_ref_lvl"),   # beyond the static scratch
+    (17, 8, 4 ** 8, "aligned"),         # flags are read four bytes at a time
+    (16, 8, 4 ** 8 - 1, "cap"),         # output too small for every finest cell
+])
+def test_static_topology_argument_errors(sig_addr, level, cap, needle):
+    """Argument checks of mwdg2_leaf_topology_static run on the host before any device
+    work, so the pointers are never dereferenced."""
+    f = _static_topology()
+    n = ctypes.c_int64(-1)
+    out = ctypes.c_void_p(256)
+    st = f(ctypes.c_void_p(sig_addr), level, 1 << level, 1 << level, out, out, out, out, cap, ctypes.byref(n), None)
+    assert st == 6
+    assert needle in mwdg2_b200.lib().mwdg2_last_error().decode()
+    assert n.value == -1
