@@ -299,6 +299,17 @@ __device__ __forceinline__ void encode_parent(const Hier<T>& hr, const Scalars<T
     hr.flags[p] = nf;
 }
 
+// Small levels are processed in bands of up to kBandDepth levels, one CTA per node of the
+// band's top level `lo`; the CTA's nodes at level l are (blockIdx.x << 2(l - lo)) + k for
+// k < 4^(l - lo), and __syncthreads orders one level's global writes before the next
+// level reads them. A band replaces up to five launches whose small grids are pure launch
+// latency; it pays for that with serial per-level latency inside each CTA, so only levels
+// up to kBandMaxLevel (at most 4^5 CTAs: one wave) are banded and larger levels get one
+// launch each (k_encode_level / k_decode_level).
+constexpr int kBandDepth = 5;
+constexpr int kBandMaxLevel = 9;
+
+// One level of parents (levels above kBandMaxLevel).
 template <typename T, bool MW, bool FULL>
 __global__ void __launch_bounds__(256) k_encode_level(Hier<T> hr, Scalars<T>* sc, int L, int level, T eps)
 {
@@ -309,16 +320,17 @@ __global__ void __launch_bounds__(256) k_encode_level(Hier<T> hr, Scalars<T>* sc
     if ((threadIdx.x & 31) == 0 && tot) atomicAdd(FULL ? &sc->enc : &sc->enc2, (unsigned long long)tot);
 }
 
-// Levels `top`..0 in one block (bottom-up, __syncthreads between levels).
+// Encode (FULL: + threshold + regularise; else scale-only re-encode) levels
+// lo + depth - 1 .. lo bottom-up (mra/encode_flow.cu, mra/regularisation.cu).
 template <typename T, bool MW, bool FULL>
-__global__ void __launch_bounds__(256) k_encode_top(Hier<T> hr, Scalars<T>* sc, int L, int top, T eps)
+__global__ void __launch_bounds__(256) k_encode_band(Hier<T> hr, Scalars<T>* sc, int L, int lo, int depth, T eps)
 {
     unsigned done = 0;
-    for (int level = top; level >= 0; --level)
+    for (int l = lo + depth - 1; l >= lo; --l)
     {
-        for (int idx = threadIdx.x; idx < (1 << (2 * level)); idx += blockDim.x)
-            encode_parent<T, MW, FULL>(hr, sc, L, level, idx, eps, done);
-        __syncthreads();
+        const int n = 1 << (2 * (l - lo)), base = (int)blockIdx.x << (2 * (l - lo));
+        for (int k = threadIdx.x; k < n; k += blockDim.x) encode_parent<T, MW, FULL>(hr, sc, L, l, base + k, eps, done);
+        if (l > lo) __syncthreads();
     }
     const unsigned tot = __reduce_add_sync(0xffffffffu, done);
     if ((threadIdx.x & 31) == 0 && tot) atomicAdd(FULL ? &sc->enc : &sc->enc2, (unsigned long long)tot);
@@ -396,26 +408,39 @@ __device__ __forceinline__ void decode_parent(const Hier<T>& hr, const Scalars<T
     }
 }
 
+// First level on the root -> node path whose node is not significant (levels 0..Tl, the
+// last being node `tcode` of level Tl); Tl + 1 if all are. Called by a whole warp: lane j
+// loads level j's flag, so the loads are independent. Needs Tl + 1 <= 32.
+__device__ __forceinline__ int path_leaf_level_warp(const uint8_t* flags, int Tl, int tcode)
+{
+    const int lane = threadIdx.x & 31;
+    const bool nonsig = lane <= Tl && !(flags[lvl_idx(lane) + (tcode >> (2 * (Tl - lane)))] & F_SIG);
+    const unsigned m = __ballot_sync(0xffffffffu, nonsig);
+    return m ? __ffs(m) - 1 : Tl + 1;
+}
+
+// Decode levels lo .. lo + depth - 1 top-down (mra/decoding.cu, mra/extra_significance.cu).
+template <typename T, bool MW>
+__global__ void __launch_bounds__(256) k_decode_band(Hier<T> hr, Scalars<T>* sc, int L, int lo, int depth, T eps)
+{
+    unsigned done = 0;
+    for (int l = lo; l < lo + depth; ++l)
+    {
+        const int n = 1 << (2 * (l - lo)), base = (int)blockIdx.x << (2 * (l - lo));
+        for (int k = threadIdx.x; k < n; k += blockDim.x) decode_parent<T, MW>(hr, sc, L, l, base + k, eps, done);
+        if (l + 1 < lo + depth) __syncthreads();
+    }
+    const unsigned tot = __reduce_add_sync(0xffffffffu, done);
+    if ((threadIdx.x & 31) == 0 && tot) atomicAdd(&sc->dec, (unsigned long long)tot);
+}
+
+// One level of parents (levels above kBandMaxLevel).
 template <typename T, bool MW>
 __global__ void __launch_bounds__(256) k_decode_level(Hier<T> hr, Scalars<T>* sc, int L, int level, T eps)
 {
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned done = 0;
     if (idx < (1 << (2 * level))) decode_parent<T, MW>(hr, sc, L, level, idx, eps, done);
-    const unsigned tot = __reduce_add_sync(0xffffffffu, done);
-    if ((threadIdx.x & 31) == 0 && tot) atomicAdd(&sc->dec, (unsigned long long)tot);
-}
-
-template <typename T, bool MW>
-__global__ void __launch_bounds__(256) k_decode_top(Hier<T> hr, Scalars<T>* sc, int L, int top, T eps)
-{
-    unsigned done = 0;
-    for (int level = 0; level <= top; ++level)
-    {
-        for (int idx = threadIdx.x; idx < (1 << (2 * level)); idx += blockDim.x)
-            decode_parent<T, MW>(hr, sc, L, level, idx, eps, done);
-        __syncthreads();
-    }
     const unsigned tot = __reduce_add_sync(0xffffffffu, done);
     if ((threadIdx.x & 31) == 0 && tot) atomicAdd(&sc->dec, (unsigned long long)tot);
 }
@@ -463,17 +488,6 @@ __global__ void __launch_bounds__(256) k_topo_level(Hier<T> hr, Scalars<T>* sc, 
 // traversal + compaction produce: mra/traverse_tree_of_sig_details.cu,
 // neighbours/compaction.cu).
 
-// First level on the root -> tile path whose node is not significant; Tl if none.
-// Called by a whole warp: lane j loads level j's flag, so the Tl (<= 10) loads are
-// independent instead of a chain of dependent loads.
-__device__ __forceinline__ int tile_leaf_level_warp(const uint8_t* flags, int Tl, int tcode)
-{
-    const int lane = threadIdx.x & 31;
-    const bool nonsig = lane < Tl && !(flags[lvl_idx(lane) + (tcode >> (2 * (Tl - lane)))] & F_SIG);
-    const unsigned m = __ballot_sync(0xffffffffu, nonsig);
-    return m ? __ffs(m) - 1 : Tl;
-}
-
 // First level j in [j0, lim) whose node on the path to finest cell `tc` is not
 // significant; lim if none. The (at most 16) flag loads are issued independently.
 __device__ __forceinline__ int first_nonsig_level(const uint8_t* flags, int L, int tc, int j0, int lim)
@@ -505,19 +519,15 @@ __device__ __forceinline__ int tile_flag_word(int Tl, int tcode, int w, int& j)
     return lvl_idx(Tl + j) + (tcode << (2 * j)) + 4 * (w - wbase);
 }
 
-// static: the header is included by more than one translation unit of the library
-static __global__ void __launch_bounds__(kTileThreads) k_tile_count(const uint8_t* flags, int L, int32_t* counts)
+// Leaves of tile `tcode` (node of level Tl = L - 5): 1 + 3 x (significant nodes of its
+// subtree) when every node on its root path is significant; otherwise 1 for the first
+// tile of the coarser leaf covering it (or its own non-significant root) and 0 for the
+// others. Called by the whole block (256 threads); returns the count in every thread.
+__device__ __forceinline__ int tile_leaf_count(const uint8_t* flags, int Tl, int tcode)
 {
     static_assert(kTileDepth == 5, "the word layout of tile_flag_word assumes 4^5-cell tiles");
-    const int Tl = L - kTileDepth;
-    const int tcode = blockIdx.x;
-    const int k = tile_leaf_level_warp(flags, Tl + 1, tcode << 2);  // levels 0..Tl, every warp finds it
-    if (k <= Tl)
-    {
-        // a coarser leaf starts in its first tile only; a non-significant root is one leaf
-        if (threadIdx.x == 0) counts[tcode] = (k == Tl || (tcode & ((1 << (2 * (Tl - k))) - 1)) == 0) ? 1 : 0;
-        return;
-    }
+    const int k = path_leaf_level_warp(flags, Tl, tcode);  // every warp finds it
+    if (k <= Tl) return (k == Tl || (tcode & ((1 << (2 * (Tl - k))) - 1)) == 0) ? 1 : 0;
     // significant nodes of the subtree: the root plus levels Tl+1 .. L-1 (85 flag words)
     int cnt = 0;
     if (threadIdx.x < 85)
@@ -527,10 +537,20 @@ static __global__ void __launch_bounds__(kTileThreads) k_tile_count(const uint8_
         cnt = __popc(w & (0x01010101u * F_SIG));
     }
     cnt = __reduce_add_sync(0xffffffffu, cnt);
-    __shared__ int s_cnt[kTileThreads / 32];
-    if ((threadIdx.x & 31) == 0) s_cnt[threadIdx.x >> 5] = cnt;
+    __shared__ int s_cnt[3];
+    if ((threadIdx.x & 31) == 0 && threadIdx.x < 96) s_cnt[threadIdx.x >> 5] = cnt;
     __syncthreads();
-    if (threadIdx.x == 0) counts[tcode] = 1 + 3 * (1 + s_cnt[0] + s_cnt[1] + s_cnt[2]);
+    const int total = 1 + 3 * (1 + s_cnt[0] + s_cnt[1] + s_cnt[2]);
+    __syncthreads();  // s_cnt may be reused by a later call
+    return total;
+}
+
+// Tile leaf counts from final flags.
+// static: the header is included by more than one translation unit of the library
+static __global__ void __launch_bounds__(kTileThreads) k_tile_count(const uint8_t* flags, int L, int32_t* counts)
+{
+    const int c = tile_leaf_count(flags, L - kTileDepth, (int)blockIdx.x);
+    if (threadIdx.x == 0) counts[blockIdx.x] = c;
 }
 
 // Exclusive scan of n tile counts in one block; total -> sc->n_leaves.
@@ -640,7 +660,7 @@ __global__ void __launch_bounds__(kTileThreads) k_tile_emit(Leaves<T> lf, const 
     // leaf levels of the cells just outside the tile (N, E, S, W), indexed by the dilated
     // tile-local coordinate along the side (x bits for N/S, y bits shifted down for E/W)
     __shared__ uint8_t halo[4][(kXBits & (kCells - 1)) + 1];
-    const int k = tile_leaf_level_warp(flags, Tl + 1, tcode << 2);  // levels 0..Tl, every warp
+    const int k = path_leaf_level_warp(flags, Tl, tcode);  // levels 0..Tl, every warp
     if (k < Tl)
     {
         if ((tcode & ((1 << (2 * (Tl - k))) - 1)) == 0)

@@ -95,6 +95,9 @@ private:
     mw::Scalars<T>* sc_ = nullptr;      // device
     mw::Scalars<T>* sc_host_ = nullptr; // pinned
     int32_t* tile_counts_ = nullptr;
+    // bands of up to kBandDepth tree levels at and below level kBandMaxLevel, bottom first
+    struct Band { int lo, depth, grid; };
+    std::vector<Band> bands_;
     int32_t* wet_list_ = nullptr;       // leaves that are not dry in an RK stage
     int64_t wet_prev_[2] = {-1, -1};    // previous step's wet-leaf count per RK stage
     mw::Src<T>* d_src_ = nullptr;
@@ -144,6 +147,24 @@ private:
             mw::k_mwdg2_stage<T, STAGE, false><<<g_solver, mw::kSolverThreads, 0, st_>>>(lf_, hin, hout, sc_, P_, B, dt_,
                                                                                          fric, nullptr);
             launches_ += 1;
+        }
+    }
+    // Bottom-up walk of the tree: one launch per level above kBandMaxLevel, then the bands.
+    // FULL: encode + threshold + regularise; else scale-only re-encode.
+    template <bool FULL> void encode_tree(const mw::Hier<T>& h, T eps)
+    {
+        for (int level = L_ - 1; level > mw::kBandMaxLevel; --level)
+        {
+            const int nb = grid_for((int64_t)1 << (2 * level), 256, 1 << 30);
+            if (mw_) mw::k_encode_level<T, true, FULL><<<nb, 256, 0, st_>>>(h, sc_, L_, level, eps);
+            else mw::k_encode_level<T, false, FULL><<<nb, 256, 0, st_>>>(h, sc_, L_, level, eps);
+            ++launches_;
+        }
+        for (const Band& b : bands_)
+        {
+            if (mw_) mw::k_encode_band<T, true, FULL><<<b.grid, 256, 0, st_>>>(h, sc_, L_, b.lo, b.depth, eps);
+            else mw::k_encode_band<T, false, FULL><<<b.grid, 256, 0, st_>>>(h, sc_, L_, b.lo, b.depth, eps);
+            ++launches_;
         }
     }
     mwdg2_status write_outputs(bool first);
@@ -201,6 +222,11 @@ template <typename T> mwdg2_status Sim<T>::init(const char* par, const mwdg2_opt
     n_all_ = mw::lvl_idx(L_ + 1);
     D_ = std::min(mw::kTileDepth, L_);
     ntiles_ = 1 << (2 * (L_ - D_));
+    for (int hi = std::min(L_ - 1, mw::kBandMaxLevel); hi >= 0; hi -= mw::kBandDepth)
+    {
+        const int lo = std::max(0, hi - mw::kBandDepth + 1);
+        bands_.push_back(Band{lo, hi - lo + 1, 1 << (2 * lo)});
+    }
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_);
     solver_blocks_ = sms * 8;
@@ -350,29 +376,24 @@ template <typename T> mwdg2_status Sim<T>::launch_step()
         ++launches_;
     }
     rec(1);
-    const int top = std::min(4, L_ - 1);
     const bool remesh = (eps > T(0) || first_);
-    if (remesh)
-    {
-        for (int level = L_ - 1; level > top; --level)
-        {
-            const int nb = grid_for((int64_t)1 << (2 * level), 256, 1 << 24);
-            if (mw) { mw::k_encode_level<T, true, true><<<nb, 256, 0, st_>>>(hr_, sc_, L_, level, eps); ++launches_; }
-            else { mw::k_encode_level<T, false, true><<<nb, 256, 0, st_>>>(hr_, sc_, L_, level, eps); ++launches_; }
-        }
-        if (mw) { mw::k_encode_top<T, true, true><<<1, 256, 0, st_>>>(hr_, sc_, L_, top, eps); ++launches_; }
-        else { mw::k_encode_top<T, false, true><<<1, 256, 0, st_>>>(hr_, sc_, L_, top, eps); ++launches_; }
-    }
+    if (remesh) encode_tree<true>(hr_, eps);
     rec(2);
     if (remesh)
     {
-        if (mw) { mw::k_decode_top<T, true><<<1, 256, 0, st_>>>(hr_, sc_, L_, top, eps); ++launches_; }
-        else { mw::k_decode_top<T, false><<<1, 256, 0, st_>>>(hr_, sc_, L_, top, eps); ++launches_; }
-        for (int level = top + 1; level < L_; ++level)
+        for (size_t k = bands_.size(); k-- > 0;)  // top band first
         {
-            const int nb = grid_for((int64_t)1 << (2 * level), 256, 1 << 24);
-            if (mw) { mw::k_decode_level<T, true><<<nb, 256, 0, st_>>>(hr_, sc_, L_, level, eps); ++launches_; }
-            else { mw::k_decode_level<T, false><<<nb, 256, 0, st_>>>(hr_, sc_, L_, level, eps); ++launches_; }
+            const Band& b = bands_[k];
+            if (mw) mw::k_decode_band<T, true><<<b.grid, 256, 0, st_>>>(hr_, sc_, L_, b.lo, b.depth, eps);
+            else mw::k_decode_band<T, false><<<b.grid, 256, 0, st_>>>(hr_, sc_, L_, b.lo, b.depth, eps);
+            ++launches_;
+        }
+        for (int level = mw::kBandMaxLevel + 1; level < L_; ++level)
+        {
+            const int nb = grid_for((int64_t)1 << (2 * level), 256, 1 << 30);
+            if (mw) mw::k_decode_level<T, true><<<nb, 256, 0, st_>>>(hr_, sc_, L_, level, eps);
+            else mw::k_decode_level<T, false><<<nb, 256, 0, st_>>>(hr_, sc_, L_, level, eps);
+            ++launches_;
         }
     }
     rec(3);
@@ -405,14 +426,7 @@ template <typename T> mwdg2_status Sim<T>::launch_step()
         rec(5);
         if (eps > T(0))
         {
-            for (int level = L_ - 1; level > top; --level)
-            {
-                const int nb = grid_for((int64_t)1 << (2 * level), 256, 1 << 24);
-                mw::k_encode_level<T, true, false><<<nb, 256, 0, st_>>>(hs_, sc_, L_, level, eps);
-                ++launches_;
-            }
-            mw::k_encode_top<T, true, false><<<1, 256, 0, st_>>>(hs_, sc_, L_, top, eps);
-            ++launches_;
+            encode_tree<false>(hs_, eps);
         }
         if (cs_.limitslopes) { mw::k_stage2_maxh<T><<<g_leaf, 256, 0, st_>>>(lf_, hs_, sc_, P_, B, dt_); ++launches_; }
         rec(6);

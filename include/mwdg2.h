@@ -110,7 +110,8 @@ mwdg2_status mwdg2_read_stage(mwdg2_sim* sim, double* out, int n);
 /* Device timing of the last step's kernels, in milliseconds, by phase:
  * [0] maxima + re-insertion (HWFV1, and MWDG2's first step; later MWDG2 steps take both
  * from the previous stage 2) + point sources, [1] encode + threshold + regularisation,
- * [2] decode + extra significance, [3] leaf topology (leaf list and neighbours),
+ * [2] decode + extra significance, [3] leaf topology (tile counts, scan, leaf list and
+ * neighbours),
  * [4] MWDG2 stage 1 (or the HWFV1 update), [5] scale re-encode of the stage-1 result +
  * stage-2 maximum depth, [6] MWDG2 stage 2, [7] whole step including the scalar read-back.
  * Requires opts.verbose >= 2 at create (CUDA events per phase); otherwise zeros. n <= 8. */
