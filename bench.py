@@ -1,6 +1,6 @@
 """Benchmark of the adaptive MWDG2/HWFV1 time step on B200.
 
-Workload (BASELINE config 2): fBm catchment, 4096 x 4096 finest cells (max_ref_lvl 12),
+Workload: fBm catchment, 4096 x 4096 finest cells (max_ref_lvl 12),
 2 m cells, Hurst 0.8, relief 0-30 m, Manning 0.03, dry start, west-edge point inflow with
 a triangular hydrograph peaking at 50 m^3/s at 30 min, epsilon 1e-3, MWDG2, FP32 state
 (--precision 64 for FP64). Seeded synthetic DEM (the reference ships no such DEM).
@@ -14,7 +14,7 @@ library's stream). Every input and the state are resident in HBM (the hierarchy 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
 --impl reference times the reference algorithm's CPU restatement (the reference itself
-has no CPU path; its CUDA build is timed separately, see DESIGN.md) on all host cores.
+has no CPU path; its CUDA build is timed separately) on all host cores.
 """
 from __future__ import annotations
 
@@ -133,7 +133,7 @@ def peaks() -> tuple[float, str]:
 
 
 def cpu_baseline(par: str, a, steps: int) -> dict:
-    """The oracle (CPU restatement of the reference algorithm) on the box's host cores."""
+    """The oracle (CPU restatement of the reference algorithm) on this machine's host cores."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle_py
     o = oracle_py.Oracle(par, a.precision)

@@ -9,9 +9,9 @@ dialect the reference reads (keyword readers `input/read_keyword_*.cpp`, raster 
 The same files feed this library, the CPU oracle and the reference build, so every
 implementation sees byte-identical inputs. Generators:
 
-* circular_dam_break  - flat bed, closed walls, radial depth step.
+* circular_dam_break  - flat bed, closed walls, radial depth step (256^2 parity case).
 * fbm_catchment       - fractional-Brownian-motion DEM, dry start, west-edge point
-                        inflow with a triangular hydrograph.
+                        inflow with a triangular hydrograph (4096^2 benchmark case).
 * lake_at_rest        - still water over an fBm bed (well-balancing checks).
 
 Reference quirks the generators respect (they would otherwise change the physics):
@@ -151,11 +151,13 @@ def circular_dam_break(directory: str, L: int = 8, solver: str = "mwdg2", eps: f
                        h_in: float = 2.5, h_out: float = 0.5, limitslopes: bool = True,
                        tol_krivo: float = 10.0, massint: float | None = 0.1,
                        cfl: float | None = None, manning: float = 0.0,
-                       stage_points: list[tuple[float, float]] | None = None) -> Case:
-    """Circular dam break on a flat bed with closed walls (BASELINE config 1 shape).
+                       stage_points: list[tuple[float, float]] | None = None,
+                       saveint: float | None = None, extra: list[str] | None = None) -> Case:
+    """Circular dam break on a flat bed with closed walls (the 256^2 parity case's shape).
 
     The start raster holds h = h_in inside `radius` of the domain centre and h_out
     outside, sampled at raster-cell centres. The bed is 0 and `wall_height` is 100.
+    `saveint` and `extra` (further .par lines, e.g. output keywords) pass through.
     """
     os.makedirs(directory, exist_ok=True)
     n = 1 << L
@@ -174,9 +176,9 @@ def circular_dam_break(directory: str, L: int = 8, solver: str = "mwdg2", eps: f
                         (domain / 2 - 12.5, domain / 2 - 12.5)]
     _write_stage(os.path.join(directory, "case.stage"), stage_points)
     lines = _common_par(solver, L, eps, sim_time, 100.0, manning, limitslopes, tol_krivo,
-                        massint, None, cfl,
+                        massint, saveint, cfl,
                         ["DEMfile       case.dem", "startfile     case.start",
-                         "stagefile     case.stage"])
+                         "stagefile     case.stage"] + list(extra or []))
     par = os.path.join(directory, "case.par")
     _write_par(par, lines)
     return Case(par=par, directory=directory, L=L, solver=solver, cellsize=dx,
@@ -212,17 +214,20 @@ def fbm_catchment(directory: str, L: int = 12, solver: str = "mwdg2", eps: float
                   t_peak: float = 1800.0, seed: int = 20261203, massint: float | None = None,
                   limitslopes: bool = False, tol_krivo: float = 10.0,
                   cfl: float | None = None, start_depth: np.ndarray | None = None,
-                  stage_points: list[tuple[float, float]] | None = None) -> Case:
-    """fBm catchment with a west-edge point inflow (BASELINE config 2 shape).
+                  stage_points: list[tuple[float, float]] | None = None,
+                  saveint: float | None = None, extra: list[str] | None = None) -> Case:
+    """fBm catchment with a west-edge point inflow (the 4096^2 benchmark case's shape).
 
     Dry start unless `start_depth` (south-up array) is given. The inflow is a
     triangular hydrograph 0 -> peak_q m^3/s at t_peak -> 0 at 2*t_peak, written as
     unit-width discharge peak_q/cellsize, padded to 2*sim_time + 2*t_peak.
+    `saveint` and `extra` (further .par lines, e.g. output keywords) pass through.
     """
     os.makedirs(directory, exist_ok=True)
     n = 1 << L
     dem = fbm_surface(n, hurst, seed, relief)
     write_esri_ascii(os.path.join(directory, "case.dem"), dem[::-1], cellsize, decimals=3)
+    user_extra = list(extra or [])
     extra = ["DEMfile       case.dem", "bcifile       case.bci", "bdyfile       case.bdy"]
     if start_depth is not None:
         write_esri_ascii(os.path.join(directory, "case.start"), start_depth[::-1], cellsize,
@@ -246,7 +251,7 @@ def fbm_catchment(directory: str, L: int = 12, solver: str = "mwdg2", eps: float
     _write_stage(os.path.join(directory, "case.stage"), stage_points)
     extra.append("stagefile     case.stage")
     lines = _common_par(solver, L, eps, sim_time, 1000.0, manning, limitslopes, tol_krivo,
-                        massint, None, cfl, extra)
+                        massint, saveint, cfl, extra + user_extra)
     par = os.path.join(directory, "case.par")
     _write_par(par, lines)
     return Case(par=par, directory=directory, L=L, solver=solver, cellsize=cellsize,

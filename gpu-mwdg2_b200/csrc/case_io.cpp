@@ -279,6 +279,13 @@ bool Case<T>::read(const std::string& par, double eps_override, int solver_overr
     // classes/PlottingParams.h:20-53, classes/SaveInterval.h:10-50
     cumulative = kf.has("cumulative");
     voutput_stage = kf.has("voutput_stage");
+    vtk = kf.has("vtk");
+    c_prop = kf.has("c_prop");
+    raster_out = kf.has("raster_out");
+    voutput = kf.has("voutput");   // a `voutput_stage` line also matches, as in the reference
+    qoutput = kf.has("qoutput");
+    elevoff = kf.has("elevoff");
+    depthoff = kf.has("depthoff");
     { std::string s = kf.str("resroot"); if (!s.empty()) resroot = s; }
     { std::string s = kf.str("dirroot"); if (!s.empty()) dirroot = s; }
     { bool f = false; T v = kf.real<T>("massint", &f); if (f) { massint = v; massint_count = 0; } }

@@ -70,6 +70,8 @@ template <typename T> struct Case
     // outputs (classes/PlottingParams.h:20-53, classes/SaveInterval.h)
     std::string dirroot = "res", resroot = "res";
     bool cumulative = false, voutput_stage = false;
+    bool vtk = false, c_prop = false, raster_out = false, voutput = false, qoutput = false, elevoff = false,
+         depthoff = false;
     T massint = T(9999.0), saveint = T(9999.0);
     int massint_count = 9999, saveint_count = 9999;
 

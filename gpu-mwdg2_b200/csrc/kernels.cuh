@@ -51,6 +51,7 @@ template <typename T> struct Params
 {
     int L, M, xsz, ysz, limit;
     T dx, tol_h, tol_q, tol_s, g, manning, CFL, initial_tstep, wall_height, tol_Krivo, eps;
+    T* dt_leaf;   // per-leaf CFL step of the final stage (VTK output), or null
 };
 
 template <typename T> struct Bnd

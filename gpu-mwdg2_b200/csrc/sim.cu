@@ -12,6 +12,7 @@
 // point-source values (when there are sources) and the scalar read-back.
 #include "../../include/mwdg2.h"
 #include "case_io.hpp"
+#include "outputs.cuh"
 #include "solver.cuh"
 
 #include <cerrno>
@@ -22,6 +23,7 @@
 #include <memory>
 #include <string>
 #include <sys/stat.h>
+#include <thread>
 #include <vector>
 
 namespace {
@@ -105,6 +107,8 @@ private:
     int32_t* d_stage_codes_ = nullptr;
     T* d_stage_out_ = nullptr;
     double* d_state_scratch_ = nullptr;
+    T* d_dt_leaf_ = nullptr;            // per-leaf CFL step of the last stage (VTK output only)
+    T* d_raster_ = nullptr;             // raster rows (saveint raster maps)
     mw::Params<T> P_{};
     // timing
     bool timed_ = false;
@@ -168,6 +172,11 @@ private:
         }
     }
     mwdg2_status write_outputs(bool first);
+    mwdg2_status write_cumulative(bool first);
+    mwdg2_status write_saveint(bool first);
+    mwdg2_status write_rasters(bool first);
+    mwdg2_status write_vtk();
+    mwdg2_status write_c_prop(bool first);
     mwdg2_status sample_stage(std::vector<T>& vals);
     mw::Bnd<T> bnd_now() const;
     int grid_for(int64_t n, int threads, int cap) const
@@ -312,6 +321,12 @@ template <typename T> mwdg2_status Sim<T>::init(const char* par, const mwdg2_opt
     P_.dx = cs_.dx; P_.tol_h = cs_.tol_h; P_.tol_q = cs_.tol_q; P_.tol_s = cs_.tol_s; P_.g = cs_.g;
     P_.manning = cs_.manning; P_.CFL = cs_.CFL; P_.initial_tstep = cs_.initial_tstep;
     P_.wall_height = cs_.wall_height; P_.tol_Krivo = cs_.tol_Krivo; P_.eps = cs_.epsilon;
+    P_.dt_leaf = nullptr;
+    if (o.write_outputs && cs_.vtk)
+    {
+        if (mwdg2_status s = dalloc(d_dt_leaf_, F_)) return s;
+        P_.dt_leaf = d_dt_leaf_;
+    }
 
     n_leaves_ = (int)F_;
     mw::k_init_leaves<T><<<grid_for(F_, 256, 4096), 256, 0, st_>>>(lf_, L_, (int)F_);
@@ -510,14 +525,7 @@ template <typename T> mwdg2_status Sim<T>::write_outputs(bool first)
     };
     if (cs_.cumulative)
     {
-        const std::string path = cs_.dirroot + "/" + cs_.resroot + ".cumu";
-        FILE* fp = fopen(path.c_str(), first ? "w" : "a");
-        if (!fp) return set_err(MWDG2_ERR_IO, "cannot write " + path);
-        if (first) fprintf(fp, "simtime,runtime_mra,runtime_solver,runtime_total,dt,reduction\n");
-        const double comp = (100.0 - 100.0 * n_leaves_ / ((double)cs_.xsz * cs_.ysz)) / 100.0;
-        fprintf(fp, "%lf,%lf,%lf,%lf,%lf,%lf\n", (double)time_, time_mra_, time_solver_, time_mra_ + time_solver_,
-                (double)dt_, comp);
-        fclose(fp);
+        if (mwdg2_status s = write_cumulative(first)) return s;
     }
     const int np = (int)cs_.stage_codes.size();
     if (np == 0) return MWDG2_OK;
@@ -581,6 +589,207 @@ template <typename T> mwdg2_status Sim<T>::write_outputs(bool first)
     return MWDG2_OK;
 }
 
+// output/write_cumulative_data.cpp:3-53 (runtime columns: host wall seconds of this loop)
+template <typename T> mwdg2_status Sim<T>::write_cumulative(bool first)
+{
+    const std::string path = cs_.dirroot + "/" + cs_.resroot + ".cumu";
+    FILE* fp = fopen(path.c_str(), first ? "w" : "a");
+    if (!fp) return set_err(MWDG2_ERR_IO, "cannot write " + path);
+    if (first) fprintf(fp, "simtime,runtime_mra,runtime_solver,runtime_total,dt,reduction\n");
+    const T comp = (T(100.0) - T(100.0) * n_leaves_ / T(cs_.xsz * cs_.ysz)) / T(100.0);
+    fprintf(fp, "%lf,%lf,%lf,%lf,%lf,%lf\n", (double)time_, time_mra_, time_solver_, time_mra_ + time_solver_,
+            (double)dt_, (double)comp);
+    fclose(fp);
+    return MWDG2_OK;
+}
+
+namespace {
+
+// Value format of the reference's text outputs (types/real.h: "%" NUM_FIG NUM_FRMT).
+template <typename T> const char* fig_fmt() { return sizeof(T) == 8 ? "%.15lf" : "%.8f"; }
+
+// Formats `rows` text rows with fmt_row(r, out) on the host's threads and writes them in
+// order (the large rasters and VTK sections are tens of millions of printf conversions).
+template <typename RowFn> bool write_rows(FILE* fp, int64_t rows, RowFn fmt_row)
+{
+    const int nt = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    const int64_t batch = (int64_t)nt * 256;
+    std::vector<std::string> buf((size_t)std::min<int64_t>(batch, std::max<int64_t>(rows, 1)));
+    for (int64_t r0 = 0; r0 < rows; r0 += batch)
+    {
+        const int64_t nr = std::min(batch, rows - r0);
+        std::vector<std::thread> th;
+        for (int t = 0; t < nt; ++t)
+            th.emplace_back([&, t] {
+                for (int64_t r = t; r < nr; r += nt)
+                {
+                    buf[r].clear();
+                    fmt_row(r0 + r, buf[r]);
+                }
+            });
+        for (auto& x : th) x.join();
+        for (int64_t r = 0; r < nr; ++r)
+            if (fwrite(buf[r].data(), 1, buf[r].size(), fp) != buf[r].size()) return false;
+    }
+    return true;
+}
+
+void append_fmt(std::string& out, const char* fmt, double v)
+{
+    char tmp[64];
+    const int k = snprintf(tmp, sizeof(tmp), fmt, v);
+    out.append(tmp, (size_t)std::max(0, std::min(k, (int)sizeof(tmp) - 1)));
+}
+
+} // namespace
+
+// run_simulation.cu:656-703
+template <typename T> mwdg2_status Sim<T>::write_saveint(bool first)
+{
+    if (cs_.vtk) { if (mwdg2_status s = write_vtk()) return s; }
+    if (cs_.raster_out) { if (mwdg2_status s = write_rasters(first)) return s; }
+    if (cs_.c_prop) { if (mwdg2_status s = write_c_prop(first)) return s; }
+    return MWDG2_OK;
+}
+
+// output/write_all_raster_maps{,_dg2,_fv1}.cu and output/write_raster_file.cu: ESRI ASCII
+// maps <dirroot>/<resroot>-<save index>.{elev,wd,qx,qy,vx,vy} and, at the first step, .dem.
+template <typename T> mwdg2_status Sim<T>::write_rasters(bool first)
+{
+    struct Map { const char* ext; int field; bool on; };
+    const Map maps[] = {{"elev", mw::R_ETA, !cs_.elevoff}, {"wd", mw::R_H, !cs_.depthoff},
+                        {"qx", mw::R_QX, cs_.qoutput}, {"qy", mw::R_QY, cs_.qoutput},
+                        {"vx", mw::R_VX, cs_.voutput}, {"vy", mw::R_VY, cs_.voutput},
+                        {"dem", mw::R_Z, first}};
+    unsigned fields = 0;
+    for (const Map& m : maps) if (m.on) fields |= 1u << m.field;
+    if (!fields) return MWDG2_OK;
+    const int nx = cs_.xsz, ny = cs_.ysz;
+    const size_t N = (size_t)nx * ny;
+    if (!d_raster_) { if (mwdg2_status s = dalloc(d_raster_, mw::R_COUNT * N)) return s; }
+    const int grid = grid_for((int64_t)N, 256, 1 << 20);
+    if (mw_) mw::k_raster<T, true><<<grid, 256, 0, st_>>>(lf_, hr_, sc_, L_, nx, ny, cs_.tol_h, fields, d_raster_);
+    else mw::k_raster<T, false><<<grid, 256, 0, st_>>>(lf_, hr_, sc_, L_, nx, ny, cs_.tol_h, fields, d_raster_);
+    CU(cudaGetLastError());
+    std::vector<T> host(N);
+    const char* vf = fig_fmt<T>();
+    const std::string vfs = std::string(vf) + " ";
+    for (const Map& m : maps)
+    {
+        if (!m.on) continue;
+        CU(cudaMemcpyAsync(host.data(), d_raster_ + (size_t)m.field * N, sizeof(T) * N, cudaMemcpyDeviceToHost, st_));
+        CU(cudaStreamSynchronize(st_));
+        const std::string path =
+            cs_.dirroot + "/" + cs_.resroot + "-" + std::to_string(cs_.saveint_count - 1) + "." + m.ext;
+        FILE* fp = fopen(path.c_str(), "w");
+        if (!fp) return set_err(MWDG2_ERR_IO, "cannot write raster " + path);
+        fprintf(fp, "ncols        %d\n", nx);
+        fprintf(fp, "nrows        %d\n", ny);
+        fprintf(fp, "xllcorner    %lf\n", (double)cs_.xmin);
+        fprintf(fp, "yllcorner    %lf\n", (double)cs_.ymin);
+        fprintf(fp, "cellsize     %lf\n", (double)cs_.dx);
+        fprintf(fp, "NODATA_value %d\n", -9999);
+        const bool ok = write_rows(fp, ny, [&](int64_t r, std::string& out) {
+            const T* row = host.data() + (size_t)(ny - 1 - r) * nx;   // top row first
+            for (int i = 0; i < nx; ++i) append_fmt(out, vfs.c_str(), (double)row[i]);
+            out.push_back('\n');
+        });
+        fclose(fp);
+        if (!ok) return set_err(MWDG2_ERR_IO, "cannot write raster " + path);
+    }
+    return MWDG2_OK;
+}
+
+// output/write_soln_vtk.cu:3-222: one quad per leaf with its CFL step and mode-0 state.
+template <typename T> mwdg2_status Sim<T>::write_vtk()
+{
+    const int n = n_leaves_;
+    std::vector<int32_t> act(n);
+    std::vector<uint8_t> lvl(n);
+    std::vector<double> st(12 * (size_t)n);
+    std::vector<T> dtl(n);
+    CU(cudaMemcpyAsync(act.data(), lf_.act, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st_));
+    CU(cudaMemcpyAsync(lvl.data(), lf_.lvl, n, cudaMemcpyDeviceToHost, st_));
+    CU(cudaMemcpyAsync(dtl.data(), d_dt_leaf_, sizeof(T) * n, cudaMemcpyDeviceToHost, st_));
+    CU(cudaStreamSynchronize(st_));
+    if (mwdg2_status s = state(st.data(), 12LL * n)) return s;
+    const std::string path = cs_.dirroot + "/" + cs_.resroot + "-" + std::to_string(cs_.saveint_count - 1) + ".vtk";
+    FILE* fp = fopen(path.c_str(), "w");
+    if (!fp) return set_err(MWDG2_ERR_IO, "cannot write " + path);
+    fprintf(fp, "# vtk DataFile Version 3.0\nMultiresolution flow and topo data\nASCII\n\n"
+                "DATASET UNSTRUCTURED_GRID\nPOINTS %d float\n", n * 4);
+    const T dx = cs_.dx, xmin = cs_.xmin, ymin = cs_.ymin;
+    bool ok = write_rows(fp, n, [&](int64_t i, std::string& out) {
+        const int l = lvl[i];
+        const int code = act[i] - mw::lvl_idx(l);
+        const T size = dx * T(1 << (L_ - l));
+        const int x = mw::compact(code), y = mw::compact(code >> 1);
+        const T xs[4] = {xmin + x * size, xmin + x * size, xmin + (x + 1) * size, xmin + (x + 1) * size};
+        const T ys[4] = {ymin + y * size, ymin + (y + 1) * size, ymin + y * size, ymin + (y + 1) * size};
+        for (int k = 0; k < 4; ++k)
+        {
+            append_fmt(out, "%lf ", (double)xs[k]);
+            append_fmt(out, "%lf ", (double)ys[k]);
+            append_fmt(out, "%lf\n", 1.0);
+        }
+    });
+    fprintf(fp, "\nCELLS %d %d\n", n, n * 5);
+    ok = ok && write_rows(fp, n, [&](int64_t i, std::string& out) {
+        char tmp[96];
+        const int p = (int)i * 4;
+        out.append(tmp, (size_t)snprintf(tmp, sizeof(tmp), "4 %d %d %d %d\n", p, p + 1, p + 2, p + 3));
+    });
+    fprintf(fp, "\nCELL_TYPES %d\n", n);
+    for (int i = 0; i < n; ++i) fputs("8\n", fp);
+    fprintf(fp, "\nCELL_DATA %d\n", n);
+    const size_t N = (size_t)n;
+    auto scalars = [&](const char* name, auto value) {
+        fprintf(fp, "\nSCALARS %s float 1\nLOOKUP_TABLE default\n", name);
+        return write_rows(fp, n, [&](int64_t i, std::string& out) { append_fmt(out, "%lf\n", (double)value(i)); });
+    };
+    ok = ok && scalars("dt", [&](int64_t i) { return dtl[i]; });
+    ok = ok && scalars("h", [&](int64_t i) { return (T)st[0 * N + i]; });
+    ok = ok && scalars("qx", [&](int64_t i) { return (T)st[1 * N + i]; });
+    ok = ok && scalars("qy", [&](int64_t i) { return (T)st[2 * N + i]; });
+    ok = ok && scalars("z", [&](int64_t i) { return (T)st[3 * N + i]; });
+    ok = ok && scalars("eta", [&](int64_t i) { return (T)((T)st[0 * N + i] + (T)st[3 * N + i]); });
+    fclose(fp);
+    if (!ok) return set_err(MWDG2_ERR_IO, "cannot write " + path);
+    return MWDG2_OK;
+}
+
+// output/write_c_prop_data.cu:3-81 and output/append_reals_to_file.cu:3-48: the cumulative
+// line, then one CSV row per save of each discharge mode over the leaves, appended to
+// <dirroot><name>.csv (the reference joins the two without a separator).
+template <typename T> mwdg2_status Sim<T>::write_c_prop(bool first)
+{
+    if (mwdg2_status s = write_cumulative(first)) return s;
+    const int n = n_leaves_;
+    struct Col { const char* name; int k; };
+    const Col cols[] = {{"qx0-c-prop", 3}, {"qy0-c-prop", 6}, {"qx1x-c-prop", 4}, {"qx1y-c-prop", 5},
+                        {"qy1x-c-prop", 7}, {"qy1y-c-prop", 8}};
+    const int ncols = mw_ ? 6 : 2;
+    std::vector<T> v(n);
+    const std::string vf = std::string(fig_fmt<T>()) + ",";
+    for (int c = 0; c < ncols; ++c)
+    {
+        CU(cudaMemcpyAsync(v.data(), lf_.un[cols[c].k], sizeof(T) * n, cudaMemcpyDeviceToHost, st_));
+        CU(cudaStreamSynchronize(st_));
+        const std::string path = cs_.dirroot + cols[c].name + ".csv";
+        FILE* fp = fopen(path.c_str(), first ? "w" : "a");
+        if (!fp) return set_err(MWDG2_ERR_IO, "cannot write " + path);
+        const int64_t per = 4096;
+        const bool ok = write_rows(fp, (n + per - 1) / per, [&](int64_t r, std::string& out) {
+            const int64_t hi = std::min<int64_t>(n, (r + 1) * per);
+            for (int64_t i = r * per; i < hi; ++i) append_fmt(out, vf.c_str(), (double)v[i]);
+        });
+        fputs("\n", fp);
+        fclose(fp);
+        if (!ok) return set_err(MWDG2_ERR_IO, "cannot write " + path);
+    }
+    return MWDG2_OK;
+}
+
 template <typename T> mwdg2_status Sim<T>::run(int64_t max_steps, int64_t* steps, int64_t* updates)
 {
     int64_t done = 0, upd = 0;
@@ -604,9 +813,13 @@ template <typename T> mwdg2_status Sim<T>::run(int64_t max_steps, int64_t* steps
         upd += n;
         if (opts_.write_outputs)
         {
-            // run_simulation.cu:656-751: saveint outputs (VTK/raster/c-prop) are not written;
+            // run_simulation.cu:656-751: saveint writes VTK / raster maps / c-prop data;
             // massint writes res.cumu (if `cumulative`) and the stage files
-            if (time_ >= cs_.saveint * cs_.saveint_count) cs_.saveint_count++;
+            if (time_ >= cs_.saveint * cs_.saveint_count)
+            {
+                cs_.saveint_count++;
+                if (mwdg2_status so = write_saveint(first)) return so;
+            }
             if (time_ >= cs_.massint * cs_.massint_count)
             {
                 cs_.massint_count++;

@@ -347,6 +347,7 @@ __global__ void __launch_bounds__(256) k_stage_classify(Leaves<T> lf, Hier<T> hi
 #pragma unroll
                     for (int k = 0; k < 9; ++k) u[k] = lf.un[k][i];
                     mx.add(u, z0);
+                    if (P.dt_leaf) P.dt_leaf[i] = P.initial_tstep;
                 }
                 put_leaf(hout, a, u, z);
             }
@@ -437,6 +438,7 @@ __global__ void __launch_bounds__(kSolverThreads) k_mwdg2_stage(Leaves<T> lf, Hi
                 mx.add(u, own.z[0]);
             }
             put_leaf(hout, a, u, own.z);
+            if (STAGE == 2 && P.dt_leaf) P.dt_leaf[i] = P.initial_tstep;
             dt_loc = fmin(dt_loc, P.initial_tstep);
             continue;
         }
@@ -534,6 +536,7 @@ __global__ void __launch_bounds__(kSolverThreads) k_mwdg2_stage(Leaves<T> lf, Hi
             mx.add(u, own.z[0]);
             put_leaf(hout, a, u, own.z);
         }
+        if (STAGE == 2 && P.dt_leaf) P.dt_leaf[i] = leaf_dt;
         dt_loc = fmin(dt_loc, leaf_dt);
     }
     if (!LIST)
@@ -626,6 +629,7 @@ __global__ void __launch_bounds__(kSolverThreads) k_hwfv1(Leaves<T> lf, Hier<T> 
             lf.un[0][i] = own.h[0];
             lf.un[3][i] = own.qx[0];
             lf.un[6][i] = own.qy[0];
+            if (P.dt_leaf) P.dt_leaf[i] = P.initial_tstep;
             dt_loc = fmin(dt_loc, P.initial_tstep);
             continue;
         }
@@ -687,6 +691,7 @@ __global__ void __launch_bounds__(kSolverThreads) k_hwfv1(Leaves<T> lf, Hier<T> 
         lf.un[0][i] = h;
         lf.un[3][i] = qx;
         lf.un[6][i] = qy;
+        if (P.dt_leaf) P.dt_leaf[i] = leaf_dt;
         dt_loc = fmin(dt_loc, leaf_dt);
     }
     dt_loc = warp_min(dt_loc);

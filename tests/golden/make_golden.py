@@ -7,9 +7,9 @@ what its observation hooks dump (oracle/ref/hooks.cu) into compressed .npz files
   per dumped step n:  leaf list (act_idcs, levels), neighbour ids/levels, significance
                       flags, dt, maxes, and the leaf state after step n.
 
-The reference only runs on a GPU, so this script is run on the GPU box:
+The reference only runs on a GPU, so this script is run on a machine with one:
 
-    python tests/golden/make_golden.py --out gpurun_out/golden
+    python tests/golden/make_golden.py --out <dir>
 
 and the resulting files are copied into tests/golden/. Tests then use them to pin the
 CPU oracle and the CUDA product. Inputs are regenerated from the same seeds, so the
