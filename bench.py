@@ -75,53 +75,75 @@ def make_case(a, rank: int) -> str:
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """SM clock and clock-event reasons sampled through NVML (read-only queries) on a
+    background thread every ~2 ms from the warm-up to the end of the end-to-end loop."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-         "clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4))
 
     def __init__(self, device: int):
-        self.path = tempfile.mktemp(suffix=".csv")
         self.device = device
-        self.p = None
+        self.rows: list[tuple[float, float, int]] = []
+        self._stop = None
+        self._thread = None
+
+    def _handle(self, nv):
+        """NVML handle of this process's CUDA device (CUDA and NVML orderings can differ)."""
+        import torch
+        p = torch.cuda.get_device_properties(self.device)
+        try:
+            return nv.nvmlDeviceGetHandleByUUID(f"GPU-{p.uuid}".encode())
+        except Exception:
+            pass
+        try:
+            bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+            return nv.nvmlDeviceGetHandleByPciBusId(bus.encode())
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(self.device)
 
     def __enter__(self):
+        import threading
         try:
-            self.f = open(self.path, "w")
-            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
-                                       "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
-                                      stderr=subprocess.DEVNULL)
+            import pynvml as nv
+            nv.nvmlInit()
+            h = self._handle(nv)
+            mx = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
         except Exception:
-            self.p = None
+            return self
+        self._stop = threading.Event()
+
+        def run():
+            while not self._stop.is_set():
+                try:
+                    sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                    rs = int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))
+                    self.rows.append((sm, mx, rs))
+                except Exception:
+                    pass
+                self._stop.wait(0.002)
+
+        self._thread = threading.Thread(target=run, daemon=True)
+        self._thread.start()
         return self
 
     def __exit__(self, *exc):
-        if self.p:
-            self.p.terminate()
-            try:
-                self.p.wait(timeout=5)
-            except Exception:
-                self.p.kill()
-            self.f.close()
+        if self._thread:
+            self._stop.set()
+            self._thread.join(timeout=5)
 
     def summary(self) -> dict:
-        rows = []
-        try:
-            for ln in open(self.path):
-                parts = [x.strip() for x in ln.split(",")]
-                if len(parts) >= 9:
-                    rows.append(parts)
-        except Exception:
-            pass
-        if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        reasons = sorted({n for _, _, r in self.rows for n, bit in self.REASONS if r & bit})
+        return {"sm_mhz": statistics.median(r[0] for r in self.rows), "sm_max_mhz": max(r[1] for r in self.rows),
+                "reasons": reasons, "samples": len(self.rows), "source": "nvml"}
+
+
+# DRAM bytes per leaf (dram__bytes_read.sum + dram__bytes_write.sum of the phase's kernels
+# divided by the leaves) from ncu captures of the same workload at max_ref_lvl 11 (1.2 M
+# leaves; the traffic grows with the leaves). Keyed by (solver, P, timing phase).
+TRAFFIC_SOURCE = "ncu, fBm catchment 2048^2 (max_ref_lvl 11), scaled by leaves"
+TRAFFIC_B_PER_LEAF: dict = {}
 
 
 def peaks() -> tuple[float, str]:
@@ -253,34 +275,56 @@ def main():
     mean_ph = ph.mean(axis=0)
     n_mean = float(np.mean(leaves))
     peak, peak_kind = peaks()
-    # per-leaf compulsory bytes of a fused MWDG2 stage kernel: topology 25 B (act, level,
-    # 4 neighbour ids + levels) + own 12 coefficients read + 18 written (stage 1: U^n, U*;
-    # stage 2: U^n read and written) = 25 + 30P
-    cand = {"k_mwdg2_stage<1> (RK stage 1: gather, friction, limiter, DG2)": (mean_ph[4], 25 + 30 * P),
-            "k_mwdg2_stage<2> (RK stage 2: gather, limiter, DG2, RK average, CFL)": (mean_ph[6], 25 + 30 * P)}
+    # Per-leaf algorithmic bytes of the reference-layout model: leaf topology 40 B (code,
+    # level, 4 x (neighbour id, level)); RK stage 1: 12P own coefficients + 16 B neighbour
+    # ids + 9P written + 9P of U^n = 30P + 16; stage 2: 21P + 16 (together the N(51P + 32)
+    # solver term of the step formula below). HWFV1: 4P own + 16 B ids + 3P written.
+    cand = {"leaf topology (k_tile_count + k_tile_scan + k_tile_emit)": (3, 40),
+            "RK stage 1 (k_stage_classify<1> + k_mwdg2_stage<1> over the wet list, or one k_mwdg2_stage<1> "
+            "sweep)": (4, 30 * P + 16),
+            "RK stage 2 (k_stage_classify<2> + k_mwdg2_stage<2> over the wet list, or one k_mwdg2_stage<2> "
+            "sweep)": (6, 21 * P + 16)}
     if a.solver == "hwfv1":
-        cand = {"k_hwfv1 (gather, friction, FV1 update, CFL)": (mean_ph[4], 25 + 7 * P)}
-    kname, (kms, per_leaf) = max(cand.items(), key=lambda kv: kv[1][0])
+        cand = {"leaf topology (k_tile_count + k_tile_scan + k_tile_emit)": (3, 40),
+                "k_hwfv1 (gather, friction, FV1 update, CFL)": (4, 7 * P + 16)}
+    kname, (kph, per_leaf) = max(cand.items(), key=lambda kv: mean_ph[kv[1][0]])
+    kms = float(mean_ph[kph])
+    traffic = TRAFFIC_B_PER_LEAF.get((a.solver, P, kph))
     achieved = per_leaf * n_mean / (kms / 1e3) / 1e9
-    c = counters[-1]
-    step_bytes = (c["encoded"] * (73 * P + 1) + c["reencoded"] * 45 * P + c["detail_slots"] * (P + 2) +
-                  c["decoded"] * 72 * P + 40 * n_mean + n_mean * (51 * P + 32))
+    # Algorithmic bytes per step of the reference-layout model, from each step's device
+    # counters: E parents encoded, E2 re-encoded (scale only), D decoded, T detail slots,
+    # N leaves; MWDG2 B = E(73P+1) + E2*45P + T(P+2) + D*72P + 40N + N(51P+32), HWFV1
+    # B = E(25P+1) + T(P+2) + D*24P + 40N + N(7P+16). This build stores no details or norms,
+    # so its encode moves fewer bytes than the model counts.
+    if a.solver == "mwdg2":
+        formula = "E(73P+1)+E2*45P+T(P+2)+D*72P+40N+N(51P+32)"
+        per_step = [c["encoded"] * (73 * P + 1) + c["reencoded"] * 45 * P + c["detail_slots"] * (P + 2) +
+                    c["decoded"] * 72 * P + 40 * c["leaves"] + c["leaves"] * (51 * P + 32) for c in counters]
+    else:
+        formula = "E(25P+1)+T(P+2)+D*24P+40N+N(7P+16)"
+        per_step = [c["encoded"] * (25 * P + 1) + c["detail_slots"] * (P + 2) + c["decoded"] * 24 * P +
+                    40 * c["leaves"] + c["leaves"] * (7 * P + 16) for c in counters]
+    step_bytes = float(np.mean(per_step))
     step_gbs = step_bytes / (statistics.mean(ms_step) / 1e3) / 1e9
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": tot_ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": f"f{a.precision}", "data": "synthetic (seeded fBm DEM, no network)", "config": workload(a),
             "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                         "frac": achieved / peak, "peak_source": peak_kind,
+                         "traffic": traffic * n_mean if traffic else None,
+                         "traffic_source": TRAFFIC_SOURCE if traffic else None,
                          "bytes_per_leaf": per_leaf, "leaves_per_launch": n_mean, "kernel_ms": kms},
-            "roofline_step": {"algorithmic_bytes": step_bytes, "achieved_gbs": step_gbs, "frac": step_gbs / peak},
+            "roofline_step": {"algorithmic_bytes": step_bytes, "achieved_gbs": step_gbs, "frac": step_gbs / peak,
+                              "formula": formula},
             "e2e": {"value": world * e2e_leaves / e2e_wall, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": int(sum(cc["launches"] for cc in counters)),
             "clocks": clk.summary(),
             "phase_ms_mean": dict(zip(("step_begin_srcs", "encode", "decode", "topology", "stage1",
                                        "reencode", "stage2", "step"), [round(x, 4) for x in mean_ph])),
-            "leaves_mean": n_mean}
+            "leaves_mean": n_mean,
+            "wet_fraction": [float(np.mean([cc[k] for cc in counters])) / n_mean for k in ("wet_stage1", "wet_stage2")]}
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(par, a, a.cpu_steps)
     sim.close()

@@ -609,16 +609,6 @@ __device__ __forceinline__ void leaf_neighbour(const uint8_t* flags, int L, int 
     lv = (uint8_t)m;
 }
 
-// Level of the leaf containing finest cell (tx, ty), searching from the first level where
-// its path leaves that of `ref` (a cell of a tile whose root is significant, so every
-// shared ancestor is significant).
-__device__ __forceinline__ int cell_leaf_level(const uint8_t* flags, int L, int ref, int tx, int ty)
-{
-    const int tc = morton(tx, ty);
-    const int b = 31 - __clz(tc ^ ref);
-    return first_nonsig_level(flags, L, tc, max(0, L - (b >> 1)), L);
-}
-
 // A tile holding one leaf (the tile's root or the first tile of a coarser leaf): threads
 // 0..3 of the block find one neighbour each.
 template <typename T>
@@ -682,15 +672,34 @@ __global__ void __launch_bounds__(kTileThreads) k_tile_emit(Leaves<T> lf, const 
             *reinterpret_cast<const uint32_t*>(flags + g) & (0x01010101u * F_SIG);
     }
     const unsigned tbase = (unsigned)tcode << (2 * D);   // finest Morton code of the tile's first cell
-    const int tw = 1 << D;
-    if (threadIdx.x < 4 * tw)
+    static_assert((1 << D) == 32, "one warp per side of the tile");
+    if (threadIdx.x < 4 * 32)
     {
-        const int side = threadIdx.x / tw, i = threadIdx.x % tw;
-        const int tx0 = compact((int)tbase), ty0 = compact((int)(tbase >> 1));
-        const int hx = (side == 0 || side == 2) ? tx0 + i : (side == 1 ? tx0 + tw : tx0 - 1);
-        const int hy = (side == 1 || side == 3) ? ty0 + i : (side == 0 ? ty0 + tw : ty0 - 1);
-        halo[side][dilate(i)] =
-            (hx >= 0 && hx < M && hy >= 0 && hy < M) ? (uint8_t)cell_leaf_level(flags, L, (int)tbase, hx, hy) : 0;
+        // warp `side` (N, E, S, W) takes the adjacent tile; lane i its i-th cell along the
+        // shared edge. The neighbouring tile's root path decides for all lanes at once unless
+        // that root is significant; then each lane reads its cell's four in-tile levels.
+        const int side = threadIdx.x >> 5, i = threadIdx.x & 31;
+        const int tx = compact(tcode), ty = compact(tcode >> 1), nt = 1 << Tl;
+        const int nx = tx + (side == 1) - (side == 3), ny = ty + (side == 0) - (side == 2);
+        uint8_t lev = 0;                               // cells outside the mesh are never looked up
+        if (nx >= 0 && ny >= 0 && nx < nt && ny < nt)  // uniform in the warp
+        {
+            const int ncode = morton(nx, ny);
+            const int kn = path_leaf_level_warp(flags, Tl, ncode);
+            if (kn <= Tl) lev = (uint8_t)kn;
+            else
+            {
+                const int lx = (side == 0 || side == 2) ? i : (side == 1 ? 0 : 31);
+                const int ly = (side == 1 || side == 3) ? i : (side == 0 ? 0 : 31);
+                const int lc = morton(lx, ly);
+                int l = L;
+#pragma unroll
+                for (int j = D - 1; j >= 1; --j)
+                    if (!(flags[lvl_idx(Tl + j) + (ncode << (2 * j)) + (lc >> (2 * (D - j)))] & F_SIG)) l = Tl + j;
+                lev = (uint8_t)l;
+            }
+        }
+        halo[side][dilate(i)] = lev;
     }
     __syncthreads();
     // leaf level of every cell: the first level below the (significant) root whose node

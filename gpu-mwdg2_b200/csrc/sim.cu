@@ -15,14 +15,17 @@
 #include "outputs.cuh"
 #include "solver.cuh"
 
+#include <algorithm>
 #include <cerrno>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <cstdlib>
 #include <memory>
 #include <string>
 #include <sys/stat.h>
+#include <unistd.h>
 #include <thread>
 #include <vector>
 
@@ -49,6 +52,18 @@ struct SimBase
     virtual ~SimBase() = default;
     virtual mwdg2_status init(const char* par, const mwdg2_opts& o) = 0;
     virtual mwdg2_status step(double* dt, int64_t* n) = 0;
+    // A step in three parts, so that many simulations can have steps in flight at once:
+    // begin_step advances the clock (MWDG2_DONE once sim_time is reached), enqueue_step puts
+    // the step's kernels and its scalar read-back on the simulation's stream and returns,
+    // finish_step waits for them and takes the new dt and leaf count.
+    virtual mwdg2_status begin_step() = 0;
+    virtual mwdg2_status enqueue_step() = 0;
+    virtual mwdg2_status finish_step(double* dt, int64_t* n) = 0;
+    virtual bool first_step() const = 0;
+    virtual mwdg2_status prepare_outputs() = 0;
+    virtual mwdg2_status after_step(bool first, double dt, int64_t n, double step_seconds) = 0;
+    // Make a relative output folder relative to `dir` instead of the working directory.
+    virtual void anchor_outputs(const std::string& dir) = 0;
     virtual mwdg2_status run(int64_t max_steps, int64_t* steps, int64_t* updates) = 0;
     virtual mwdg2_status info(double* out, int n) = 0;
     virtual mwdg2_status leaves(int32_t* a, int32_t* l, int32_t* ids, int32_t* lv, int64_t cap) = 0;
@@ -67,6 +82,16 @@ public:
 
     mwdg2_status init(const char* par, const mwdg2_opts& o) override;
     mwdg2_status step(double* dt_out, int64_t* n_out) override;
+    mwdg2_status begin_step() override;
+    mwdg2_status enqueue_step() override;
+    mwdg2_status finish_step(double* dt_out, int64_t* n_out) override;
+    bool first_step() const override { return first_; }
+    mwdg2_status prepare_outputs() override;
+    mwdg2_status after_step(bool first, double dt, int64_t n, double step_seconds) override;
+    void anchor_outputs(const std::string& dir) override
+    {
+        if (!cs_.dirroot.empty() && cs_.dirroot[0] != '/') cs_.dirroot = dir + "/" + cs_.dirroot;
+    }
     mwdg2_status run(int64_t max_steps, int64_t* steps, int64_t* updates) override;
     mwdg2_status info(double* out, int n) override;
     mwdg2_status leaves(int32_t* a, int32_t* l, int32_t* ids, int32_t* lv, int64_t cap) override;
@@ -130,7 +155,8 @@ private:
         return MWDG2_OK;
     }
     void release();
-    mwdg2_status launch_step();
+    mwdg2_status launch_step();    // enqueue only
+    mwdg2_status collect_step();   // wait, timing, counters
     // One MWDG2 RK stage. When fewer than half of the leaves were wet in this stage last
     // step, a light pass finishes the dry leaves and lists the others for the full kernel
     // (whose grid is sized from last step's wet count); otherwise one sweep over all leaves.
@@ -451,6 +477,12 @@ template <typename T> mwdg2_status Sim<T>::launch_step()
     CU(cudaGetLastError());
     CU(cudaMemcpyAsync(sc_host_, sc_, sizeof(mw::Scalars<T>), cudaMemcpyDeviceToHost, st_));
     rec(8);
+    return MWDG2_OK;
+}
+
+template <typename T> mwdg2_status Sim<T>::collect_step()
+{
+    const bool mw = mw_;
     CU(cudaStreamSynchronize(st_));
     if (timed_)
     {
@@ -475,7 +507,7 @@ template <typename T> mwdg2_status Sim<T>::launch_step()
     return MWDG2_OK;
 }
 
-template <typename T> mwdg2_status Sim<T>::step(double* dt_out, int64_t* n_out)
+template <typename T> mwdg2_status Sim<T>::begin_step()
 {
     if (finished_ || !(time_ < cs_.sim_time))
     {
@@ -491,8 +523,27 @@ template <typename T> mwdg2_status Sim<T>::step(double* dt_out, int64_t* n_out)
         dt_ = cs_.sim_time - time_;
         time_ += dt_;
     }
-    mwdg2_status s = launch_step();
+    return MWDG2_OK;
+}
+
+template <typename T> mwdg2_status Sim<T>::enqueue_step()
+{
+    CU(cudaSetDevice(device_));
+    return launch_step();
+}
+
+template <typename T> mwdg2_status Sim<T>::step(double* dt_out, int64_t* n_out)
+{
+    mwdg2_status s = begin_step();
     if (s != MWDG2_OK) return s;
+    if ((s = launch_step()) != MWDG2_OK) return s;
+    return finish_step(dt_out, n_out);
+}
+
+template <typename T> mwdg2_status Sim<T>::finish_step(double* dt_out, int64_t* n_out)
+{
+    CU(cudaSetDevice(device_));
+    if (mwdg2_status s = collect_step()) return s;
     if (sc_host_->status & 1) return set_err(MWDG2_ERR_NUMERIC, "NaN in the leaf state");
     n_leaves_ = sc_host_->n_leaves;
     dt_ = sc_host_->dt_min;
@@ -790,15 +841,47 @@ template <typename T> mwdg2_status Sim<T>::write_c_prop(bool first)
     return MWDG2_OK;
 }
 
+template <typename T> mwdg2_status Sim<T>::prepare_outputs()
+{
+    if (!opts_.write_outputs) return MWDG2_OK;
+    // classes/PlottingParams.h:55-60 (mkdir dirroot)
+    if (mkdir(cs_.dirroot.c_str(), 0755) != 0 && errno != EEXIST)
+        return set_err(MWDG2_ERR_IO, "cannot create output directory " + cs_.dirroot);
+    return MWDG2_OK;
+}
+
+// Everything the reference's loop does after the solver (run_simulation.cu:656-766): saveint
+// writes VTK / raster maps / c-prop data; massint writes res.cumu (if `cumulative`) and the
+// stage files; the periodic progress line.
+template <typename T> mwdg2_status Sim<T>::after_step(bool first, double dt, int64_t n, double step_seconds)
+{
+    time_solver_ += step_seconds;
+    if (opts_.write_outputs)
+    {
+        if (time_ >= cs_.saveint * cs_.saveint_count)
+        {
+            cs_.saveint_count++;
+            if (mwdg2_status so = write_saveint(first)) return so;
+        }
+        if (time_ >= cs_.massint * cs_.massint_count)
+        {
+            cs_.massint_count++;
+            if (mwdg2_status so = write_outputs(first)) return so;
+        }
+    }
+    if (opts_.verbose && (timestep_ - 1) % 10000 == 1)
+    {
+        const double comp = 100.0 - 100.0 * n / ((double)cs_.xsz * cs_.ysz);
+        printf("Elements: %lld, compression: %f%%, time step: %f, timestep: %d, sim time: %f\n", (long long)n, comp,
+               dt, timestep_ - 1, (double)time_);
+    }
+    return MWDG2_OK;
+}
+
 template <typename T> mwdg2_status Sim<T>::run(int64_t max_steps, int64_t* steps, int64_t* updates)
 {
     int64_t done = 0, upd = 0;
-    if (opts_.write_outputs)
-    {
-        // classes/PlottingParams.h:55-60 (mkdir dirroot)
-        if (mkdir(cs_.dirroot.c_str(), 0755) != 0 && errno != EEXIST)
-            return set_err(MWDG2_ERR_IO, "cannot create output directory " + cs_.dirroot);
-    }
+    if (mwdg2_status s = prepare_outputs()) return s;
     while (max_steps <= 0 || done < max_steps)
     {
         const bool first = first_;
@@ -808,30 +891,10 @@ template <typename T> mwdg2_status Sim<T>::run(int64_t max_steps, int64_t* steps
         mwdg2_status s = step(&dt, &n);
         if (s == MWDG2_DONE) break;
         if (s != MWDG2_OK) return s;
-        time_solver_ += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         ++done;
         upd += n;
-        if (opts_.write_outputs)
-        {
-            // run_simulation.cu:656-751: saveint writes VTK / raster maps / c-prop data;
-            // massint writes res.cumu (if `cumulative`) and the stage files
-            if (time_ >= cs_.saveint * cs_.saveint_count)
-            {
-                cs_.saveint_count++;
-                if (mwdg2_status so = write_saveint(first)) return so;
-            }
-            if (time_ >= cs_.massint * cs_.massint_count)
-            {
-                cs_.massint_count++;
-                if (mwdg2_status so = write_outputs(first)) return so;
-            }
-        }
-        if (opts_.verbose && (timestep_ - 1) % 10000 == 1)
-        {
-            const double comp = 100.0 - 100.0 * n / ((double)cs_.xsz * cs_.ysz);
-            printf("Elements: %lld, compression: %f%%, time step: %f, timestep: %d, sim time: %f\n", (long long)n, comp,
-                   dt, timestep_ - 1, (double)time_);
-        }
+        const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (mwdg2_status so = after_step(first, dt, n, secs)) return so;
     }
     if (steps) *steps = done;
     if (updates) *updates = upd;
@@ -940,6 +1003,44 @@ struct mwdg2_sim
     std::unique_ptr<SimBase> impl;
 };
 
+struct mwdg2_batch
+{
+    std::vector<std::unique_ptr<mwdg2_sim>> members;
+    std::vector<uint8_t> done;
+};
+
+namespace {
+
+// Runs fn(i) for every member index on up to eight host threads (launching kernels from
+// several threads hides the per-launch host cost of many small members); returns the first
+// failing member's status, its message recorded for mwdg2_last_error.
+template <typename Fn> mwdg2_status for_members(int n, Fn fn)
+{
+    const int nt = std::max(1, std::min({n, 8, (int)std::max(1u, std::thread::hardware_concurrency())}));
+    std::vector<mwdg2_status> st(n, MWDG2_OK);
+    std::vector<std::string> msg(n);
+    auto work = [&](int t) {
+        for (int i = t; i < n; i += nt)
+        {
+            st[i] = fn(i);
+            if (st[i] != MWDG2_OK && st[i] != MWDG2_DONE) msg[i] = g_last_error;
+        }
+    };
+    if (nt == 1) work(0);
+    else
+    {
+        std::vector<std::thread> th;
+        for (int t = 0; t < nt; ++t) th.emplace_back(work, t);
+        for (auto& x : th) x.join();
+    }
+    for (int i = 0; i < n; ++i)
+        if (st[i] != MWDG2_OK && st[i] != MWDG2_DONE)
+            return set_err(st[i], "batch member " + std::to_string(i) + ": " + msg[i]);
+    return MWDG2_OK;
+}
+
+} // namespace
+
 extern "C" {
 
 void mwdg2_default_opts(mwdg2_opts* o)
@@ -1039,6 +1140,115 @@ mwdg2_status mwdg2_last_step_counters(mwdg2_sim* s, int64_t* out, int n)
 }
 
 void mwdg2_destroy(mwdg2_sim* s) { delete s; }
+
+mwdg2_status mwdg2_batch_create(int n, const char* const* par_paths, const mwdg2_opts* opts, mwdg2_batch** out)
+{
+    if (!out || !par_paths || n < 1) return set_err(MWDG2_ERR_ARG, "mwdg2_batch_create: need n >= 1 paths and an output");
+    *out = nullptr;
+    std::unique_ptr<mwdg2_batch> b(new mwdg2_batch());
+    char cwd[4096];
+    if (!getcwd(cwd, sizeof(cwd))) return set_err(MWDG2_ERR_IO, "mwdg2_batch_create: getcwd failed");
+    for (int i = 0; i < n; ++i)
+    {
+        if (!par_paths[i]) return set_err(MWDG2_ERR_ARG, "mwdg2_batch_create: null path " + std::to_string(i));
+        // relative names in a member's .par (and its dirroot) resolve against its own folder
+        const std::string path = par_paths[i];
+        const size_t cut = path.find_last_of('/');
+        const std::string dir = cut == std::string::npos ? "." : (cut == 0 ? "/" : path.substr(0, cut));
+        char absdir[4096];
+        if (!realpath(dir.c_str(), absdir) || chdir(absdir) != 0)
+            return set_err(MWDG2_ERR_IO, "batch member " + std::to_string(i) + ": cannot enter the folder of " + path);
+        mwdg2_sim* s = nullptr;
+        const std::string base = cut == std::string::npos ? path : path.substr(cut + 1);
+        mwdg2_status st = mwdg2_create(base.c_str(), opts, &s);
+        if (chdir(cwd) != 0 && st == MWDG2_OK) st = set_err(MWDG2_ERR_IO, "cannot return to the working directory");
+        if (st != MWDG2_OK)
+        {
+            delete s;
+            return set_err(st, "batch member " + std::to_string(i) + ": " + g_last_error);
+        }
+        b->members.emplace_back(s);
+        s->impl->anchor_outputs(absdir);
+        if ((st = s->impl->prepare_outputs()) != MWDG2_OK) return st;
+    }
+    b->done.assign(n, 0);
+    *out = b.release();
+    return MWDG2_OK;
+}
+
+mwdg2_status mwdg2_batch_step(mwdg2_batch* b, double* dts, int64_t* leaves, int32_t* active)
+{
+    if (!b) return set_err(MWDG2_ERR_ARG, "null batch");
+    const int n = (int)b->members.size();
+    std::vector<uint8_t> stepped(n, 0), first(n, 0);
+    std::vector<std::chrono::steady_clock::time_point> t0(n);
+    // clock updates and kernels of every member, without waiting
+    mwdg2_status st = for_members(n, [&](int i) -> mwdg2_status {
+        if (b->done[i]) return MWDG2_OK;
+        SimBase& m = *b->members[i]->impl;
+        first[i] = m.first_step();
+        t0[i] = std::chrono::steady_clock::now();
+        mwdg2_status s = m.begin_step();
+        if (s == MWDG2_DONE) { b->done[i] = 1; return MWDG2_OK; }
+        if (s != MWDG2_OK) return s;
+        stepped[i] = 1;
+        return m.enqueue_step();
+    });
+    // then wait for each member, take its dt and write its outputs
+    mwdg2_status st2 = for_members(n, [&](int i) -> mwdg2_status {
+        double dt = 0;
+        int64_t nl = 0;
+        if (stepped[i])
+        {
+            SimBase& m = *b->members[i]->impl;
+            mwdg2_status s = m.finish_step(&dt, &nl);
+            if (s != MWDG2_OK) return s;
+            const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0[i]).count();
+            if ((s = m.after_step(first[i], dt, nl, secs)) != MWDG2_OK) return s;
+        }
+        if (dts) dts[i] = dt;
+        if (leaves) leaves[i] = nl;
+        return MWDG2_OK;
+    });
+    if (st != MWDG2_OK) return st;
+    if (st2 != MWDG2_OK) return st2;
+    int32_t k = 0;
+    for (int i = 0; i < n; ++i) k += stepped[i];
+    if (active) *active = k;
+    return k ? MWDG2_OK : MWDG2_DONE;
+}
+
+mwdg2_status mwdg2_batch_run(mwdg2_batch* b, int64_t max_batch_steps, int64_t* batch_steps, int64_t* member_steps,
+                             int64_t* updates)
+{
+    if (!b) return set_err(MWDG2_ERR_ARG, "null batch");
+    const int n = (int)b->members.size();
+    std::vector<int64_t> nl(n);
+    int64_t bs = 0, ms = 0, upd = 0;
+    while (max_batch_steps <= 0 || bs < max_batch_steps)
+    {
+        int32_t k = 0;
+        mwdg2_status st = mwdg2_batch_step(b, nullptr, nl.data(), &k);
+        if (st == MWDG2_DONE) break;
+        if (st != MWDG2_OK) return st;
+        ++bs;
+        ms += k;
+        for (int i = 0; i < n; ++i) upd += nl[i];
+    }
+    if (batch_steps) *batch_steps = bs;
+    if (member_steps) *member_steps = ms;
+    if (updates) *updates = upd;
+    return MWDG2_OK;
+}
+
+mwdg2_status mwdg2_batch_member(mwdg2_batch* b, int i, mwdg2_sim** out)
+{
+    if (!b || !out || i < 0 || i >= (int)b->members.size()) return set_err(MWDG2_ERR_ARG, "mwdg2_batch_member: bad index");
+    *out = b->members[i].get();
+    return MWDG2_OK;
+}
+
+void mwdg2_batch_destroy(mwdg2_batch* b) { delete b; }
 
 mwdg2_status mwdg2_run_simulation(int argc, char** argv)
 {

@@ -298,9 +298,11 @@ template <typename T> struct StateMax
 // Wet-list construction for one RK stage: dry leaves are finished here, the others are
 // appended to `wet` for k_mwdg2_stage<.., LIST=true>. Stage 1 gives a dry leaf's state,
 // with the discharge cleared by friction, to U^n (un) and to the stage hierarchy `hout`;
-// stage 2 leaves it unchanged and re-inserts U^n into the hierarchy `hout`.
+// stage 2 leaves it unchanged and re-inserts U^n into the hierarchy `hout`. The kernel is
+// latency-bound on its gathers, so its registers are capped for more resident warps
+// (FP32: 40, 6 blocks per SM; FP64: 80, 3 blocks).
 template <typename T, int STAGE>
-__global__ void __launch_bounds__(256) k_stage_classify(Leaves<T> lf, Hier<T> hin, Hier<T> hout, Scalars<T>* sc,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 6 : 3) k_stage_classify(Leaves<T> lf, Hier<T> hin, Hier<T> hout, Scalars<T>* sc,
                                                         Params<T> P, Bnd<T> B, T dt, bool friction, int32_t* wet)
 {
     const int n = sc->n_leaves;

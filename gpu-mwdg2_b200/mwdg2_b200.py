@@ -80,9 +80,16 @@ def lib():
         L.mwdg2_last_step_timing.argtypes = [vp, dp, ctypes.c_int]
         L.mwdg2_last_step_counters.argtypes = [vp, i64p, ctypes.c_int]
         L.mwdg2_destroy.argtypes = [vp]
+        L.mwdg2_batch_create.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(Opts),
+                                         ctypes.POINTER(vp)]
+        L.mwdg2_batch_step.argtypes = [vp, dp, i64p, i32p]
+        L.mwdg2_batch_run.argtypes = [vp, ctypes.c_int64, i64p, i64p, i64p]
+        L.mwdg2_batch_member.argtypes = [vp, ctypes.c_int, ctypes.POINTER(vp)]
+        L.mwdg2_batch_destroy.argtypes = [vp]
         for name in ("mwdg2_create", "mwdg2_step", "mwdg2_run", "mwdg2_run_simulation", "mwdg2_info",
                      "mwdg2_get_leaves", "mwdg2_get_state", "mwdg2_get_sig", "mwdg2_get_hierarchy",
-                     "mwdg2_read_stage", "mwdg2_last_step_timing", "mwdg2_last_step_counters"):
+                     "mwdg2_read_stage", "mwdg2_last_step_timing", "mwdg2_last_step_counters", "mwdg2_batch_create",
+                     "mwdg2_batch_step", "mwdg2_batch_run", "mwdg2_batch_member"):
             getattr(L, name).restype = ctypes.c_int
         _lib = L
     return _lib
@@ -120,25 +127,26 @@ class Simulation:
                  device: int = -1, timing: bool = False):
         self.par = os.path.abspath(par)
         self.dir = os.path.dirname(self.par)
-        o = Opts()
-        lib().mwdg2_default_opts(ctypes.byref(o))
-        o.precision = precision
-        o.device = device
-        o.epsilon = -1.0 if epsilon is None else float(epsilon)
-        o.solver = {None: 0, "hwfv1": 1, "mwdg2": 2}[solver]
-        self._dirroot = dirroot.encode() if dirroot else None
-        o.dirroot = self._dirroot
-        o.write_outputs = 1 if write_outputs else 0
-        o.verbose = 2 if timing else 0
+        o = _opts(precision, epsilon, solver, dirroot, write_outputs, device, timing)
+        self._dirroot = o.dirroot
         h = ctypes.c_void_p()
         with _cwd(self.dir):
             _check(lib().mwdg2_create(self.par.encode(), ctypes.byref(o), ctypes.byref(h)))
         self._h = h
+        self._owned = True
         self.precision = precision
+
+    @classmethod
+    def _view(cls, handle: ctypes.c_void_p, par: str, precision: int, owner) -> "Simulation":
+        """A member of a Batch: getters only; the batch owns and steps it."""
+        s = cls.__new__(cls)
+        s.par, s.dir, s._h, s._owned, s.precision, s._owner = par, os.path.dirname(par), handle, False, precision, owner
+        return s
 
     def close(self):
         if getattr(self, "_h", None):
-            lib().mwdg2_destroy(self._h)
+            if getattr(self, "_owned", True):
+                lib().mwdg2_destroy(self._h)
             self._h = None
 
     def __enter__(self):
@@ -220,6 +228,75 @@ class Simulation:
         _check(lib().mwdg2_last_step_counters(self._h, _p(out, ctypes.c_int64), 8))
         return dict(zip(("encoded", "reencoded", "decoded", "leaves", "detail_slots", "launches", "wet_stage1",
                          "wet_stage2"), out.tolist()))
+
+
+def _opts(precision, epsilon, solver, dirroot, write_outputs, device, timing) -> Opts:
+    o = Opts()
+    lib().mwdg2_default_opts(ctypes.byref(o))
+    o.precision = precision
+    o.device = device
+    o.epsilon = -1.0 if epsilon is None else float(epsilon)
+    o.solver = {None: 0, "hwfv1": 1, "mwdg2": 2}[solver]
+    o.dirroot = dirroot.encode() if dirroot else None
+    o.write_outputs = 1 if write_outputs else 0
+    o.verbose = 2 if timing else 0
+    return o
+
+
+class Batch:
+    """An ensemble of independent simulations stepped together (mwdg2_batch_*): one batch
+    step enqueues a time step of every unfinished member on its own stream, then waits for
+    all of them. Relative names in each .par resolve against that .par's folder."""
+
+    def __init__(self, pars: list[str], precision: int = 64, epsilon: float | None = None,
+                 solver: str | None = None, write_outputs: bool = False, device: int = -1, timing: bool = False):
+        self.pars = [os.path.abspath(p) for p in pars]
+        o = _opts(precision, epsilon, solver, None, write_outputs, device, timing)
+        arr = (ctypes.c_char_p * len(self.pars))(*[p.encode() for p in self.pars])
+        h = ctypes.c_void_p()
+        _check(lib().mwdg2_batch_create(len(self.pars), arr, ctypes.byref(o), ctypes.byref(h)))
+        self._h = h
+        self.precision = precision
+
+    def __len__(self):
+        return len(self.pars)
+
+    def step(self) -> tuple[int, np.ndarray, np.ndarray]:
+        """(members stepped, next dt per member, leaves per member); 0 members when all are done."""
+        n = len(self.pars)
+        dts = np.zeros(n)
+        leaves = np.zeros(n, np.int64)
+        k = ctypes.c_int32()
+        _check(lib().mwdg2_batch_step(self._h, _p(dts, ctypes.c_double), _p(leaves, ctypes.c_int64), ctypes.byref(k)))
+        return k.value, dts, leaves
+
+    def run(self, max_batch_steps: int = 0) -> tuple[int, int, int]:
+        """(batch steps, member steps, leaf updates) until every member is done."""
+        bs, ms, upd = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        _check(lib().mwdg2_batch_run(self._h, max_batch_steps, ctypes.byref(bs), ctypes.byref(ms), ctypes.byref(upd)))
+        return bs.value, ms.value, upd.value
+
+    def member(self, i: int) -> Simulation:
+        h = ctypes.c_void_p()
+        _check(lib().mwdg2_batch_member(self._h, i, ctypes.byref(h)))
+        return Simulation._view(h, self.pars[i], self.precision, self)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().mwdg2_batch_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def run_simulation(argv: list[str]) -> int:

@@ -125,6 +125,42 @@ mwdg2_status mwdg2_last_step_counters(mwdg2_sim* sim, int64_t* out, int n);
 
 void mwdg2_destroy(mwdg2_sim* sim);
 
+/* ---------------------------------------------------------------- batched ensembles
+ * Several independent simulations advanced together, for ensembles of scenarios (different
+ * DEMs, inflows, Manning n, epsilon). The reference runs one case per process; the
+ * `mwdg2_batch_create(n, pars, ...)` / `mwdg2_batch_step` pair is this library's way to run
+ * many. Each member keeps its own device state and CUDA stream. A batch step advances the
+ * clock of every unfinished member, enqueues one time step of each from a few host threads
+ * without waiting, then waits for all of them, so the members' kernels overlap on the GPU
+ * and small members fill SMs that one alone would leave idle. Members may differ in size,
+ * solver and end time; all take the options given at creation. Relative file names inside
+ * each member's .par, and its dirroot, resolve against that .par's folder (a single
+ * simulation resolves them against the working directory, as the reference does);
+ * mwdg2_batch_create changes the working directory while it reads each member, so call it
+ * while no other thread depends on the working directory. Members write their output files
+ * like mwdg2_run. */
+typedef struct mwdg2_batch mwdg2_batch;
+
+mwdg2_status mwdg2_batch_create(int n, const char* const* par_paths, const mwdg2_opts* opts, mwdg2_batch** out);
+
+/* One time step of every member that has not reached its sim_time. dts and leaves (n
+ * entries each, either may be NULL) receive each member's next dt and leaf count (0 and 0
+ * for members already done); *active (may be NULL) the number of members stepped.
+ * Returns MWDG2_DONE when every member is done; on an error, the first failing member's
+ * status, with mwdg2_last_error naming the member. */
+mwdg2_status mwdg2_batch_step(mwdg2_batch* b, double* dts, int64_t* leaves, int32_t* active);
+
+/* Batch steps until every member is done (max_batch_steps <= 0: no limit): batch steps
+ * taken, member steps taken and leaf updates summed over members. */
+mwdg2_status mwdg2_batch_run(mwdg2_batch* b, int64_t max_batch_steps, int64_t* batch_steps, int64_t* member_steps,
+                             int64_t* updates);
+
+/* Member i as a simulation handle for the getters above (mwdg2_info, mwdg2_get_state, ...).
+ * The batch owns it: do not pass it to mwdg2_destroy or step it on its own. */
+mwdg2_status mwdg2_batch_member(mwdg2_batch* b, int i, mwdg2_sim** out);
+
+void mwdg2_batch_destroy(mwdg2_batch* b);
+
 /* Leaf topology from significance flags, allocating no device memory. No counterpart in
  * the reference: it is for callers that cannot call cudaMalloc -- code running under a
  * memory manager that owns all device memory (a framework that reserves the device heap

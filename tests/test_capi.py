@@ -76,3 +76,17 @@ def test_static_topology_argument_errors(sig_addr, level, cap, needle):
     assert st == 6
     assert needle in mwdg2_b200.lib().mwdg2_last_error().decode()
     assert n.value == -1
+
+
+def test_batch_argument_errors(tmp_path):
+    """Batch creation checks its arguments and names the failing member; a member whose
+    .par is missing fails while reading, before any device work."""
+    lib = mwdg2_b200.lib()
+    h = ctypes.c_void_p()
+    assert lib.mwdg2_batch_create(0, None, None, ctypes.byref(h)) == 6
+    missing = str(tmp_path / "nope.par").encode()
+    arr = (ctypes.c_char_p * 1)(missing)
+    assert lib.mwdg2_batch_create(1, arr, None, ctypes.byref(h)) == 1
+    assert "batch member 0" in lib.mwdg2_last_error().decode()
+    assert lib.mwdg2_batch_step(None, None, None, None) == 6
+    assert lib.mwdg2_batch_member(None, 0, ctypes.byref(h)) == 6
