@@ -302,7 +302,7 @@ template <typename T> struct StateMax
 // latency-bound on its gathers, so its registers are capped for more resident warps
 // (FP32: 40, 6 blocks per SM; FP64: 80, 3 blocks).
 template <typename T, int STAGE>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 6 : 3) k_stage_classify(Leaves<T> lf, Hier<T> hin, Hier<T> hout, Scalars<T>* sc,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 5 : 3) k_stage_classify(Leaves<T> lf, Hier<T> hin, Hier<T> hout, Scalars<T>* sc,
                                                         Params<T> P, Bnd<T> B, T dt, bool friction, int32_t* wet)
 {
     const int n = sc->n_leaves;
@@ -319,17 +319,44 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 6 : 3) k_stage_classify(
             int32_t nid[4];
 #pragma unroll
             for (int d = 0; d < 4; ++d) nid[d] = lf.nb[d][i];
-            T h0 = hin.s[0][0][a] - hin.s[3][0][a];
-            T qx0 = hin.s[1][0][a], qy0 = hin.s[2][0][a];
-            const T z0 = hin.s[3][0][a];
+            // Everything a dry leaf needs is loaded before the dry test (almost every leaf
+            // is dry where this kernel runs), so the loads are in flight together.
+            T c[4][3];                     // own coefficients [field][mode]; stage 2: mode 0 + bed
+            T u[9];                        // stage 2: U^n
+#pragma unroll
+            for (int m = 0; m < 3; ++m)
+            {
+                c[3][m] = hin.s[3][m][a];
+                if (STAGE == 1 || m == 0)
+                {
+                    c[0][m] = hin.s[0][m][a];
+                    c[1][m] = hin.s[1][m][a];
+                    c[2][m] = hin.s[2][m][a];
+                }
+            }
+            if (STAGE == 2)
+            {
+#pragma unroll
+                for (int k = 0; k < 9; ++k) u[k] = lf.un[k][i];
+            }
+            T nbh[4];
+#pragma unroll
+            for (int d = 0; d < 4; ++d)
+                nbh[d] = (nid[d] != -1) ? hin.s[0][0][nid[d]] - hin.s[3][0][nid[d]] : T(0.0);
+            T h0 = c[0][0] - c[3][0];
+            T qx0 = c[1][0], qy0 = c[2][0];
+            const T z0 = c[3][0];
             T gh[4], gqx[4], gqy[4];
             ghost_pass(h0, qx0, qy0, z0, nid, level, a, P, B, dt, gh, gqx, gqy);
-            is_wet = !leaf_is_dry(hin, h0, nid, gh, P.tol_h);
-            any_dry |= !is_wet;
-            if (!is_wet)
+            // the dry rule of leaf_is_dry
+            bool dry = h0 < P.tol_h;
+#pragma unroll
+            for (int d = 0; d < 4; ++d) dry = dry && ((nid[d] != -1) ? nbh[d] : gh[d]) < P.tol_h;
+            is_wet = !dry;
+            any_dry |= dry;
+            if (dry)
             {
-                const T z[3] = {z0, hin.s[3][1][a], hin.s[3][2][a]};
-                T u[9];
+                const T z[3] = {c[3][0], c[3][1], c[3][2]};
                 if (STAGE == 1)
                 {
                     if (friction) { qx0 = T(0.0); qy0 = T(0.0); }
@@ -337,17 +364,15 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 6 : 3) k_stage_classify(
 #pragma unroll
                     for (int m = 1; m < 3; ++m)
                     {
-                        u[m] = hin.s[0][m][a] - z[m];
-                        u[3 + m] = hin.s[1][m][a];
-                        u[6 + m] = hin.s[2][m][a];
+                        u[m] = c[0][m] - z[m];
+                        u[3 + m] = c[1][m];
+                        u[6 + m] = c[2][m];
                     }
 #pragma unroll
                     for (int k = 0; k < 9; ++k) lf.un[k][i] = u[k];
                 }
                 else
                 {
-#pragma unroll
-                    for (int k = 0; k < 9; ++k) u[k] = lf.un[k][i];
                     mx.add(u, z0);
                     if (P.dt_leaf) P.dt_leaf[i] = P.initial_tstep;
                 }
