@@ -297,7 +297,7 @@ __device__ __forceinline__ void encode_parent(const Hier<T>& hr, const Scalars<T
         }
         ++n_done;
     }
-    hr.flags[p] = nf;
+    if (nf != f) hr.flags[p] = nf;   // most large-level parents keep their flags
 }
 
 // Small levels are processed in bands of up to kBandDepth levels, one CTA per node of the
