@@ -143,7 +143,7 @@ class Clocks:
 # divided by the leaves) from ncu captures of the same workload at max_ref_lvl 11 (1.2 M
 # leaves; the traffic grows with the leaves). Keyed by (solver, P, timing phase).
 TRAFFIC_SOURCE = "ncu, fBm catchment 2048^2 (max_ref_lvl 11), scaled by leaves"
-TRAFFIC_B_PER_LEAF: dict = {}
+TRAFFIC_B_PER_LEAF: dict = {("mwdg2", 4, 3): 2.7, ("mwdg2", 4, 4): 191.7, ("mwdg2", 4, 6): 152.5}
 
 
 def peaks() -> tuple[float, str]:
