@@ -47,6 +47,10 @@ def parse():
     ap.add_argument("--cpu-steps", type=int, default=2, help="timed oracle steps for cpu_baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--case-dir", default=None)
+    ap.add_argument("--workload", default="catchment", choices=["catchment", "ensemble"],
+                    help="ensemble: a batch of seeded uneven scenarios (mwdg2_batch_*) against the same "
+                         "members stepped one after another; prints its own line")
+    ap.add_argument("--members", type=int, default=64)
     return ap.parse_args()
 
 
@@ -199,10 +203,78 @@ def run_reference(a):
     print(json.dumps(line), flush=True)
 
 
+def run_ensemble(a):
+    """Batched ensemble: `--members` seeded scenarios (512^2 to 2048^2 fBm catchments, dam
+    breaks or point inflows, Manning n and epsilon drawn per member) advanced together by
+    mwdg2_batch_step, against the same members each stepped alone, one after another. Both
+    are timed on the host clock around synchronised loops (the batch has one stream per
+    member); a step of a member updates its leaves once. Every member takes W warm-up steps,
+    then K timed steps (members that reach their end time stop earlier)."""
+    import numpy as np
+    import torch
+    import cases
+    import mwdg2_b200
+    torch.cuda.set_device(0)
+    base = a.case_dir or os.path.join(tempfile.gettempdir(), "mwdg2_bench_cases")
+    root = os.path.join(base, f"ensemble-{a.members}-{a.solver}-v1")
+    if not os.path.exists(os.path.join(root, "READY")):
+        os.makedirs(root, exist_ok=True)
+        cases.ensemble(root, n=a.members, solver=a.solver)
+        open(os.path.join(root, "READY"), "w").close()
+    pars = sorted(os.path.join(root, d, "case.par") for d in os.listdir(root) if d.startswith("member"))
+    sizes = [1 << (int(open(p).read().split("max_ref_lvl")[1].split()[0])) for p in pars]
+
+    with mwdg2_b200.Batch(pars, precision=a.precision) as b:
+        for _ in range(a.warmup):
+            b.step()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        upd, member_steps = 0, 0
+        for _ in range(a.steps):
+            k, _, n = b.step()
+            upd += int(n.sum())
+            member_steps += k
+        torch.cuda.synchronize()
+        t_batch = time.perf_counter() - t0
+
+    t_seq, upd_seq = 0.0, 0
+    for p in pars:
+        s = mwdg2_b200.Simulation(p, precision=a.precision)
+        for _ in range(a.warmup):
+            s.step()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(a.steps):
+            ok, _, n = s.step()
+            if not ok:
+                break
+            upd_seq += n
+        torch.cuda.synchronize()
+        t_seq += time.perf_counter() - t0
+        s.close()
+    line = {"metric": "active-cell updates/s (batched ensemble of adaptive MWDG2 time steps)",
+            "value": upd / t_batch, "unit": UNIT, "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+            "higher_is_better": True, "impl": "ours-batch", "dtype": f"f{a.precision}",
+            "data": "synthetic (seeded fBm DEMs, no network)",
+            "config": {"workload": f"ensemble of {a.members} seeded scenarios: finest grids 512^2/1024^2/2048^2 "
+                                   "(uniform), fBm Hurst U(0.6,0.9), dam break (radius U(0.05,0.25) x domain, "
+                                   "2.5/0.5 m) or point inflow (peak U(5,40) m3/s), n U(0.01,0.05), "
+                                   "epsilon {1e-3,1e-4}", "solver": a.solver, "members": len(pars),
+                       "grids": {str(m): sizes.count(m) for m in sorted(set(sizes))},
+                       "timing": "host clock around synchronised loops"},
+            "batch": {"seconds": t_batch, "member_steps": member_steps, "leaf_updates": upd},
+            "sequential": {"value": upd_seq / t_seq, "seconds": t_seq, "leaf_updates": upd_seq},
+            "batch_over_sequential": (upd / t_batch) / (upd_seq / t_seq)}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+        return
+    if a.workload == "ensemble":
+        run_ensemble(a)
         return
     import numpy as np
     import torch

@@ -13,6 +13,8 @@ implementation sees byte-identical inputs. Generators:
 * fbm_catchment       - fractional-Brownian-motion DEM, dry start, west-edge point
                         inflow with a triangular hydrograph (4096^2 benchmark case).
 * lake_at_rest        - still water over an fBm bed (well-balancing checks).
+* ensemble            - seeded mix of fBm catchments with dam breaks or point inflows
+                        of uneven sizes (batched-ensemble benchmark).
 
 Reference quirks the generators respect (they would otherwise change the physics):
 * `wall_height` is set above every bed value, because `operators/dg2_update.cu:46`
@@ -277,3 +279,43 @@ def lake_at_rest(directory: str, L: int = 7, solver: str = "mwdg2", eps: float =
     _write_par(par, lines)
     return Case(par=par, directory=directory, L=L, solver=solver, cellsize=cellsize,
                 sim_time=sim_time, dem=dem, start_h=h, meta={"kind": "lake_at_rest"})
+
+
+def ensemble(root: str, n: int = 64, seed: int = 20261203, levels: tuple[int, ...] = (9, 10, 11),
+             solver: str = "mwdg2", sim_time: float = 600.0, cellsize: float = 2.0) -> list[Case]:
+    """Seeded ensemble of uneven scenarios, one folder each under `root`.
+
+    Member i draws (PCG64 stream `seed`): max_ref_lvl uniformly from `levels`; an fBm DEM
+    with Hurst ~ U(0.6, 0.9) over 0-30 m; with equal chance a dam break (depth 2.5 m inside
+    a radius ~ U(0.05, 0.25) x domain around a random centre, 0.5 m outside, no inflow) or a
+    dry start with a west-edge point inflow peaking at ~ U(5, 40) m^3/s at 300 s; Manning
+    n ~ U(0.01, 0.05); epsilon 1e-3 or 1e-4.
+    """
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        L = int(rng.choice(levels))
+        hurst = float(rng.uniform(0.6, 0.9))
+        manning = float(rng.uniform(0.01, 0.05))
+        eps = float(rng.choice([1e-3, 1e-4]))
+        dam = bool(rng.integers(0, 2))
+        m = 1 << L
+        d = os.path.join(root, f"member{i:03d}")
+        if dam:
+            ext = m * cellsize
+            radius = float(rng.uniform(0.05, 0.25)) * ext
+            cx, cy = rng.uniform(0.25, 0.75, size=2) * ext
+            c = (np.arange(m) + 0.5) * cellsize
+            X, Y = np.meshgrid(c, c)
+            depth = np.where(np.hypot(X - cx, Y - cy) < radius, 2.5, 0.5)
+            case = fbm_catchment(d, L=L, solver=solver, eps=eps, sim_time=sim_time, cellsize=cellsize,
+                                 hurst=hurst, manning=manning, peak_q=0.0, t_peak=300.0,
+                                 seed=seed + i, start_depth=depth)
+        else:
+            peak = float(rng.uniform(5.0, 40.0))
+            case = fbm_catchment(d, L=L, solver=solver, eps=eps, sim_time=sim_time, cellsize=cellsize,
+                                 hurst=hurst, manning=manning, peak_q=peak, t_peak=300.0, seed=seed + i)
+        case.meta.update({"member": i, "kind": "dam_break" if dam else "inflow", "eps": eps, "manning": manning})
+        out.append(case)
+    return out
+
