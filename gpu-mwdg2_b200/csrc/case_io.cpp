@@ -258,8 +258,9 @@ bool Case<T>::read(const std::string& par, double eps_override, int solver_overr
     ymax = ymin + ysz * cellsize;
     sim_time = kf.real<T>("sim_time");
     manning = kf.real<T>("fpfric");
-    if (kf.has("monai") || kf.has("oregon-seaside"))
-        return fail(2, "the monai / oregon-seaside boundary specials are not supported");
+    // classes/SimulationParams.cpp:31-32 (monai wins when both are present, as in
+    // neighbours/add_ghost_cells.cu:450-471)
+    west_special = kf.has("monai") ? 1 : (kf.has("oregon-seaside") ? 2 : 0);
     const int M = 1 << L;
     if (xsz <= 0 || ysz <= 0 || xsz > M || ysz > M) return fail(2, "DEM size must be within 2^max_ref_lvl");
     // input/read_cell_size.cpp:5-41 (fifth header value)

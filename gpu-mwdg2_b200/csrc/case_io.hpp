@@ -58,6 +58,7 @@ template <typename T> struct Case
     T initial_tstep = T(0), epsilon = T(0), tol_h = T(1e-3), tol_q = T(0), tol_s = T(1e-9);
     T wall_height = T(0), CFL = T(0.3), tol_Krivo = T(9999.0);
     bool limitslopes = false, refine_wall = false, startq2d = false;
+    int west_special = 0;             // west HFIX/HVAR ghost: 1 monai, 2 oregon-seaside (SimulationParams.h:29-30)
     int ref_thickness = 0;
     // classes/SimulationParams.h:8-32
     T xmin = T(0), ymin = T(0), xmax = T(0), ymax = T(0), g = T(9.80665), sim_time = T(0), manning = T(0);

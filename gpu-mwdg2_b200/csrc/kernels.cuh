@@ -58,6 +58,8 @@ template <typename T> struct Bnd
 {
     int start[4], end[4], type[4];   // N, E, S, W
     T inlet[4];
+    int west_special;                // 1 monai, 2 oregon-seaside wave makers on the west side
+    T time;                          // simulated time of the step (oregon-seaside wave maker)
 };
 
 template <typename T> struct Src { int code, type; T value; };

@@ -234,6 +234,8 @@ template <typename T> mw::Bnd<T> Sim<T>::bnd_now() const
         b.type[d] = cs_.bnd[d].type;
         b.inlet[d] = cs_.bnd[d].inlet;
     }
+    b.west_special = cs_.west_special;
+    b.time = time_;
     return b;
 }
 

@@ -29,6 +29,50 @@ template <typename T, bool MW> __device__ __forceinline__ void load_cell(const H
     }
 }
 
+// Non-reflecting wave maker of the Monai valley benchmark (operators/non_reflective_wave.cuh:
+// 15-94): the characteristic reaching the boundary cell is traced back over one step by
+// Newton's method (at most 101 iterations); the outgoing invariant there and the incoming
+// one set by the target level h_inlet (still water 0.13535 m) give the boundary depth and
+// velocity. The arithmetic follows the reference term by term, so both builds agree.
+template <typename T>
+__device__ __forceinline__ void monai_inflow(T h_inlet, T dt, T dxl, T hp, T up, T hb, T ub, T g, T& h_out, T& u_out)
+{
+    const T tol = T(1e-6), xa = -dxl / T(2.0);
+    T p0 = dxl / T(2.0), p1 = p0 - dxl / T(2.0), dp = T(0.0), f1 = T(0.0);
+    T f0 = (p0 - xa) + dt * ((ub - (p0 - xa) / dxl * (ub - up)) - sqrt(g * (hb - (p0 - xa) / dxl * (hb - hp))));
+    int cond = 0;
+    for (int k = 0; k <= 100 && cond == 0; ++k)
+    {
+        const T df = T(1.0) + dt * ((up - ub) / dxl - T(0.5) * pow((g * (hb - (p0 - xa) / dxl * (hb - hp))), T(-0.5)) *
+                                                         (g * (hp - hb) / dxl));
+        if (fabs(df) <= T(0.0))
+        {
+            cond = 1;   // zero slope: keep the current point
+            dp = p1 - p0;
+            p1 = p0;
+        }
+        else
+        {
+            dp = f0 / df;
+            p1 = p0 - dp;
+        }
+        f1 = (p1 - xa) + dt * ((ub - (p1 - xa) / dxl * (ub - up)) - sqrt(g * (hb - (p1 - xa) / dxl * (hb - hp))));
+        const T relerr = fabs(dp) / (fabs(p1) + T(0.0));
+        if (relerr < tol) cond = 2;
+        if (fabs(f1) < tol) cond = 3;
+        if (relerr <= tol && fabs(f1) < tol) cond = 4;
+        p0 = p1;
+        f0 = f1;
+    }
+    const T hr = hb - (hb - hp) * (p1 - xa) / dxl;
+    const T ur = ub - (ub - up) * (p1 - xa) / dxl;
+    const T cr = sqrt(g * hr);
+    const T beta_minus = ur - T(2.0) * cr;
+    const T beta_plus = T(2.0) * sqrt(g * (h_inlet + T(0.13535))) + h_inlet * sqrt(g / T(0.13535));
+    h_out = T(1.0) / T(16.0) / g * (beta_plus - beta_minus) * (beta_plus - beta_minus);
+    u_out = T(0.5) * (beta_plus + beta_minus);
+}
+
 // Ghost cells of a leaf at the domain border, raster cases
 // (neighbours/add_ghost_cells.cu:18-500): directions N, E, S, W in order; a fine
 // boundary cell of an HFIX/HVAR/QFIX/QVAR segment also resets the leaf's own depth.
@@ -59,6 +103,23 @@ __device__ __forceinline__ void ghost_pass(T& own_h0, T own_qx0, T own_qy0, T ow
             gh[d] = pow((q * q) / P.g, T(1.0) / T(3.0));
             gqx[d] = own_qx0;
             gqy[d] = own_qy0;
+        }
+        else if ((t == HFIX || t == HVAR) && d == 3 && B.west_special == 1)
+        {
+            // monai: the ghost carries the wave maker's state, the leaf keeps its own
+            const T up = (own_h0 > P.tol_h) ? own_qx0 / own_h0 : T(0.0);
+            T hb, ub;
+            monai_inflow(B.inlet[d], dt, P.dx, own_h0, up, T(0.13535), T(0.0), P.g, hb, ub);
+            gh[d] = hb - own_z0;
+            gqx[d] = hb * ub;
+        }
+        else if ((t == HFIX || t == HVAR) && d == 3 && B.west_special == 2)
+        {
+            // oregon-seaside: wave-maker speed s(t), the ghost reflects the leaf's velocity about 2s
+            gh[d] = own_h0;
+            const T s = T(0.6) * exp(-T(0.25) * (B.time - T(14.75)) * (B.time - T(14.75)));
+            const T v0 = (own_h0 > P.tol_h) ? own_qx0 / own_h0 : T(0.0);
+            gqx[d] = ((T(2.0) * s - v0) * gh[d]);
         }
         else if (t == HFIX || t == HVAR)
         {
