@@ -297,7 +297,9 @@ def main():
         torch.cuda.synchronize()
 
     par = make_case(a, rank)
+    t_init = time.perf_counter()
     sim = mwdg2_b200.Simulation(par, precision=a.precision, device=local, timing=True)
+    t_init = time.perf_counter() - t_init   # reading the rasters + device initialisation
     clk = Clocks(local).__enter__()   # sampled from the warm-up through the end-to-end loop
     for _ in range(a.warmup):
         sim.step()
@@ -396,6 +398,7 @@ def main():
             "phase_ms_mean": dict(zip(("step_begin_srcs", "encode", "decode", "topology", "stage1",
                                        "reencode", "stage2", "step"), [round(x, 4) for x in mean_ph])),
             "leaves_mean": n_mean,
+            "init_s": t_init,
             "wet_fraction": [float(np.mean([cc[k] for cc in counters])) / n_mean for k in ("wet_stage1", "wet_stage2")]}
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(par, a, a.cpu_steps)

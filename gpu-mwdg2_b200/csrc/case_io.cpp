@@ -397,7 +397,7 @@ bool Case<T>::read(const std::string& par, double eps_override, int solver_overr
         for (int j = 0; j < ref_thickness; ++j) for (int i = 0; i < ysz; ++i) mark(morton(xsz - 1 - j, i));
     }
 
-    // initial modes: rasters -> nodes -> modal projection (DG2) or direct (FV1), row-major
+    // initial rasters (h, qx, qy, z), row-major as read
     const size_t F = (size_t)M * M;
     std::vector<T> hr(F, T(0)), qxr(F, T(0)), qyr(F, T(0)), zr(F, wall_height);
     const std::string start = kf.str("startfile");
@@ -413,62 +413,9 @@ bool Case<T>::read(const std::string& par, double eps_override, int solver_overr
         read_raster<T>(start + ".Qx", qxr, M, wall_height, e2);
         read_raster<T>(start + ".Qy", qyr, M, wall_height, e2);
     }
-    const bool mw = (solver == 2);
-    const int nfields = mw ? 12 : 4;
-    for (int f = 0; f < nfields; ++f) fine[f].assign(F, T(0));
-    // Z-order placement of the finest modes (zorder/get_sorting_indices.cu,
-    // zorder/sort_finest_scale_coeffs_z_order.cu): cell (x, y) goes to slot morton(x, y)
-    if (!mw)
-    {
-        const std::vector<T>* src[4] = {&hr, &qxr, &qyr, &zr};
-        for (int y = 0; y < M; ++y)
-            for (int x = 0; x < M; ++x)
-            {
-                const size_t rmi = (size_t)y * M + x, zi = (size_t)morton(x, y);
-                for (int f = 0; f < 4; ++f) fine[f][zi] = (*src[f])[rmi];
-            }
-    }
-    else
-    {
-        const int ID = M + 1, ix = xsz + 1, iy = ysz + 1;
-        // node arrays (input/read_and_project_modes_dg2.cu:60-78): last interior row and
-        // column of the DEM extent and of the mesh repeat the neighbouring raster cell
-        std::vector<T> nh((size_t)ID * ID), nqx((size_t)ID * ID), nqy((size_t)ID * ID), nz((size_t)ID * ID);
-        for (int y = 0; y < ID; ++y)
-            for (int x = 0; x < ID; ++x)
-            {
-                const int i = (x == ix - 1 || x == ID - 1) ? x - 1 : x;
-                const int j = (y == iy - 1 || y == ID - 1) ? y - 1 : y;
-                const size_t ni = (size_t)(ID - 1 - y) * ID + x, mi = (size_t)(M - 1 - j) * M + i;
-                nh[ni] = hr[mi]; nqx[ni] = qxr[mi]; nqy[ni] = qyr[mi]; nz[ni] = zr[mi];
-            }
-        std::vector<T>().swap(hr); std::vector<T>().swap(qxr); std::vector<T>().swap(qyr); std::vector<T>().swap(zr);
-        // mra/modal_projections.cu:28-88 (row-major cell idx -> Z-ordered slot)
-        const T s3x4 = T(4.0) * std::sqrt(T(3.0));
-        const std::vector<T>* nodal[4] = {&nh, &nqx, &nqy, &nz};
-        for (int y = 0; y < M; ++y)
-            for (int x = 0; x < M; ++x)
-            {
-                const size_t SW = (size_t)y * ID + x, SE = SW + 1, NW = (size_t)(y + 1) * ID + x, NE = NW + 1;
-                const size_t zi = (size_t)morton(x, y);
-                for (int f = 0; f < 4; ++f)
-                {
-                    const std::vector<T>& a = *nodal[f];
-                    fine[f][zi] = T(0.25) * (a[NW] + a[NE] + a[SE] + a[SW]);
-                    fine[4 + f][zi] = (a[NE] - a[NW] + a[SE] - a[SW]) / s3x4;
-                    fine[8 + f][zi] = (a[NE] - a[SE] + a[NW] - a[SW]) / s3x4;
-                }
-            }
-    }
-    // mra/insert_point_srcs.cu:3-29 -- affects only the first step's maxima; the HFIX/HVAR
-    // branch subtracts the bed of the cell whose Z-index equals the source's index
-    h0_for_maxes = fine[0];
-    for (size_t i = 0; i < srcs.size(); ++i)
-    {
-        const auto& s = srcs[i];
-        if (s.type == 4 || s.type == 8) h0_for_maxes[s.code] = s.value - fine[3][i];
-        else if (s.type == 16 || s.type == 32) h0_for_maxes[s.code] += s.value * dt0 / dx;
-    }
+    // the modal projection, Z-order placement and initial point-source insertion run on the
+    // device (init.cuh)
+    raster[0].swap(hr); raster[1].swap(qxr); raster[2].swap(qyr); raster[3].swap(zr);
     return true;
 }
 

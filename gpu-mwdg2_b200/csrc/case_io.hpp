@@ -78,8 +78,7 @@ template <typename T> struct Case
 
     // initial state
     std::vector<uint8_t> preflag;     // get_lvl_idx(L) bytes
-    std::vector<T> fine[12];          // Z-ordered finest modes: h0 qx0 qy0 z0 h1x qx1x qy1x z1x h1y qx1y qy1y z1y
-    std::vector<T> h0_for_maxes;      // fine h0 after the initial point-source insertion
+    std::vector<T> raster[4];         // h, qx, qy, z as read: row-major M x M (k_init_finest projects them)
 
     std::string error;
     int error_kind = 0;               // 1 IO, 2 PARSE

@@ -12,6 +12,7 @@
 // point-source values (when there are sources) and the scalar read-back.
 #include "../../include/mwdg2.h"
 #include "case_io.hpp"
+#include "init.cuh"
 #include "outputs.cuh"
 #include "solver.cuh"
 
@@ -312,28 +313,33 @@ template <typename T> mwdg2_status Sim<T>::init(const char* par, const mwdg2_opt
         CU(cudaMemcpyAsync(d_stage_codes_, cs_.stage_codes.data(), sizeof(int32_t) * nst, cudaMemcpyHostToDevice, st_));
     }
 
-    // finest level of the hierarchy (zorder/copy_finest_coefficients.cu:3-35)
+    // finest level of the hierarchy and the initial leaf state, projected on the device from
+    // the rasters (zorder/copy_finest_coefficients.cu:3-35; init.cuh)
     {
         const int fin = mw::lvl_idx(L_);
-        std::vector<T> tmp(F_);
-        for (int m = 0; m < modes; ++m)
+        T* d_raster = nullptr;
+        CU(cudaMalloc(&d_raster, sizeof(T) * 4 * F_));
+        for (int f = 0; f < 4; ++f)
         {
-            const std::vector<T>& h = cs_.fine[4 * m + 0];
-            const std::vector<T>& qx = cs_.fine[4 * m + 1];
-            const std::vector<T>& qy = cs_.fine[4 * m + 2];
-            const std::vector<T>& z = cs_.fine[4 * m + 3];
-            for (int64_t k = 0; k < F_; ++k) tmp[k] = h[k] + z[k];
-            CU(cudaMemcpy(hr_.s[0][m] + fin, tmp.data(), sizeof(T) * F_, cudaMemcpyHostToDevice));
-            CU(cudaMemcpy(hr_.s[1][m] + fin, qx.data(), sizeof(T) * F_, cudaMemcpyHostToDevice));
-            CU(cudaMemcpy(hr_.s[2][m] + fin, qy.data(), sizeof(T) * F_, cudaMemcpyHostToDevice));
-            CU(cudaMemcpy(hr_.s[3][m] + fin, z.data(), sizeof(T) * F_, cudaMemcpyHostToDevice));
-            // initial leaf state (all finest cells): h of mode 0 carries the initial
-            // point-source insertion, which only the first step's maxima see
-            const std::vector<T>& h_leaf = (m == 0) ? cs_.h0_for_maxes : h;
-            CU(cudaMemcpy(lf_.un[0 + m], h_leaf.data(), sizeof(T) * F_, cudaMemcpyHostToDevice));
-            CU(cudaMemcpy(lf_.un[3 + m], qx.data(), sizeof(T) * F_, cudaMemcpyHostToDevice));
-            CU(cudaMemcpy(lf_.un[6 + m], qy.data(), sizeof(T) * F_, cudaMemcpyHostToDevice));
+            cudaError_t e = cudaMemcpy(d_raster + (size_t)f * F_, cs_.raster[f].data(), sizeof(T) * F_, cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) { cudaFree(d_raster); CU(e); }
+            std::vector<T>().swap(cs_.raster[f]);
         }
+        const int grid = grid_for(F_, 256, 1 << 20);
+        if (mw_) mw::k_init_finest<T, true><<<grid, 256, 0, st_>>>(d_raster, M_, cs_.xsz, cs_.ysz, hr_, lf_, fin);
+        else mw::k_init_finest<T, false><<<grid, 256, 0, st_>>>(d_raster, M_, cs_.xsz, cs_.ysz, hr_, lf_, fin);
+        const int nsrc0 = (int)cs_.srcs.size();
+        if (nsrc0 > 0)
+        {
+            // source values at t = 0.001, as the reference's PointSources constructor reads them
+            for (int i = 0; i < nsrc0; ++i) h_src_[i] = mw::Src<T>{cs_.srcs[i].code, cs_.srcs[i].type, cs_.srcs[i].value};
+            CU(cudaMemcpyAsync(d_src_, h_src_, sizeof(mw::Src<T>) * nsrc0, cudaMemcpyHostToDevice, st_));
+            mw::k_init_point_srcs<T><<<1, 1, 0, st_>>>(lf_, hr_, d_src_, nsrc0, T(0.001), cs_.dx, fin);
+        }
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st_);
+        cudaFree(d_raster);
+        CU(e);
     }
     // flags: all significant (mra/init_sig_details.cu) plus preflags
     {
@@ -341,9 +347,6 @@ template <typename T> mwdg2_status Sim<T>::init(const char* par, const mwdg2_opt
         for (int i = 0; i < n_det_; ++i) fl[i] = mw::F_SIG | (cs_.preflag[i] ? mw::F_PRE : 0);
         CU(cudaMemcpy(hr_.flags, fl.data(), n_det_, cudaMemcpyHostToDevice));
     }
-    // release host copies of the initial grid
-    for (auto& v : cs_.fine) std::vector<T>().swap(v);
-    std::vector<T>().swap(cs_.h0_for_maxes);
 
     P_.L = L_; P_.M = M_; P_.xsz = cs_.xsz; P_.ysz = cs_.ysz; P_.limit = cs_.limitslopes ? 1 : 0;
     P_.dx = cs_.dx; P_.tol_h = cs_.tol_h; P_.tol_q = cs_.tol_q; P_.tol_s = cs_.tol_s; P_.g = cs_.g;
