@@ -64,6 +64,14 @@ template <typename T> struct Bnd
 
 template <typename T> struct Src { int code, type; T value; };
 
+// Values that change from step to step, in device memory: the step's first operation copies
+// them from pinned host memory, so a captured step replays with new values.
+template <typename T> struct StepArgs
+{
+    T dt;        // the step's time step
+    Bnd<T> B;    // boundary segments, inlet values and time at this step
+};
+
 // ---------------------------------------------------------------- atomics on non-negative reals
 __device__ __forceinline__ void atomic_max_nn(double* a, double v)
 {
@@ -177,10 +185,12 @@ __global__ void __launch_bounds__(256) k_maxes_reinsert(Leaves<T> lf, Hier<T> hr
 }
 
 // Point sources into the finest level (mra/reinsert_point_srcs.cu:3-29).
-template <typename T> __global__ void k_point_sources(Hier<T> hr, const Src<T>* src, int n, T dt, T dx, int L)
+template <typename T>
+__global__ void k_point_sources(Hier<T> hr, const Src<T>* src, int n, const StepArgs<T>* args, T dx, int L)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    const T dt = args->dt;
     const int h = lvl_idx(L) + src[i].code;
     const int t = src[i].type;
     if (t == HFIX || t == HVAR) hr.s[0][0][h] = src[i].value;

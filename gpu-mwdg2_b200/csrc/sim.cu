@@ -127,6 +127,16 @@ private:
     struct Band { int lo, depth, grid; };
     std::vector<Band> bands_;
     int32_t* wet_list_ = nullptr;       // leaves that are not dry in an RK stage
+    mw::StepArgs<T>* d_args_ = nullptr; // this step's dt and boundary values (device)
+    mw::StepArgs<T>* h_args_ = nullptr; // pinned; copied to d_args_ by the step's first operation
+    // Per-leaf kernels run persistent grids (grid-stride loops): SMs x resident blocks of each
+    // kernel, so a step's launches do not depend on the leaf count and can be replayed.
+    int grid_leaf_ = 0, grid_classify_ = 0, grid_stage_ = 0;
+    // A step after the first is captured once per variant (which RK stages take the wet
+    // list) and replayed as one CUDA graph; capture failures fall back to direct launches.
+    bool use_graphs_ = true, capturing_ = false;
+    cudaGraphExec_t graphs_[4] = {};
+    int graph_launches_[4] = {};
     int64_t wet_prev_[2] = {-1, -1};    // previous step's wet-leaf count per RK stage
     mw::Src<T>* d_src_ = nullptr;
     mw::Src<T>* h_src_ = nullptr;       // pinned
@@ -156,27 +166,31 @@ private:
         return MWDG2_OK;
     }
     void release();
-    mwdg2_status launch_step();    // enqueue only
+    mwdg2_status launch_step();    // enqueue only (graph replay or direct launches)
+    mwdg2_status enqueue_device(); // the step's device work, on st_
     mwdg2_status collect_step();   // wait, timing, counters
     // One MWDG2 RK stage. When fewer than half of the leaves were wet in this stage last
-    // step, a light pass finishes the dry leaves and lists the others for the full kernel
-    // (whose grid is sized from last step's wet count); otherwise one sweep over all leaves.
-    template <int STAGE>
-    void stage(const mw::Hier<T>& hin, const mw::Hier<T>& hout, const mw::Bnd<T>& B, bool fric, int g_leaf, int g_solver)
+    // step, a light pass finishes the dry leaves and lists the others for the full kernel;
+    // otherwise one sweep over all leaves.
+    bool use_list(int stage) const
     {
-        const int64_t w = wet_prev_[STAGE - 1];
-        if (w >= 0 && 2 * w < n_leaves_)
+        const int64_t w = wet_prev_[stage - 1];
+        return w >= 0 && 2 * w < n_leaves_;
+    }
+    template <int STAGE> void stage(const mw::Hier<T>& hin, const mw::Hier<T>& hout, bool fric)
+    {
+        if (use_list(STAGE))
         {
-            mw::k_stage_classify<T, STAGE><<<g_leaf, 256, 0, st_>>>(lf_, hin, hout, sc_, P_, B, dt_, fric, wet_list_);
-            const int64_t hint = std::min<int64_t>(F_, w + w / 4 + 4096);
-            mw::k_mwdg2_stage<T, STAGE, true><<<grid_for(hint, mw::kSolverThreads, 1 << 20), mw::kSolverThreads, 0,
-                                                st_>>>(lf_, hin, hout, sc_, P_, B, dt_, fric, wet_list_);
+            mw::k_stage_classify<T, STAGE><<<grid_classify_, 256, 0, st_>>>(lf_, hin, hout, sc_, P_, d_args_, fric,
+                                                                             wet_list_);
+            mw::k_mwdg2_stage<T, STAGE, true><<<grid_stage_, mw::kSolverThreads, 0, st_>>>(lf_, hin, hout, sc_, P_,
+                                                                                          d_args_, fric, wet_list_);
             launches_ += 2;
         }
         else
         {
-            mw::k_mwdg2_stage<T, STAGE, false><<<g_solver, mw::kSolverThreads, 0, st_>>>(lf_, hin, hout, sc_, P_, B, dt_,
-                                                                                         fric, nullptr);
+            mw::k_mwdg2_stage<T, STAGE, false><<<grid_stage_, mw::kSolverThreads, 0, st_>>>(lf_, hin, hout, sc_, P_,
+                                                                                           d_args_, fric, nullptr);
             launches_ += 1;
         }
     }
@@ -218,6 +232,8 @@ template <typename T> void Sim<T>::release()
 {
     if (device_ >= 0) cudaSetDevice(device_);
     for (auto& e : ev_) if (e) { cudaEventDestroy(e); e = nullptr; }
+    for (auto& g : graphs_) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    if (h_args_) { cudaFreeHost(h_args_); h_args_ = nullptr; }
     for (void* p : allocs_) cudaFree(p);
     allocs_.clear();
     if (sc_host_) { cudaFreeHost(sc_host_); sc_host_ = nullptr; }
@@ -298,6 +314,20 @@ template <typename T> mwdg2_status Sim<T>::init(const char* par, const mwdg2_opt
     if (mwdg2_status s = dalloc(sc_, 1)) return s;
     if (mwdg2_status s = dalloc(tile_counts_, ntiles_)) return s;
     if (mw_) { if (mwdg2_status s = dalloc(wet_list_, F_)) return s; }
+    if (mwdg2_status s = dalloc(d_args_, 1)) return s;
+    CU(cudaMallocHost(&h_args_, sizeof(mw::StepArgs<T>)));
+    {
+        // persistent grids: SMs x resident blocks of the kernel
+        auto resident = [&](auto kernel, int threads) {
+            int b = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, threads, 0) != cudaSuccess || b < 1) b = 1;
+            return b;
+        };
+        grid_leaf_ = sms * resident(mw::k_maxes_reinsert<T, true>, 256);
+        grid_classify_ = sms * resident(mw::k_stage_classify<T, 1>, 256);
+        grid_stage_ = sms * (mw_ ? resident(mw::k_mwdg2_stage<T, 1, false>, mw::kSolverThreads)
+                                 : resident(mw::k_hwfv1<T>, mw::kSolverThreads));
+    }
     CU(cudaMallocHost(&sc_host_, sizeof(mw::Scalars<T>)));
     const int nsrc = (int)cs_.srcs.size();
     if (nsrc > 0)
@@ -388,37 +418,73 @@ template <typename T> mwdg2_status Sim<T>::init(const char* par, const mwdg2_opt
 
 template <typename T> mwdg2_status Sim<T>::launch_step()
 {
+    // host-side values of this step: point-source values (classes/PointSources.h:453-472)
+    // and boundary inlets (classes/Boundaries.h:28-39) at the current time, and dt
+    for (auto& src : cs_.srcs)
+        if (src.varying) src.value = src.series.at(time_);
+    for (int i = 0; i < (int)cs_.srcs.size(); ++i)
+        h_src_[i] = mw::Src<T>{cs_.srcs[i].code, cs_.srcs[i].type, cs_.srcs[i].value};
+    for (int d = 0; d < 4; ++d)
+        if (cs_.bnd[d].varying) cs_.bnd[d].inlet = cs_.bnd[d].series.at(time_);
+    h_args_->dt = dt_;
+    h_args_->B = bnd_now();
+    // the first step has its own kernels (initial maxima, full encode); later steps differ
+    // only in which RK stages take the wet list
+    if (!use_graphs_ || first_) return enqueue_device();
+    const int key = (mw_ && use_list(1) ? 1 : 0) | (mw_ && use_list(2) ? 2 : 0);
+    if (!graphs_[key])
+    {
+        cudaGraph_t g = nullptr;
+        cudaGraphExec_t ge = nullptr;
+        bool ok = cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+        capturing_ = ok;
+        const mwdg2_status st = ok ? enqueue_device() : MWDG2_OK;
+        capturing_ = false;
+        if (ok) ok = cudaStreamEndCapture(st_, &g) == cudaSuccess && st == MWDG2_OK;
+        if (ok) ok = cudaGraphInstantiate(&ge, g, 0) == cudaSuccess;
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();   // a refused capture leaves its error here; the direct path follows
+        if (!ok)
+        {
+            if (ge) cudaGraphExecDestroy(ge);
+            use_graphs_ = false;
+            return enqueue_device();
+        }
+        graphs_[key] = ge;
+        graph_launches_[key] = launches_;
+    }
+    launches_ = graph_launches_[key];
+    CU(cudaGraphLaunch(graphs_[key], st_));
+    return MWDG2_OK;
+}
+
+template <typename T> mwdg2_status Sim<T>::enqueue_device()
+{
     const bool mw = mw_;
     const T eps = cs_.epsilon;
-    auto rec = [&](int k) { if (timed_) cudaEventRecord(ev_[k], st_); };
+    // under stream capture the records must be external to become event nodes of the graph
+    auto rec = [&](int k) {
+        if (!timed_) return;
+        if (capturing_) cudaEventRecordWithFlags(ev_[k], st_, cudaEventRecordExternal);
+        else cudaEventRecord(ev_[k], st_);
+    };
     launches_ = 0;
     rec(0);
+    CU(cudaMemcpyAsync(d_args_, h_args_, sizeof(mw::StepArgs<T>), cudaMemcpyHostToDevice, st_));
     // MWDG2 after its first step: the previous step's stage 2 re-inserted the state into
     // the hierarchy and reduced its maxima, so only the point sources remain here
     const bool carry = mw && !first_;
     mw::k_step_begin<T><<<1, 1, 0, st_>>>(sc_, carry);
     ++launches_;
     const int nfix = first_ ? (int)F_ : -1;
-    // leaf count before remeshing is known exactly; after remeshing it is near the previous
-    // step's, so per-leaf grids are sized from it (grid-stride loops cover any growth)
-    const int g_prev = grid_for(n_leaves_, 256, 1 << 20);
-    const int64_t n_hint = std::min<int64_t>(F_, (int64_t)n_leaves_ + n_leaves_ / 4 + 1024);
-    const int g_leaf = grid_for(n_hint, 256, 1 << 20);
-    const int g_solver = grid_for(n_hint, mw::kSolverThreads, 1 << 20);
-    if (mw) { if (!carry) { mw::k_maxes_reinsert<T, true><<<g_prev, 256, 0, st_>>>(lf_, hr_, sc_, nfix, false); ++launches_; } }
-    else { mw::k_maxes_reinsert<T, false><<<g_prev, 256, 0, st_>>>(lf_, hr_, sc_, nfix, !first_); ++launches_; }
-    // point sources (classes/PointSources.h:453-472 on the host, then the kernel)
+    if (mw) { if (!carry) { mw::k_maxes_reinsert<T, true><<<grid_leaf_, 256, 0, st_>>>(lf_, hr_, sc_, nfix, false); ++launches_; } }
+    else { mw::k_maxes_reinsert<T, false><<<grid_leaf_, 256, 0, st_>>>(lf_, hr_, sc_, nfix, !first_); ++launches_; }
+    // point sources
     const int nsrc = (int)cs_.srcs.size();
     if (nsrc > 0)
     {
-        for (int i = 0; i < nsrc; ++i)
-        {
-            auto& s = cs_.srcs[i];
-            if (s.varying) s.value = s.series.at(time_);
-            h_src_[i] = mw::Src<T>{s.code, s.type, s.value};
-        }
         CU(cudaMemcpyAsync(d_src_, h_src_, sizeof(mw::Src<T>) * nsrc, cudaMemcpyHostToDevice, st_));
-        mw::k_point_sources<T><<<(nsrc + 127) / 128, 128, 0, st_>>>(hr_, d_src_, nsrc, dt_, cs_.dx, L_);
+        mw::k_point_sources<T><<<(nsrc + 127) / 128, 128, 0, st_>>>(hr_, d_src_, nsrc, d_args_, cs_.dx, L_);
         ++launches_;
     }
     rec(1);
@@ -453,14 +519,10 @@ template <typename T> mwdg2_status Sim<T>::launch_step()
         ++launches_;
     }
     rec(4);
-    // boundary inlets at the current time (classes/Boundaries.h:28-39)
-    for (int d = 0; d < 4; ++d)
-        if (cs_.bnd[d].varying) cs_.bnd[d].inlet = cs_.bnd[d].series.at(time_);
-    const mw::Bnd<T> B = bnd_now();
     const bool fric = cs_.manning > T(0);
     if (!mw)
     {
-        mw::k_hwfv1<T><<<g_solver, mw::kSolverThreads, 0, st_>>>(lf_, hr_, sc_, P_, B, dt_, fric);
+        mw::k_hwfv1<T><<<grid_stage_, mw::kSolverThreads, 0, st_>>>(lf_, hr_, sc_, P_, d_args_, fric);
         ++launches_;
         rec(5);
         rec(6);
@@ -468,15 +530,12 @@ template <typename T> mwdg2_status Sim<T>::launch_step()
     }
     else
     {
-        stage<1>(hr_, hs_, B, fric, g_leaf, g_solver);
+        stage<1>(hr_, hs_, fric);
         rec(5);
-        if (eps > T(0))
-        {
-            encode_tree<false>(hs_, eps);
-        }
-        if (cs_.limitslopes) { mw::k_stage2_maxh<T><<<g_leaf, 256, 0, st_>>>(lf_, hs_, sc_, P_, B, dt_); ++launches_; }
+        if (eps > T(0)) encode_tree<false>(hs_, eps);
+        if (cs_.limitslopes) { mw::k_stage2_maxh<T><<<grid_leaf_, 256, 0, st_>>>(lf_, hs_, sc_, P_, d_args_); ++launches_; }
         rec(6);
-        stage<2>(hs_, hr_, B, false, g_leaf, g_solver);
+        stage<2>(hs_, hr_, false);
         rec(7);
     }
     CU(cudaGetLastError());

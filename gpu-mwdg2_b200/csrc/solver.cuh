@@ -364,8 +364,10 @@ template <typename T> struct StateMax
 // (FP32: 40, 6 blocks per SM; FP64: 80, 3 blocks).
 template <typename T, int STAGE>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 5 : 3) k_stage_classify(Leaves<T> lf, Hier<T> hin, Hier<T> hout, Scalars<T>* sc,
-                                                        Params<T> P, Bnd<T> B, T dt, bool friction, int32_t* wet)
+                                                        Params<T> P, const StepArgs<T>* args, bool friction, int32_t* wet)
 {
+    const T dt = args->dt;
+    const Bnd<T>& B = args->B;
     const int n = sc->n_leaves;
     bool any_dry = false;
     StateMax<T> mx;
@@ -466,9 +468,11 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 5 : 3) k_stage_classify(
 // the wet list built by k_stage_classify; otherwise every leaf.
 template <typename T, int STAGE, bool LIST>
 __global__ void __launch_bounds__(kSolverThreads) k_mwdg2_stage(Leaves<T> lf, Hier<T> hin, Hier<T> hout, Scalars<T>* sc,
-                                                                Params<T> P, Bnd<T> B, T dt, bool friction,
+                                                                Params<T> P, const StepArgs<T>* args, bool friction,
                                                                 const int32_t* wet)
 {
+    const T dt = args->dt;
+    const Bnd<T>& B = args->B;
     const Hier<T>& hr = hin;
     StateMax<T> mx;
     const int n = LIST ? sc->wet[STAGE - 1] : sc->n_leaves;
@@ -652,8 +656,11 @@ __global__ void __launch_bounds__(kSolverThreads) k_mwdg2_stage(Leaves<T> lf, Hi
 
 // max |h0| of the stage-2 leaf state after ghost cells (run_simulation.cu:613-620).
 template <typename T>
-__global__ void __launch_bounds__(256) k_stage2_maxh(Leaves<T> lf, Hier<T> hr, Scalars<T>* sc, Params<T> P, Bnd<T> B, T dt)
+__global__ void __launch_bounds__(256) k_stage2_maxh(Leaves<T> lf, Hier<T> hr, Scalars<T>* sc, Params<T> P,
+                                                     const StepArgs<T>* args)
 {
+    const T dt = args->dt;
+    const Bnd<T>& B = args->B;
     const int n = sc->n_leaves;
     T mh = T(0);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
@@ -679,9 +686,11 @@ __global__ void __launch_bounds__(256) k_stage2_maxh(Leaves<T> lf, Hier<T> hr, S
 
 // operators/fv1_update.cu:3-243 with friction and ghost cells fused; in-place update.
 template <typename T>
-__global__ void __launch_bounds__(kSolverThreads) k_hwfv1(Leaves<T> lf, Hier<T> hr, Scalars<T>* sc, Params<T> P, Bnd<T> B,
-                                                          T dt, bool friction)
+__global__ void __launch_bounds__(kSolverThreads) k_hwfv1(Leaves<T> lf, Hier<T> hr, Scalars<T>* sc, Params<T> P,
+                                                          const StepArgs<T>* args, bool friction)
 {
+    const T dt = args->dt;
+    const Bnd<T>& B = args->B;
     const int n = sc->n_leaves;
     T dt_loc = (sizeof(T) == 8) ? T(1.0e308) : T(3.0e38);
     bool nan_seen = false;
