@@ -566,31 +566,67 @@ static __global__ void __launch_bounds__(kTileThreads) k_tile_count(const uint8_
     if (threadIdx.x == 0) counts[blockIdx.x] = c;
 }
 
-// Exclusive scan of n tile counts in one block; total -> sc->n_leaves.
+// Exclusive scan of n tile counts in one block of 1024 threads; total -> sc->n_leaves.
+// Thread t owns a contiguous chunk (read as int4 when chunks are multiples of four; tile
+// counts come in powers of four), warps scan their chunk sums with shuffles, and the 32 warp
+// totals are scanned by one warp.
 template <typename T> __global__ void __launch_bounds__(1024) k_tile_scan(int32_t* counts, int n, Scalars<T>* sc)
 {
-    __shared__ int32_t part[1024];
-    const int per = (n + blockDim.x - 1) / blockDim.x;
+    __shared__ int32_t warp_sum[32];
+    const int per = (n + 1023) / 1024;
     const int lo = min(n, (int)threadIdx.x * per), hi = min(n, lo + per);
+    const bool vec = (per % 4) == 0;
     int32_t s = 0;
-    for (int i = lo; i < hi; ++i) s += counts[i];
-    part[threadIdx.x] = s;
+    if (vec)
+        for (int i = lo; i < hi; i += 4)
+        {
+            const int4 v = *reinterpret_cast<const int4*>(counts + i);
+            s += v.x + v.y + v.z + v.w;
+        }
+    else
+        for (int i = lo; i < hi; ++i) s += counts[i];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int32_t incl = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1)
+    {
+        const int32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    if (lane == 31) warp_sum[w] = incl;
     __syncthreads();
-    for (int o = 1; o < (int)blockDim.x; o <<= 1)
+    if (w == 0)
     {
-        const int32_t v = (threadIdx.x >= (unsigned)o) ? part[threadIdx.x - o] : 0;
-        __syncthreads();
-        part[threadIdx.x] += v;
-        __syncthreads();
+        int32_t t = warp_sum[lane], ti = t;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1)
+        {
+            const int32_t v = __shfl_up_sync(0xffffffffu, ti, o);
+            if (lane >= o) ti += v;
+        }
+        warp_sum[lane] = ti - t;   // exclusive prefix of the warp totals
+        if (lane == 31) sc->n_leaves = ti;
     }
-    int32_t run = (threadIdx.x == 0) ? 0 : part[threadIdx.x - 1];
-    for (int i = lo; i < hi; ++i)
-    {
-        const int32_t c = counts[i];
-        counts[i] = run;
-        run += c;
-    }
-    if (threadIdx.x == blockDim.x - 1) sc->n_leaves = part[blockDim.x - 1];
+    __syncthreads();
+    int32_t run = warp_sum[w] + incl - s;   // exclusive prefix of this thread's chunk
+    if (vec)
+        for (int i = lo; i < hi; i += 4)
+        {
+            int4 v = *reinterpret_cast<const int4*>(counts + i);
+            const int4 c = v;
+            v.x = run; run += c.x;
+            v.y = run; run += c.y;
+            v.z = run; run += c.z;
+            v.w = run; run += c.w;
+            *reinterpret_cast<int4*>(counts + i) = v;
+        }
+    else
+        for (int i = lo; i < hi; ++i)
+        {
+            const int32_t c = counts[i];
+            counts[i] = run;
+            run += c;
+        }
 }
 
 // Neighbour of a leaf (level l, finest reference cell code `ref`) across the finest cell

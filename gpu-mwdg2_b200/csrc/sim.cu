@@ -511,7 +511,8 @@ template <typename T> mwdg2_status Sim<T>::enqueue_device()
     rec(3);
     if (remesh)
     {
-        mw::k_tile_count<<<ntiles_, mw::kTileThreads, 0, st_>>>(hr_.flags, L_, tile_counts_);
+        // 96 threads: the count reads 85 flag words of the tile's subtree
+        mw::k_tile_count<<<ntiles_, 96, 0, st_>>>(hr_.flags, L_, tile_counts_);
         ++launches_;
         mw::k_tile_scan<T><<<1, 1024, 0, st_>>>(tile_counts_, ntiles_, sc_);
         ++launches_;
