@@ -43,6 +43,7 @@ template <typename T> struct Scalars
     int32_t n_leaves;
     int32_t status;                   // bit 0: NaN seen in the state
     unsigned long long enc, enc2, dec;
+    uint32_t sig_level[16];           // significant parents decoded per level (levels above the bands)
     int32_t wet[2];                   // leaves not dry in RK stage 1 / stage 2 (wet-list lengths)
     T next_max[4];                    // maxima of the state at the end of the step (eta, h, qx, z)
 };
@@ -143,6 +144,8 @@ template <typename T> __global__ void k_step_begin(Scalars<T>* sc, bool carry)
     sc->dt_min = (sizeof(T) == 8) ? T(1.0e308) : T(3.0e38);
     sc->enc = 0; sc->enc2 = 0; sc->dec = 0;
     sc->wet[0] = 0; sc->wet[1] = 0;
+#pragma unroll
+    for (int l = 0; l < 16; ++l) sc->sig_level[l] = 0;
 }
 
 // Maxima of the leaf state (mra/get_max_scale_coeffs.cu:3-27, with the reference's
@@ -455,7 +458,71 @@ __global__ void __launch_bounds__(256) k_decode_level(Hier<T> hr, Scalars<T>* sc
     unsigned done = 0;
     if (idx < (1 << (2 * level))) decode_parent<T, MW>(hr, sc, L, level, idx, eps, done);
     const unsigned tot = __reduce_add_sync(0xffffffffu, done);
-    if ((threadIdx.x & 31) == 0 && tot) atomicAdd(&sc->dec, (unsigned long long)tot);
+    if ((threadIdx.x & 31) == 0 && tot)
+    {
+        atomicAdd(&sc->dec, (unsigned long long)tot);
+        atomicAdd(&sc->sig_level[level], tot);
+    }
+}
+
+// Sparse form of one level (a level whose significant parents were few last step): a
+// thread reads the flags of eight consecutive parents as one aligned 8-byte word
+// (lvl_idx(level) is a multiple of 8 for level >= 2), finishes the parents that are not
+// significant itself (FULL encode: clear their flag bits) and lists the significant ones
+// in shared memory; the warp's lanes then take the listed parents in turn. A level of 4M
+// parents with a handful significant costs 512K threads that read 8 bytes each instead of
+// 4M threads. Op 0: FULL encode, 1: scale-only re-encode, 2: decode.
+template <typename T, bool MW, int OP>
+__global__ void __launch_bounds__(256) k_level_sparse(Hier<T> hr, Scalars<T>* sc, int L, int level, T eps)
+{
+    __shared__ int list[8][256];   // per warp: up to 32 lanes x 8 parents
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t first = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * 8;
+    const int64_t np = (int64_t)1 << (2 * level);
+    unsigned done = 0;
+    uint32_t sig = 0;
+    if (first < np)
+    {
+        const uint2 w = *reinterpret_cast<const uint2*>(hr.flags + lvl_idx(level) + first);
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+        {
+            const uint32_t f = ((j < 4 ? w.x : w.y) >> (8 * (j & 3))) & 0xffu;
+            if (f & F_SIG) sig |= 1u << j;
+            else if (OP == 0) encode_parent<T, MW, true>(hr, sc, L, level, (int)(first + j), eps, done);
+        }
+    }
+    const int c = __popc(sig);
+    int incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1)
+    {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    int k = incl - c;
+    for (int j = 0; j < 8; ++j)
+        if (sig & (1u << j)) list[warp][k++] = (int)(first + j);
+    __syncwarp();
+    for (int e = lane; e < total; e += 32)
+    {
+        const int idx = list[warp][e];
+        if (OP == 0) encode_parent<T, MW, true>(hr, sc, L, level, idx, eps, done);
+        else if (OP == 1) encode_parent<T, MW, false>(hr, sc, L, level, idx, eps, done);
+        else decode_parent<T, MW>(hr, sc, L, level, idx, eps, done);
+    }
+    const unsigned tot = __reduce_add_sync(0xffffffffu, done);
+    if (lane == 0 && tot)
+    {
+        if (OP == 0) atomicAdd(&sc->enc, (unsigned long long)tot);
+        else if (OP == 1) atomicAdd(&sc->enc2, (unsigned long long)tot);
+        else
+        {
+            atomicAdd(&sc->dec, (unsigned long long)tot);
+            atomicAdd(&sc->sig_level[level], tot);
+        }
+    }
 }
 
 // Bed encoding of one level and preflagging (mra/encode_topography_kernel_{mw,hw}.cu).

@@ -23,6 +23,7 @@
 #include <cstdio>
 #include <cstring>
 #include <cstdlib>
+#include <map>
 #include <memory>
 #include <string>
 #include <sys/stat.h>
@@ -135,8 +136,22 @@ private:
     // A step after the first is captured once per variant (which RK stages take the wet
     // list) and replayed as one CUDA graph; capture failures fall back to direct launches.
     bool use_graphs_ = true, capturing_ = false;
-    cudaGraphExec_t graphs_[4] = {};
-    int graph_launches_[4] = {};
+    struct Captured { cudaGraphExec_t exec; int launches; };
+    std::map<int, Captured> graphs_;   // keyed by the step's launch choices (variant_key)
+    // significant parents per level last step (levels above the bands): a level under one
+    // in eight significant takes the sparse kernel (k_level_sparse)
+    int64_t sig_prev_[16] = {-1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1};
+    bool sparse_level(int level) const
+    {
+        return sig_prev_[level] >= 0 && sig_prev_[level] * 8 < ((int64_t)1 << (2 * level));
+    }
+    int variant_key() const
+    {
+        int key = (mw_ && use_list(1) ? 1 : 0) | (mw_ && use_list(2) ? 2 : 0);
+        for (int level = mw::kBandMaxLevel + 1; level < L_; ++level)
+            if (sparse_level(level)) key |= 4 << (level - mw::kBandMaxLevel - 1);
+        return key;
+    }
     int64_t wet_prev_[2] = {-1, -1};    // previous step's wet-leaf count per RK stage
     mw::Src<T>* d_src_ = nullptr;
     mw::Src<T>* h_src_ = nullptr;       // pinned
@@ -200,9 +215,18 @@ private:
     {
         for (int level = L_ - 1; level > mw::kBandMaxLevel; --level)
         {
-            const int nb = grid_for((int64_t)1 << (2 * level), 256, 1 << 30);
-            if (mw_) mw::k_encode_level<T, true, FULL><<<nb, 256, 0, st_>>>(h, sc_, L_, level, eps);
-            else mw::k_encode_level<T, false, FULL><<<nb, 256, 0, st_>>>(h, sc_, L_, level, eps);
+            if (sparse_level(level))
+            {
+                const int nb = grid_for(((int64_t)1 << (2 * level)) / 8, 256, 1 << 30);
+                if (mw_) mw::k_level_sparse<T, true, FULL ? 0 : 1><<<nb, 256, 0, st_>>>(h, sc_, L_, level, eps);
+                else mw::k_level_sparse<T, false, FULL ? 0 : 1><<<nb, 256, 0, st_>>>(h, sc_, L_, level, eps);
+            }
+            else
+            {
+                const int nb = grid_for((int64_t)1 << (2 * level), 256, 1 << 30);
+                if (mw_) mw::k_encode_level<T, true, FULL><<<nb, 256, 0, st_>>>(h, sc_, L_, level, eps);
+                else mw::k_encode_level<T, false, FULL><<<nb, 256, 0, st_>>>(h, sc_, L_, level, eps);
+            }
             ++launches_;
         }
         for (const Band& b : bands_)
@@ -232,7 +256,8 @@ template <typename T> void Sim<T>::release()
 {
     if (device_ >= 0) cudaSetDevice(device_);
     for (auto& e : ev_) if (e) { cudaEventDestroy(e); e = nullptr; }
-    for (auto& g : graphs_) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    for (auto& g : graphs_) cudaGraphExecDestroy(g.second.exec);
+    graphs_.clear();
     if (h_args_) { cudaFreeHost(h_args_); h_args_ = nullptr; }
     for (void* p : allocs_) cudaFree(p);
     allocs_.clear();
@@ -431,8 +456,8 @@ template <typename T> mwdg2_status Sim<T>::launch_step()
     // the first step has its own kernels (initial maxima, full encode); later steps differ
     // only in which RK stages take the wet list
     if (!use_graphs_ || first_) return enqueue_device();
-    const int key = (mw_ && use_list(1) ? 1 : 0) | (mw_ && use_list(2) ? 2 : 0);
-    if (!graphs_[key])
+    const int key = variant_key();
+    if (!graphs_.count(key))
     {
         cudaGraph_t g = nullptr;
         cudaGraphExec_t ge = nullptr;
@@ -450,11 +475,10 @@ template <typename T> mwdg2_status Sim<T>::launch_step()
             use_graphs_ = false;
             return enqueue_device();
         }
-        graphs_[key] = ge;
-        graph_launches_[key] = launches_;
+        graphs_[key] = Captured{ge, launches_};
     }
-    launches_ = graph_launches_[key];
-    CU(cudaGraphLaunch(graphs_[key], st_));
+    launches_ = graphs_[key].launches;
+    CU(cudaGraphLaunch(graphs_[key].exec, st_));
     return MWDG2_OK;
 }
 
@@ -502,9 +526,18 @@ template <typename T> mwdg2_status Sim<T>::enqueue_device()
         }
         for (int level = mw::kBandMaxLevel + 1; level < L_; ++level)
         {
-            const int nb = grid_for((int64_t)1 << (2 * level), 256, 1 << 30);
-            if (mw) mw::k_decode_level<T, true><<<nb, 256, 0, st_>>>(hr_, sc_, L_, level, eps);
-            else mw::k_decode_level<T, false><<<nb, 256, 0, st_>>>(hr_, sc_, L_, level, eps);
+            if (sparse_level(level))
+            {
+                const int nb = grid_for(((int64_t)1 << (2 * level)) / 8, 256, 1 << 30);
+                if (mw) mw::k_level_sparse<T, true, 2><<<nb, 256, 0, st_>>>(hr_, sc_, L_, level, eps);
+                else mw::k_level_sparse<T, false, 2><<<nb, 256, 0, st_>>>(hr_, sc_, L_, level, eps);
+            }
+            else
+            {
+                const int nb = grid_for((int64_t)1 << (2 * level), 256, 1 << 30);
+                if (mw) mw::k_decode_level<T, true><<<nb, 256, 0, st_>>>(hr_, sc_, L_, level, eps);
+                else mw::k_decode_level<T, false><<<nb, 256, 0, st_>>>(hr_, sc_, L_, level, eps);
+            }
             ++launches_;
         }
     }
@@ -561,6 +594,8 @@ template <typename T> mwdg2_status Sim<T>::collect_step()
     }
     if (mw)
         for (int s = 0; s < 2; ++s) wet_prev_[s] = sc_host_->wet[s];
+    if (cs_.epsilon > T(0) || first_)   // a step that remeshed counted its significant parents
+        for (int l = mw::kBandMaxLevel + 1; l < L_ && l < 16; ++l) sig_prev_[l] = sc_host_->sig_level[l];
     last_cnt_[0] = (int64_t)sc_host_->enc;
     last_cnt_[1] = (int64_t)sc_host_->enc2;
     last_cnt_[2] = (int64_t)sc_host_->dec;
