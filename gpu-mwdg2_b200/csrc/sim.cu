@@ -132,7 +132,10 @@ private:
     mw::StepArgs<T>* h_args_ = nullptr; // pinned; copied to d_args_ by the step's first operation
     // Per-leaf kernels run persistent grids (grid-stride loops): SMs x resident blocks of each
     // kernel, so a step's launches do not depend on the leaf count and can be replayed.
-    int grid_leaf_ = 0, grid_classify_ = 0, grid_stage_ = 0;
+    int grid_leaf_ = 0, grid_wet_ = 0, grid_dry_ = 0, grid_stage_ = 0;
+    uint8_t* dry_ = nullptr;            // dry marks of one RK stage (k_stage_wet -> k_stage_dry)
+    cudaStream_t st2_ = nullptr;        // the wet-list kernels, beside the dry-leaf writers
+    cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
     // A step after the first is captured once per variant (which RK stages take the wet
     // list) and replayed as one CUDA graph; capture failures fall back to direct launches.
     bool use_graphs_ = true, capturing_ = false;
@@ -192,15 +195,22 @@ private:
         const int64_t w = wet_prev_[stage - 1];
         return w >= 0 && 2 * w < n_leaves_;
     }
+    // With the wet list: the wet test, then the dry leaves' writer on st_ beside the wet-list
+    // kernel on st2_ (disjoint leaves; the writer is bandwidth-bound, the wet-list kernel
+    // latency-bound), joined before the stage ends.
     template <int STAGE> void stage(const mw::Hier<T>& hin, const mw::Hier<T>& hout, bool fric)
     {
         if (use_list(STAGE))
         {
-            mw::k_stage_classify<T, STAGE><<<grid_classify_, 256, 0, st_>>>(lf_, hin, hout, sc_, P_, d_args_, fric,
-                                                                             wet_list_);
-            mw::k_mwdg2_stage<T, STAGE, true><<<grid_stage_, mw::kSolverThreads, 0, st_>>>(lf_, hin, hout, sc_, P_,
-                                                                                          d_args_, fric, wet_list_);
-            launches_ += 2;
+            mw::k_stage_wet<T, STAGE><<<grid_wet_, 256, 0, st_>>>(lf_, hin, sc_, P_, d_args_, dry_, wet_list_);
+            cudaEventRecord(ev_fork_, st_);
+            cudaStreamWaitEvent(st2_, ev_fork_, 0);
+            mw::k_mwdg2_stage<T, STAGE, true><<<grid_stage_, mw::kSolverThreads, 0, st2_>>>(lf_, hin, hout, sc_, P_,
+                                                                                           d_args_, fric, wet_list_);
+            mw::k_stage_dry<T, STAGE><<<grid_dry_, 256, 0, st_>>>(lf_, hin, hout, sc_, P_, fric, dry_);
+            cudaEventRecord(ev_join_, st2_);
+            cudaStreamWaitEvent(st_, ev_join_, 0);
+            launches_ += 3;
         }
         else
         {
@@ -263,6 +273,9 @@ template <typename T> void Sim<T>::release()
     allocs_.clear();
     if (sc_host_) { cudaFreeHost(sc_host_); sc_host_ = nullptr; }
     if (h_src_) { cudaFreeHost(h_src_); h_src_ = nullptr; }
+    if (ev_fork_) { cudaEventDestroy(ev_fork_); ev_fork_ = nullptr; }
+    if (ev_join_) { cudaEventDestroy(ev_join_); ev_join_ = nullptr; }
+    if (st2_) { cudaStreamDestroy(st2_); st2_ = nullptr; }
     if (st_) { cudaStreamDestroy(st_); st_ = nullptr; }
 }
 
@@ -338,7 +351,14 @@ template <typename T> mwdg2_status Sim<T>::init(const char* par, const mwdg2_opt
     }
     if (mwdg2_status s = dalloc(sc_, 1)) return s;
     if (mwdg2_status s = dalloc(tile_counts_, ntiles_)) return s;
-    if (mw_) { if (mwdg2_status s = dalloc(wet_list_, F_)) return s; }
+    if (mw_)
+    {
+        if (mwdg2_status s = dalloc(wet_list_, F_)) return s;
+        if (mwdg2_status s = dalloc(dry_, F_)) return s;
+        CU(cudaStreamCreateWithFlags(&st2_, cudaStreamNonBlocking));
+        CU(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming));
+        CU(cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming));
+    }
     if (mwdg2_status s = dalloc(d_args_, 1)) return s;
     CU(cudaMallocHost(&h_args_, sizeof(mw::StepArgs<T>)));
     {
@@ -349,7 +369,8 @@ template <typename T> mwdg2_status Sim<T>::init(const char* par, const mwdg2_opt
             return b;
         };
         grid_leaf_ = sms * resident(mw::k_maxes_reinsert<T, true>, 256);
-        grid_classify_ = sms * resident(mw::k_stage_classify<T, 1>, 256);
+        grid_wet_ = sms * resident(mw::k_stage_wet<T, 1>, 256);
+        grid_dry_ = sms * resident(mw::k_stage_dry<T, 1>, 256);
         grid_stage_ = sms * (mw_ ? resident(mw::k_mwdg2_stage<T, 1, false>, mw::kSolverThreads)
                                  : resident(mw::k_hwfv1<T>, mw::kSolverThreads));
     }

@@ -356,21 +356,19 @@ template <typename T> struct StateMax
     }
 };
 
-// Wet-list construction for one RK stage: dry leaves are finished here, the others are
-// appended to `wet` for k_mwdg2_stage<.., LIST=true>. Stage 1 gives a dry leaf's state,
-// with the discharge cleared by friction, to U^n (un) and to the stage hierarchy `hout`;
-// stage 2 leaves it unchanged and re-inserts U^n into the hierarchy `hout`. The kernel is
-// latency-bound on its gathers, so its registers are capped for more resident warps
-// (FP32: 40, 6 blocks per SM; FP64: 80, 3 blocks).
+// Wet test of one RK stage (the rule of leaf_is_dry, after ghost cells): wet leaves are
+// appended to `wet` (warp-aggregated) for k_mwdg2_stage<.., LIST=true>, dry ones marked in
+// `dry` for k_stage_dry, which then runs beside the wet-list kernel (the two touch disjoint
+// leaves). Stage 1 also keeps a dry leaf's depth after ghost cells in U^n (un[0]); stage 2
+// reports initial_tstep as the CFL step of dry leaves (dg2_update.cu:61).
 template <typename T, int STAGE>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 5 : 3) k_stage_classify(Leaves<T> lf, Hier<T> hin, Hier<T> hout, Scalars<T>* sc,
-                                                        Params<T> P, const StepArgs<T>* args, bool friction, int32_t* wet)
+__global__ void __launch_bounds__(256) k_stage_wet(Leaves<T> lf, Hier<T> hin, Scalars<T>* sc, Params<T> P,
+                                                   const StepArgs<T>* args, uint8_t* dry, int32_t* wet)
 {
     const T dt = args->dt;
     const Bnd<T>& B = args->B;
     const int n = sc->n_leaves;
     bool any_dry = false;
-    StateMax<T> mx;
     for (int i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x)
     {
         const int i = i0 + threadIdx.x;
@@ -382,65 +380,22 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 5 : 3) k_stage_classify(
             int32_t nid[4];
 #pragma unroll
             for (int d = 0; d < 4; ++d) nid[d] = lf.nb[d][i];
-            // Everything a dry leaf needs is loaded before the dry test (almost every leaf
-            // is dry where this kernel runs), so the loads are in flight together.
-            T c[4][3];                     // own coefficients [field][mode]; stage 2: mode 0 + bed
-            T u[9];                        // stage 2: U^n
-#pragma unroll
-            for (int m = 0; m < 3; ++m)
-            {
-                c[3][m] = hin.s[3][m][a];
-                if (STAGE == 1 || m == 0)
-                {
-                    c[0][m] = hin.s[0][m][a];
-                    c[1][m] = hin.s[1][m][a];
-                    c[2][m] = hin.s[2][m][a];
-                }
-            }
-            if (STAGE == 2)
-            {
-#pragma unroll
-                for (int k = 0; k < 9; ++k) u[k] = lf.un[k][i];
-            }
+            // own and neighbour loads issued together (almost every leaf is dry here)
+            const T e0 = hin.s[0][0][a], z0 = hin.s[3][0][a], qx0 = hin.s[1][0][a], qy0 = hin.s[2][0][a];
             T nbh[4];
 #pragma unroll
             for (int d = 0; d < 4; ++d)
                 nbh[d] = (nid[d] != -1) ? hin.s[0][0][nid[d]] - hin.s[3][0][nid[d]] : T(0.0);
-            T h0 = c[0][0] - c[3][0];
-            T qx0 = c[1][0], qy0 = c[2][0];
-            const T z0 = c[3][0];
+            T h0 = e0 - z0;
             T gh[4], gqx[4], gqy[4];
             ghost_pass(h0, qx0, qy0, z0, nid, level, a, P, B, dt, gh, gqx, gqy);
-            // the dry rule of leaf_is_dry
-            bool dry = h0 < P.tol_h;
+            bool is_dry = h0 < P.tol_h;
 #pragma unroll
-            for (int d = 0; d < 4; ++d) dry = dry && ((nid[d] != -1) ? nbh[d] : gh[d]) < P.tol_h;
-            is_wet = !dry;
-            any_dry |= dry;
-            if (dry)
-            {
-                const T z[3] = {c[3][0], c[3][1], c[3][2]};
-                if (STAGE == 1)
-                {
-                    if (friction) { qx0 = T(0.0); qy0 = T(0.0); }
-                    u[0] = h0; u[3] = qx0; u[6] = qy0;
-#pragma unroll
-                    for (int m = 1; m < 3; ++m)
-                    {
-                        u[m] = c[0][m] - z[m];
-                        u[3 + m] = c[1][m];
-                        u[6 + m] = c[2][m];
-                    }
-#pragma unroll
-                    for (int k = 0; k < 9; ++k) lf.un[k][i] = u[k];
-                }
-                else
-                {
-                    mx.add(u, z0);
-                    if (P.dt_leaf) P.dt_leaf[i] = P.initial_tstep;
-                }
-                put_leaf(hout, a, u, z);
-            }
+            for (int d = 0; d < 4; ++d) is_dry = is_dry && ((nid[d] != -1) ? nbh[d] : gh[d]) < P.tol_h;
+            is_wet = !is_dry;
+            any_dry |= is_dry;
+            dry[i] = is_dry ? 1 : 0;
+            if (STAGE == 1 && is_dry) lf.un[0][i] = h0;
         }
         // warp-aggregated append
         const unsigned mask = __ballot_sync(0xffffffffu, is_wet);
@@ -450,12 +405,51 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 5 : 3) k_stage_classify(
         base = __shfl_sync(0xffffffffu, base, 0);
         if (is_wet) wet[base + __popc(mask & ((1u << lane) - 1u))] = i;
     }
-    if (STAGE == 2)
+    if (STAGE == 2 && __syncthreads_or(any_dry) && threadIdx.x == 0) atomic_min_nn(&sc->dt_min, P.initial_tstep);
+}
+
+// The dry leaves of one RK stage, marked by k_stage_wet (bandwidth-bound; it runs beside
+// the latency-bound wet-list kernel). Stage 1 (hin: hierarchy, hout: stage hierarchy): U^n
+// is the leaf's state with the discharge cleared by friction (depth after ghost cells as
+// k_stage_wet left it in un[0]) and U* equals it. Stage 2 (hout: hierarchy): the leaf keeps
+// U^n, which is re-inserted into the hierarchy and enters the next step's maxima.
+template <typename T, int STAGE>
+__global__ void __launch_bounds__(256) k_stage_dry(Leaves<T> lf, Hier<T> hin, Hier<T> hout, Scalars<T>* sc, Params<T> P,
+                                                   bool friction, const uint8_t* dry)
+{
+    const int n = sc->n_leaves;
+    StateMax<T> mx;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     {
-        mx.flush(sc);
-        // dry leaves report initial_tstep as their CFL step (dg2_update.cu:61)
-        if (__syncthreads_or(any_dry) && threadIdx.x == 0) atomic_min_nn(&sc->dt_min, P.initial_tstep);
+        if (!dry[i]) continue;
+        const int a = lf.act[i];
+        const T z[3] = {hin.s[3][0][a], hin.s[3][1][a], hin.s[3][2][a]};
+        T u[9];
+        if (STAGE == 1)
+        {
+            u[0] = lf.un[0][i];
+            u[3] = friction ? T(0.0) : hin.s[1][0][a];
+            u[6] = friction ? T(0.0) : hin.s[2][0][a];
+#pragma unroll
+            for (int m = 1; m < 3; ++m)
+            {
+                u[m] = hin.s[0][m][a] - z[m];
+                u[3 + m] = hin.s[1][m][a];
+                u[6 + m] = hin.s[2][m][a];
+            }
+#pragma unroll
+            for (int k = 1; k < 9; ++k) lf.un[k][i] = u[k];
+        }
+        else
+        {
+#pragma unroll
+            for (int k = 0; k < 9; ++k) u[k] = lf.un[k][i];
+            mx.add(u, z[0]);
+            if (P.dt_leaf) P.dt_leaf[i] = P.initial_tstep;
+        }
+        put_leaf(hout, a, u, z);
     }
+    if (STAGE == 2) mx.flush(sc);
 }
 
 // One RK2 stage of MWDG2, reading the hierarchy `hin` and writing each leaf's result into
@@ -465,7 +459,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 5 : 3) k_stage_classify(
 // STAGE 2 (hin: stage hierarchy, hout: hierarchy): limiter with the stage's max depth,
 // U^{n+1} = (U** + U^n)/2 -> un and hout (the next step's re-insertion,
 // mra/reinsert_assem_sol.cu), the next step's maxima, CFL dt. LIST: only the leaves in
-// the wet list built by k_stage_classify; otherwise every leaf.
+// the wet list built by k_stage_wet; otherwise every leaf.
 template <typename T, int STAGE, bool LIST>
 __global__ void __launch_bounds__(kSolverThreads) k_mwdg2_stage(Leaves<T> lf, Hier<T> hin, Hier<T> hout, Scalars<T>* sc,
                                                                 Params<T> P, const StepArgs<T>* args, bool friction,
