@@ -160,6 +160,9 @@ private:
     mw::Src<T>* h_src_ = nullptr;       // pinned
     int32_t* d_stage_codes_ = nullptr;
     T* d_stage_out_ = nullptr;
+    T* h_stage_ = nullptr;              // pinned: stage-point values sampled at the end of each step
+    size_t scal_bytes_ = 0;             // scalars + stage-point values (device block sc_, host sc_host_)
+    bool stage_fresh_ = false;          // h_stage_ holds the current state's values
     double* d_state_scratch_ = nullptr;
     T* d_dt_leaf_ = nullptr;            // per-leaf CFL step of the last stage (VTK output only)
     T* d_raster_ = nullptr;             // raster rows (saveint raster maps)
@@ -273,6 +276,7 @@ template <typename T> void Sim<T>::release()
     allocs_.clear();
     if (sc_host_) { cudaFreeHost(sc_host_); sc_host_ = nullptr; }
     if (h_src_) { cudaFreeHost(h_src_); h_src_ = nullptr; }
+    h_stage_ = nullptr;   // part of the sc_host_ block
     if (ev_fork_) { cudaEventDestroy(ev_fork_); ev_fork_ = nullptr; }
     if (ev_join_) { cudaEventDestroy(ev_join_); ev_join_ = nullptr; }
     if (st2_) { cudaStreamDestroy(st2_); st2_ = nullptr; }
@@ -349,7 +353,21 @@ template <typename T> mwdg2_status Sim<T>::init(const char* par, const mwdg2_opt
         lf_.un[k] = nullptr;
         if (mw_ || k % 3 == 0) { if (mwdg2_status s = dalloc(lf_.un[k], F_)) return s; }
     }
-    if (mwdg2_status s = dalloc(sc_, 1)) return s;
+    // the step's scalars and the stage-point values sampled at its end share one block, so
+    // a single copy brings both back
+    const int nst = (int)cs_.stage_codes.size();
+    const size_t stage_off = (sizeof(mw::Scalars<T>) + 15) / 16 * 16;
+    scal_bytes_ = stage_off + sizeof(T) * 4 * nst;
+    {
+        char* block = nullptr;
+        if (mwdg2_status s = dalloc(block, scal_bytes_)) return s;
+        sc_ = reinterpret_cast<mw::Scalars<T>*>(block);
+        if (nst > 0) d_stage_out_ = reinterpret_cast<T*>(block + stage_off);
+        char* hblock = nullptr;
+        CU(cudaMallocHost(&hblock, scal_bytes_));
+        sc_host_ = reinterpret_cast<mw::Scalars<T>*>(hblock);
+        if (nst > 0) h_stage_ = reinterpret_cast<T*>(hblock + stage_off);
+    }
     if (mwdg2_status s = dalloc(tile_counts_, ntiles_)) return s;
     if (mw_)
     {
@@ -374,18 +392,15 @@ template <typename T> mwdg2_status Sim<T>::init(const char* par, const mwdg2_opt
         grid_stage_ = sms * (mw_ ? resident(mw::k_mwdg2_stage<T, 1, false>, mw::kSolverThreads)
                                  : resident(mw::k_hwfv1<T>, mw::kSolverThreads));
     }
-    CU(cudaMallocHost(&sc_host_, sizeof(mw::Scalars<T>)));
     const int nsrc = (int)cs_.srcs.size();
     if (nsrc > 0)
     {
         if (mwdg2_status s = dalloc(d_src_, nsrc)) return s;
         CU(cudaMallocHost(&h_src_, sizeof(mw::Src<T>) * nsrc));
     }
-    const int nst = (int)cs_.stage_codes.size();
     if (nst > 0)
     {
         if (mwdg2_status s = dalloc(d_stage_codes_, nst)) return s;
-        if (mwdg2_status s = dalloc(d_stage_out_, 4 * nst)) return s;
         CU(cudaMemcpyAsync(d_stage_codes_, cs_.stage_codes.data(), sizeof(int32_t) * nst, cudaMemcpyHostToDevice, st_));
     }
 
@@ -593,8 +608,16 @@ template <typename T> mwdg2_status Sim<T>::enqueue_device()
         stage<2>(hs_, hr_, false);
         rec(7);
     }
+    // the stage points of the new state come back with the step's scalars
+    const int np = (int)cs_.stage_codes.size();
+    if (np > 0)
+    {
+        mw::k_sample_points<T><<<(np + 127) / 128, 128, 0, st_>>>(lf_, hr_, sc_, L_, d_stage_codes_, np, tile_counts_,
+                                                                  ntiles_, d_stage_out_);
+        ++launches_;
+    }
     CU(cudaGetLastError());
-    CU(cudaMemcpyAsync(sc_host_, sc_, sizeof(mw::Scalars<T>), cudaMemcpyDeviceToHost, st_));
+    CU(cudaMemcpyAsync(sc_host_, sc_, scal_bytes_, cudaMemcpyDeviceToHost, st_));
     rec(8);
     return MWDG2_OK;
 }
@@ -603,6 +626,7 @@ template <typename T> mwdg2_status Sim<T>::collect_step()
 {
     const bool mw = mw_;
     CU(cudaStreamSynchronize(st_));
+    stage_fresh_ = !cs_.stage_codes.empty();
     if (timed_)
     {
         float ms = 0;
@@ -680,7 +704,14 @@ template <typename T> mwdg2_status Sim<T>::sample_stage(std::vector<T>& vals)
     const int np = (int)cs_.stage_codes.size();
     vals.assign(4 * (size_t)np, T(0));
     if (np == 0) return MWDG2_OK;
-    mw::k_sample_points<T><<<(np + 127) / 128, 128, 0, st_>>>(lf_, hr_, sc_, L_, d_stage_codes_, np, d_stage_out_);
+    if (stage_fresh_)   // sampled by the last step
+    {
+        std::copy(h_stage_, h_stage_ + 4 * (size_t)np, vals.begin());
+        return MWDG2_OK;
+    }
+    // before the first step: the leaf list is every finest cell and no tile offsets exist
+    mw::k_sample_points<T><<<(np + 127) / 128, 128, 0, st_>>>(lf_, hr_, sc_, L_, d_stage_codes_, np, nullptr, 0,
+                                                              d_stage_out_);
     CU(cudaGetLastError());
     CU(cudaMemcpyAsync(vals.data(), d_stage_out_, sizeof(T) * 4 * np, cudaMemcpyDeviceToHost, st_));
     CU(cudaStreamSynchronize(st_));

@@ -802,13 +802,25 @@ __global__ void __launch_bounds__(kSolverThreads) k_hwfv1(Leaves<T> lf, Hier<T> 
 // Leaf containing each finest cell code (binary search over the leaves' Z-order starts)
 // and its depth eta0 - z0, discharges and bed (output/project_assem_sol.cu:3-77).
 template <typename T>
-__global__ void k_sample_points(Leaves<T> lf, Hier<T> hr, Scalars<T>* sc, int L, const int32_t* codes, int np, T* out)
+// tile_offsets (the scanned leaf counts of the 4^5-cell tiles, ntiles of them; null before
+// the first step) narrow the search: leaves are in Z order, so the leaf holding finest cell
+// c is among the leaves of tile c >> 10, or is the last leaf before them when a coarser leaf
+// covers the whole tile.
+__global__ void k_sample_points(Leaves<T> lf, Hier<T> hr, Scalars<T>* sc, int L, const int32_t* codes, int np,
+                                const int32_t* tile_offsets, int ntiles, T* out)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= np) return;
     const int n = sc->n_leaves;
     const int c = codes[k];
     int lo = 0, hi = n - 1;
+    if (tile_offsets)
+    {
+        const int t = c >> (2 * kTileDepth);
+        lo = tile_offsets[t];
+        hi = (t + 1 < ntiles ? tile_offsets[t + 1] : n) - 1;
+        if (hi < lo) lo = hi = lo - 1;
+    }
     while (lo < hi)
     {
         const int mid = (lo + hi + 1) >> 1;
