@@ -143,11 +143,11 @@ class Clocks:
                 "reasons": reasons, "samples": len(self.rows), "source": "nvml"}
 
 
-# DRAM bytes per leaf (dram__bytes_read.sum + dram__bytes_write.sum of the phase's kernels
-# divided by the leaves) from ncu captures of the same workload at max_ref_lvl 11 (1.2 M
-# leaves; the traffic grows with the leaves). Keyed by (solver, P, timing phase).
-TRAFFIC_SOURCE = "ncu, fBm catchment 2048^2 (max_ref_lvl 11), scaled by leaves"
-TRAFFIC_B_PER_LEAF: dict = {("mwdg2", 4, 3): 2.7, ("mwdg2", 4, 4): 191.7, ("mwdg2", 4, 6): 152.5}
+# DRAM bytes per leaf (dram__bytes_read.sum + dram__bytes_write.sum of the phase's kernels,
+# summed, divided by the step's leaves) from a one-pass ncu launch list of this workload
+# (4096^2, FP32, 3.0 M leaves). Keyed by (solver, P, timing phase).
+TRAFFIC_SOURCE = "ncu launch list (dram bytes, 1 pass) of the same workload, per leaf x leaves"
+TRAFFIC_B_PER_LEAF: dict = {("mwdg2", 4, 3): 10.8, ("mwdg2", 4, 4): 224.9, ("mwdg2", 4, 6): 184.0}
 
 
 def peaks() -> tuple[float, str]:
@@ -341,8 +341,10 @@ def main():
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         e2e_wall = float(tt.item())
     P = a.precision // 8
-    h2d = 1 * (8 + P)            # one point source record {code, type, value}
-    d2h = (6 * P + 8 + 24) + 4 * P * n_pts
+    # bytes the library copied per step (its counters): host->device the step's dt, boundary
+    # and point-source values; device->host its scalars and the stage-point values
+    h2d = int(counters[-1]["h2d_bytes"])
+    d2h = int(counters[-1]["d2h_bytes"])
 
     # roofline of the dominant kernel, from its live event timing
     ph = np.array(ms_phase)
@@ -354,10 +356,10 @@ def main():
     # ids + 9P written + 9P of U^n = 30P + 16; stage 2: 21P + 16 (together the N(51P + 32)
     # solver term of the step formula below). HWFV1: 4P own + 16 B ids + 3P written.
     cand = {"leaf topology (k_tile_count + k_tile_scan + k_tile_emit)": (3, 40),
-            "RK stage 1 (k_stage_classify<1> + k_mwdg2_stage<1> over the wet list, or one k_mwdg2_stage<1> "
-            "sweep)": (4, 30 * P + 16),
-            "RK stage 2 (k_stage_classify<2> + k_mwdg2_stage<2> over the wet list, or one k_mwdg2_stage<2> "
-            "sweep)": (6, 21 * P + 16)}
+            "RK stage 1 (k_stage_wet<1>, then k_stage_dry<1> beside k_mwdg2_stage<1> over the wet list; or "
+            "one k_mwdg2_stage<1> sweep)": (4, 30 * P + 16),
+            "RK stage 2 (k_stage_wet<2>, then k_stage_dry<2> beside k_mwdg2_stage<2> over the wet list; or "
+            "one k_mwdg2_stage<2> sweep)": (6, 21 * P + 16)}
     if a.solver == "hwfv1":
         cand = {"leaf topology (k_tile_count + k_tile_scan + k_tile_emit)": (3, 40),
                 "k_hwfv1 (gather, friction, FV1 update, CFL)": (4, 7 * P + 16)}

@@ -171,7 +171,7 @@ private:
     bool timed_ = false;
     cudaEvent_t ev_[9] = {};
     double last_ms_[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    int64_t last_cnt_[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int64_t last_cnt_[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     int launches_ = 0;
     // outputs
     std::chrono::steady_clock::time_point t_start_;
@@ -649,6 +649,8 @@ template <typename T> mwdg2_status Sim<T>::collect_step()
     last_cnt_[5] = launches_;
     last_cnt_[6] = mw ? sc_host_->wet[0] : 0;
     last_cnt_[7] = mw ? sc_host_->wet[1] : 0;
+    last_cnt_[8] = (int64_t)(sizeof(mw::StepArgs<T>) + sizeof(mw::Src<T>) * cs_.srcs.size());
+    last_cnt_[9] = (int64_t)scal_bytes_;
     return MWDG2_OK;
 }
 
@@ -1139,7 +1141,7 @@ template <typename T> mwdg2_status Sim<T>::timing(double* out, int n)
 
 template <typename T> mwdg2_status Sim<T>::counters(int64_t* out, int n)
 {
-    for (int i = 0; i < n && i < 8; ++i) out[i] = last_cnt_[i];
+    for (int i = 0; i < n && i < 10; ++i) out[i] = last_cnt_[i];
     return MWDG2_OK;
 }
 

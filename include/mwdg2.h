@@ -120,7 +120,9 @@ mwdg2_status mwdg2_last_step_timing(mwdg2_sim* sim, double* out, int n);
 /* Counters of the last step used for the algorithmic-bytes roofline:
  * [0] parents encoded (E), [1] parents re-encoded scale-only (E2), [2] parents decoded (D),
  * [3] leaves (N_a), [4] detail slots (T = get_lvl_idx(L) - 3), [5] kernels launched in the
- * step, [6] / [7] MWDG2 leaves not dry in RK stage 1 / stage 2 (0 for HWFV1). n <= 8. */
+ * step, [6] / [7] MWDG2 leaves not dry in RK stage 1 / stage 2 (0 for HWFV1), [8] bytes the
+ * step copied host->device (dt, boundary and point-source values), [9] bytes it copied
+ * device->host (its scalars and the stage-point values). n <= 10. */
 mwdg2_status mwdg2_last_step_counters(mwdg2_sim* sim, int64_t* out, int n);
 
 void mwdg2_destroy(mwdg2_sim* sim);
