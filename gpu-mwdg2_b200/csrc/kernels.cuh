@@ -758,11 +758,11 @@ __global__ void __launch_bounds__(kTileThreads) k_tile_emit(Leaves<T> lf, const 
     const int off = offsets[tcode];
     // subtree flags at lvl_idx(j) + local index (j = 1..4); lvl_idx(D) bytes
     __shared__ __align__(4) uint8_t sflag[((1 << (2 * D)) - 1) / 3 + 3];
-    __shared__ uint8_t cell_lvl[kCells];              // leaf level of each finest cell, tile-local Morton order
+    // leaf level of each node of level L - 1 (four finest cells), tile-local Morton order;
+    // L when the node is significant (its four cells are leaves of level L)
+    __shared__ uint8_t node_lvl[kCells / 4];
     __shared__ uint16_t start_of[kCells];             // tile-local start cell of the leaf of each rank
-    __shared__ uint32_t bits[kCells / 32];            // leaf starts
-    __shared__ int32_t prefix[kCells / 32];
-    __shared__ int s_total;
+    __shared__ int32_t warp_starts[kTileThreads / 32];
     // leaf levels of the cells just outside the tile (N, E, S, W), indexed by the dilated
     // tile-local coordinate along the side (x bits for N/S, y bits shifted down for E/W)
     __shared__ uint8_t halo[4][(kXBits & (kCells - 1)) + 1];
@@ -817,40 +817,43 @@ __global__ void __launch_bounds__(kTileThreads) k_tile_emit(Leaves<T> lf, const 
         halo[side][dilate(i)] = lev;
     }
     __syncthreads();
-    // leaf level of every cell: the first level below the (significant) root whose node
-    // on the cell's path is not significant
-    for (int c = threadIdx.x; c < kCells; c += blockDim.x)
-    {
-        int lev = L;
+    // one node q of level L - 1 per thread: its leaf level is the first level below the
+    // (significant) root whose node on q's path is not significant, or L when q itself is
+    // significant; its cells hold 4 leaf starts (level L), 1 (a leaf of level lev <= L - 1
+    // starting at q's first cell) or none. A block scan of those counts ranks the leaves.
+    static_assert(kTileThreads == kCells / 4, "one thread per node of level L - 1");
+    const int q = threadIdx.x;
+    int qlev = L;
 #pragma unroll
-        for (int j = D - 1; j >= 1; --j)
-            if (!sflag[lvl_idx(j) + (c >> (2 * (D - j)))]) lev = Tl + j;
-        cell_lvl[c] = (uint8_t)lev;
-        const unsigned start = __ballot_sync(0xffffffffu, (c & ((1 << (2 * (L - lev))) - 1)) == 0);
-        if ((threadIdx.x & 31) == 0) bits[c >> 5] = start;
-    }
-    __syncthreads();
-    if (threadIdx.x < 32)
+    for (int j = D - 1; j >= 1; --j)
+        if (!sflag[lvl_idx(j) + (q >> (2 * (D - 1 - j)))]) qlev = Tl + j;
+    node_lvl[q] = (uint8_t)qlev;
+    const int nstart = (qlev == L) ? 4 : (((4 * q) & ((1 << (2 * (L - qlev))) - 1)) == 0 ? 1 : 0);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int incl = nstart;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1)
     {
-        const int cnt = __popc(bits[threadIdx.x]);
-        int incl = cnt;
-        for (int o = 1; o < 32; o <<= 1)
-        {
-            const int v = __shfl_up_sync(0xffffffffu, incl, o);
-            if ((int)threadIdx.x >= o) incl += v;
-        }
-        prefix[threadIdx.x] = incl - cnt;
-        if (threadIdx.x == 31) s_total = incl;
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
     }
+    if (lane == 31) warp_starts[warp] = incl;
     __syncthreads();
-    for (int c = threadIdx.x; c < kCells; c += blockDim.x)
+    int rank = incl - nstart, total = 0;
+#pragma unroll
+    for (int w = 0; w < kTileThreads / 32; ++w)
     {
-        const int w = c >> 5;
-        const uint32_t b = bits[w];
-        if (b & (1u << (c & 31))) start_of[prefix[w] + __popc(b & ((1u << (c & 31)) - 1u))] = (uint16_t)c;
+        const int c = warp_starts[w];
+        rank += (w < warp) ? c : 0;
+        total += c;
     }
+    if (nstart == 4)
+    {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) start_of[rank + i] = (uint16_t)(4 * q + i);
+    }
+    else if (nstart) start_of[rank] = (uint16_t)(4 * q);
     __syncthreads();
-    const int total = s_total;
     const unsigned lmask = kCells - 1;
     // dilated coordinates of the mesh's last row/column and of the DEM's
     const unsigned mesh_x = kXBits & ((1u << (2 * L)) - 1u), mesh_y = mesh_x << 1;
@@ -858,7 +861,7 @@ __global__ void __launch_bounds__(kTileThreads) k_tile_emit(Leaves<T> lf, const 
     for (int r = threadIdx.x; r < total; r += blockDim.x)
     {
         const int c = start_of[r];
-        const int lev = cell_lvl[c];
+        const int lev = node_lvl[c >> 2];
         const int sh = 2 * (L - lev);
         const unsigned gc = tbase + (unsigned)c;       // finest code of the leaf's south-west cell
         const int pos = off + r;
@@ -881,7 +884,7 @@ __global__ void __launch_bounds__(kTileThreads) k_tile_emit(Leaves<T> lf, const 
             {
                 const unsigned t = tc[d];
                 int lt;
-                if ((t >> (2 * D)) == (unsigned)tcode) lt = cell_lvl[t & lmask];
+                if ((t >> (2 * D)) == (unsigned)tcode) lt = node_lvl[(t & lmask) >> 2];
                 else if (d == 0 || d == 2) lt = halo[d][t & lmask & kXBits];
                 else lt = halo[d][(t & lmask & kYBits) >> 1];
                 lv = lev < lt ? lev : lt;
