@@ -726,7 +726,7 @@ __device__ __forceinline__ void leaf_neighbour(const uint8_t* flags, int L, int 
 
 // A tile holding one leaf (the tile's root or the first tile of a coarser leaf): threads
 // 0..3 of the block find one neighbour each.
-template <typename T>
+template <typename T, bool NBL>
 __device__ __forceinline__ void emit_single_leaf(const Leaves<T>& lf, const uint8_t* flags, int L, int M, int xsz,
                                                  int ysz, int pos, int act, int l)
 {
@@ -737,7 +737,7 @@ __device__ __forceinline__ void emit_single_leaf(const Leaves<T>& lf, const uint
     uint8_t lv;
     leaf_neighbour(flags, L, M, xsz, ysz, act, l, d, id, lv);
     lf.nb[d][pos] = id;
-    lf.nbl[d][pos] = lv;
+    if (NBL) lf.nbl[d][pos] = lv;
 }
 
 // Leaves of one tile in Z order with their neighbours. The tile's subtree flags are
@@ -748,7 +748,9 @@ __device__ __forceinline__ void emit_single_leaf(const Leaves<T>& lf, const uint
 // finest cell at min(own level, that cell's leaf level) (neighbours/find_neighbours.cu:
 // 100-108), -1 across the DEM or mesh border (neighbours/find_neighbours.cu:51-428).
 // Neighbouring cells are found by dilated-integer steps on the leaf's Morton code.
-template <typename T>
+// NBL: also write the neighbours' levels (lf.nbl), which level_of(id) gives wherever the id
+// is not -1 (-1: the leaf's own level).
+template <typename T, bool NBL>
 __global__ void __launch_bounds__(kTileThreads) k_tile_emit(Leaves<T> lf, const uint8_t* flags, const int32_t* offsets,
                                                             int L, int M, int xsz, int ysz)
 {
@@ -770,12 +772,12 @@ __global__ void __launch_bounds__(kTileThreads) k_tile_emit(Leaves<T> lf, const 
     if (k < Tl)
     {
         if ((tcode & ((1 << (2 * (Tl - k))) - 1)) == 0)
-            emit_single_leaf(lf, flags, L, M, xsz, ysz, off, lvl_idx(k) + (tcode >> (2 * (Tl - k))), k);
+            emit_single_leaf<T, NBL>(lf, flags, L, M, xsz, ysz, off, lvl_idx(k) + (tcode >> (2 * (Tl - k))), k);
         return;
     }
     if (k == Tl)
     {
-        emit_single_leaf(lf, flags, L, M, xsz, ysz, off, lvl_idx(Tl) + tcode, Tl);
+        emit_single_leaf<T, NBL>(lf, flags, L, M, xsz, ysz, off, lvl_idx(Tl) + tcode, Tl);
         return;
     }
     if (threadIdx.x < 85)
@@ -891,7 +893,7 @@ __global__ void __launch_bounds__(kTileThreads) k_tile_emit(Leaves<T> lf, const 
                 id = lvl_idx(lv) + (int)(t >> (2 * (L - lv)));
             }
             lf.nb[d][pos] = id;
-            lf.nbl[d][pos] = (uint8_t)lv;
+            if (NBL) lf.nbl[d][pos] = (uint8_t)lv;
         }
     }
 }

@@ -27,12 +27,17 @@ enum : uint8_t {
 // utilities/get_lvl_idx.cuh:11-24 -- first slot of level n (3 padding slots)
 MW_HD int lvl_idx(int level) { return ((1 << (2 * level)) - 1) / 3 + 3; }
 
-// Level of a hierarchy index (inverse of lvl_idx).
+// Level of a hierarchy index h >= 3 (inverse of lvl_idx): 3 (h - 3) + 1 lies in
+// [4^l, 4^(l+1)), so l is half the position of its highest set bit (32 bits hold it for
+// l <= 15).
 MW_HD int level_of(int h)
 {
-    int l = 0;
-    while (lvl_idx(l + 1) <= h) ++l;
-    return l;
+    const unsigned v = 3u * (unsigned)(h - 3) + 1u;
+#ifdef __CUDA_ARCH__
+    return (31 - __clz((int)v)) >> 1;
+#else
+    return (31 - __builtin_clz(v)) >> 1;
+#endif
 }
 
 // zorder/dilate.cuh:25-41, zorder/compact.cuh:9-21, zorder/generate_morton_code.cuh:7-16

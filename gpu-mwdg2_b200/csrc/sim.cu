@@ -343,10 +343,11 @@ template <typename T> mwdg2_status Sim<T>::init(const char* par, const mwdg2_opt
     // leaves (capacity: every finest cell)
     if (mwdg2_status s = dalloc(lf_.act, F_)) return s;
     if (mwdg2_status s = dalloc(lf_.lvl, F_)) return s;
+    // neighbour ids only: a neighbour's level is level_of(id) (the leaf's own across a border)
     for (int d = 0; d < 4; ++d)
     {
         if (mwdg2_status s = dalloc(lf_.nb[d], F_)) return s;
-        if (mwdg2_status s = dalloc(lf_.nbl[d], F_)) return s;
+        lf_.nbl[d] = nullptr;
     }
     for (int k = 0; k < 9; ++k)
     {
@@ -585,7 +586,7 @@ template <typename T> mwdg2_status Sim<T>::enqueue_device()
         ++launches_;
         mw::k_tile_scan<T><<<1, 1024, 0, st_>>>(tile_counts_, ntiles_, sc_);
         ++launches_;
-        mw::k_tile_emit<T><<<ntiles_, mw::kTileThreads, 0, st_>>>(lf_, hr_.flags, tile_counts_, L_, M_, cs_.xsz, cs_.ysz);
+        mw::k_tile_emit<T, false><<<ntiles_, mw::kTileThreads, 0, st_>>>(lf_, hr_.flags, tile_counts_, L_, M_, cs_.xsz, cs_.ysz);
         ++launches_;
     }
     rec(4);
@@ -1077,14 +1078,14 @@ template <typename T> mwdg2_status Sim<T>::leaves(int32_t* a, int32_t* l, int32_
         CU(cudaMemcpy(tmp.data(), lf_.lvl, n, cudaMemcpyDeviceToHost));
         for (int i = 0; i < n; ++i) l[i] = tmp[i];
     }
+    if (lv && !l) CU(cudaMemcpy(tmp.data(), lf_.lvl, n, cudaMemcpyDeviceToHost));
+    std::vector<int32_t> nb(lv ? n : 0);
     for (int d = 0; d < 4; ++d)
     {
-        if (ids) CU(cudaMemcpy(ids + (size_t)d * n, lf_.nb[d], sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
+        int32_t* dst = ids ? ids + (size_t)d * n : (lv ? nb.data() : nullptr);
+        if (dst) CU(cudaMemcpy(dst, lf_.nb[d], sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
         if (lv)
-        {
-            CU(cudaMemcpy(tmp.data(), lf_.nbl[d], n, cudaMemcpyDeviceToHost));
-            for (int i = 0; i < n; ++i) lv[(size_t)d * n + i] = tmp[i];
-        }
+            for (int i = 0; i < n; ++i) lv[(size_t)d * n + i] = dst[i] == -1 ? (int32_t)tmp[i] : mw::level_of(dst[i]);
     }
     return MWDG2_OK;
 }

@@ -482,7 +482,7 @@ __global__ void __launch_bounds__(kSolverThreads) k_mwdg2_stage(Leaves<T> lf, Hi
         int32_t nid[4];
         int nl[4];
 #pragma unroll
-        for (int d = 0; d < 4; ++d) { nid[d] = lf.nb[d][i]; nl[d] = lf.nbl[d][i]; }
+        for (int d = 0; d < 4; ++d) { nid[d] = lf.nb[d][i]; nl[d] = nid[d] == -1 ? level : level_of(nid[d]); }
         Cell<T> own;
         load_cell<T, true>(hr, a, own);
         T gh[4], gqx[4], gqy[4];
