@@ -46,6 +46,7 @@ template <typename T> struct Scalars
     uint32_t sig_level[16];           // significant parents decoded per level (levels above the bands)
     int32_t wet[2];                   // leaves not dry in RK stage 1 / stage 2 (wet-list lengths)
     T next_max[4];                    // maxima of the state at the end of the step (eta, h, qx, z)
+    T xs_factor;                      // 2^(M_BAR+1) of the extra-significance threshold (extra_eps)
 };
 
 template <typename T> struct Params
@@ -144,6 +145,9 @@ template <typename T> __global__ void k_step_begin(Scalars<T>* sc, bool carry)
     sc->dt_min = (sizeof(T) == 8) ? T(1.0e308) : T(3.0e38);
     sc->enc = 0; sc->enc2 = 0; sc->dec = 0;
     sc->wet[0] = 0; sc->wet[1] = 0;
+    // the expression of mra/extra_significance_kernel.cu, evaluated once per step instead of
+    // once per parent (the same expression on the device gives the same bits everywhere)
+    sc->xs_factor = pow(T(2.0), T(1.5) + 1);
 #pragma unroll
     for (int l = 0; l < 16; ++l) sc->sig_level[l] = 0;
 }
@@ -238,6 +242,14 @@ template <typename T> __device__ __forceinline__ T encode_eps(T eps, int L, int 
     return eps / (1 << (L - lv));
 }
 
+// Extra-significance threshold of a parent at `level` (mra/extra_significance_kernel.cu):
+// eps_l * 2^(M_BAR+1) with M_BAR = 1.5 (the factor from k_step_begin).
+template <typename T> __device__ __forceinline__ T extra_eps(T eps, int L, int level, const Scalars<T>* sc)
+{
+    const T eps_local = eps / (1 << (L - level));
+    return eps_local * sc->xs_factor;
+}
+
 // Encode one parent (mra/encode_flow_kernel_{mw,hw}.cu), threshold it and OR in the
 // children's significance (mra/regularisation_kernel.cu). FULL = false re-encodes scale
 // coefficients of significant parents only (run_simulation.cu:573-588).
@@ -305,6 +317,7 @@ __device__ __forceinline__ void encode_parent(const Hier<T>& hr, const Scalars<T
             }
         }
         if (nd >= encode_eps(eps, L, level) || (f & F_PRE)) nf |= F_SIG;
+        if (level <= L - 2 && nd >= extra_eps(eps, L, level, sc)) nf |= F_XS;
         if (!(nf & F_SIG) && level <= L - 2)
         {
             const uint32_t ch = *reinterpret_cast<const uint32_t*>(hr.flags + c);
@@ -361,7 +374,9 @@ __global__ void __launch_bounds__(256) k_encode_band(Hier<T> hr, Scalars<T>* sc,
 // the result is bit-identical to the encode's and no detail arrays are stored. Parents
 // made significant without being encoded have zero details and zero norm, as in the
 // reference (mra/zero_details.cu).
-template <typename T, bool MW>
+// FLAGS = false: values only; the flags of the children are then set by k_extra_sig_level
+// from F_XS, which the encode derived from the same details.
+template <typename T, bool MW, bool FLAGS = true>
 __device__ __forceinline__ void decode_parent(const Hier<T>& hr, const Scalars<T>* sc, int L, int level, int idx, T eps,
                                               unsigned& n_done)
 {
@@ -416,11 +431,9 @@ __device__ __forceinline__ void decode_parent(const Hier<T>& hr, const Scalars<T
         }
     }
     ++n_done;
-    if (level <= L - 2)
+    if (FLAGS && level <= L - 2)
     {
-        const T eps_local = eps / (1 << (L - level));
-        const T eps_extra = eps_local * pow(T(2.0), T(1.5) + 1);
-        if (nd >= eps_extra) *reinterpret_cast<uint32_t*>(hr.flags + c) |= 0x01010101u;
+        if (nd >= extra_eps(eps, L, level, sc)) *reinterpret_cast<uint32_t*>(hr.flags + c) |= 0x01010101u;
     }
 }
 
@@ -450,13 +463,37 @@ __global__ void __launch_bounds__(256) k_decode_band(Hier<T> hr, Scalars<T>* sc,
     if ((threadIdx.x & 31) == 0 && tot) atomicAdd(&sc->dec, (unsigned long long)tot);
 }
 
-// One level of parents (levels above kBandMaxLevel).
+// Extra significance of one level of parents from their flags (levels above kBandMaxLevel,
+// level <= L - 2): a significant parent makes its children significant when its encode set
+// F_XS, or, not encoded (zero details, zero norm), when the threshold is not above zero.
+// Four parents per thread (one aligned flag word). The flags are final after this, so the
+// leaf topology can run beside the value decode of the level (k_decode_level).
+template <typename T>
+__global__ void __launch_bounds__(256) k_extra_sig_level(uint8_t* flags, const Scalars<T>* sc, int L, int level, T eps)
+{
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= (1 << (2 * level - 2))) return;
+    const uint32_t word = *reinterpret_cast<const uint32_t*>(flags + lvl_idx(level) + 4 * w);
+    if (!(word & (0x01010101u * F_SIG))) return;
+    const bool zero_norm_extra = T(0.0) >= extra_eps(eps, L, level, sc);
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+    {
+        const uint32_t f = (word >> (8 * j)) & 0xffu;
+        if (!(f & F_SIG)) continue;
+        const bool xs = (f & F_ENC) ? (f & F_XS) != 0 : zero_norm_extra;
+        if (xs) *reinterpret_cast<uint32_t*>(flags + lvl_idx(level + 1) + 4 * (4 * w + j)) |= 0x01010101u;
+    }
+}
+
+// One level of parents (levels above kBandMaxLevel), values only (k_extra_sig_level set the
+// children's flags).
 template <typename T, bool MW>
 __global__ void __launch_bounds__(256) k_decode_level(Hier<T> hr, Scalars<T>* sc, int L, int level, T eps)
 {
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned done = 0;
-    if (idx < (1 << (2 * level))) decode_parent<T, MW>(hr, sc, L, level, idx, eps, done);
+    if (idx < (1 << (2 * level))) decode_parent<T, MW, false>(hr, sc, L, level, idx, eps, done);
     const unsigned tot = __reduce_add_sync(0xffffffffu, done);
     if ((threadIdx.x & 31) == 0 && tot)
     {
@@ -471,7 +508,8 @@ __global__ void __launch_bounds__(256) k_decode_level(Hier<T> hr, Scalars<T>* sc
 // significant itself (FULL encode: clear their flag bits) and lists the significant ones
 // in shared memory; the warp's lanes then take the listed parents in turn. A level of 4M
 // parents with a handful significant costs 512K threads that read 8 bytes each instead of
-// 4M threads. Op 0: FULL encode, 1: scale-only re-encode, 2: decode.
+// 4M threads. Op 0: FULL encode, 1: scale-only re-encode, 2: decode (values only, as
+// k_decode_level).
 template <typename T, bool MW, int OP>
 __global__ void __launch_bounds__(256) k_level_sparse(Hier<T> hr, Scalars<T>* sc, int L, int level, T eps)
 {
@@ -510,7 +548,7 @@ __global__ void __launch_bounds__(256) k_level_sparse(Hier<T> hr, Scalars<T>* sc
         const int idx = list[warp][e];
         if (OP == 0) encode_parent<T, MW, true>(hr, sc, L, level, idx, eps, done);
         else if (OP == 1) encode_parent<T, MW, false>(hr, sc, L, level, idx, eps, done);
-        else decode_parent<T, MW>(hr, sc, L, level, idx, eps, done);
+        else decode_parent<T, MW, false>(hr, sc, L, level, idx, eps, done);
     }
     const unsigned tot = __reduce_add_sync(0xffffffffu, done);
     if (lane == 0 && tot)

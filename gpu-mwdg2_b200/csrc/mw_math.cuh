@@ -20,7 +20,10 @@ enum Inlet : int { CLOSED = 1, FREE = 2, HFIX = 4, HVAR = 8, QFIX = 16, QVAR = 3
 enum : uint8_t {
     F_SIG = 1,   // significant: the node is refined (its children exist in the tree)
     F_ENC = 2,   // details of this node were computed by this step's encode
-    F_PRE = 4    // preflagged: always significant once encoded (mra/preflag_*.cu)
+    F_PRE = 4,   // preflagged: always significant once encoded (mra/preflag_*.cu)
+    F_XS = 8     // encoded this step with details reaching the extra-significance threshold
+                 // (mra/extra_significance_kernel.cu): a significant parent with F_XS makes
+                 // its four children significant
 };
 
 // ---------------------------------------------------------------- indexing

@@ -136,6 +136,11 @@ private:
     uint8_t* dry_ = nullptr;            // dry marks of one RK stage (k_stage_wet -> k_stage_dry)
     cudaStream_t st2_ = nullptr;        // the wet-list kernels, beside the dry-leaf writers
     cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
+    // the value decode of the levels above the bands, beside the leaf topology (its own
+    // stream and events: sharing the stage kernels' ones ties the two forks together in
+    // the captured graph and serialised the RK stage-1 branches)
+    cudaStream_t st_dec_ = nullptr;
+    cudaEvent_t ev_dec_fork_ = nullptr, ev_dec_join_ = nullptr;
     // A step after the first is captured once per variant (which RK stages take the wet
     // list) and replayed as one CUDA graph; capture failures fall back to direct launches.
     bool use_graphs_ = true, capturing_ = false;
@@ -280,6 +285,9 @@ template <typename T> void Sim<T>::release()
     if (ev_fork_) { cudaEventDestroy(ev_fork_); ev_fork_ = nullptr; }
     if (ev_join_) { cudaEventDestroy(ev_join_); ev_join_ = nullptr; }
     if (st2_) { cudaStreamDestroy(st2_); st2_ = nullptr; }
+    if (ev_dec_fork_) { cudaEventDestroy(ev_dec_fork_); ev_dec_fork_ = nullptr; }
+    if (ev_dec_join_) { cudaEventDestroy(ev_dec_join_); ev_dec_join_ = nullptr; }
+    if (st_dec_) { cudaStreamDestroy(st_dec_); st_dec_ = nullptr; }
     if (st_) { cudaStreamDestroy(st_); st_ = nullptr; }
 }
 
@@ -378,6 +386,9 @@ template <typename T> mwdg2_status Sim<T>::init(const char* par, const mwdg2_opt
         CU(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming));
         CU(cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming));
     }
+    CU(cudaStreamCreateWithFlags(&st_dec_, cudaStreamNonBlocking));
+    CU(cudaEventCreateWithFlags(&ev_dec_fork_, cudaEventDisableTiming));
+    CU(cudaEventCreateWithFlags(&ev_dec_join_, cudaEventDisableTiming));
     if (mwdg2_status s = dalloc(d_args_, 1)) return s;
     CU(cudaMallocHost(&h_args_, sizeof(mw::StepArgs<T>)));
     {
@@ -561,26 +572,40 @@ template <typename T> mwdg2_status Sim<T>::enqueue_device()
             else mw::k_decode_band<T, false><<<b.grid, 256, 0, st_>>>(hr_, sc_, L_, b.lo, b.depth, eps);
             ++launches_;
         }
-        for (int level = mw::kBandMaxLevel + 1; level < L_; ++level)
+        // the levels above the bands: their flags first (extra significance from F_XS), so
+        // the flags are final and the leaf topology below can run beside the value decode
+        for (int level = mw::kBandMaxLevel + 1; level <= L_ - 2; ++level)
         {
-            if (sparse_level(level))
-            {
-                const int nb = grid_for(((int64_t)1 << (2 * level)) / 8, 256, 1 << 30);
-                if (mw) mw::k_level_sparse<T, true, 2><<<nb, 256, 0, st_>>>(hr_, sc_, L_, level, eps);
-                else mw::k_level_sparse<T, false, 2><<<nb, 256, 0, st_>>>(hr_, sc_, L_, level, eps);
-            }
-            else
-            {
-                const int nb = grid_for((int64_t)1 << (2 * level), 256, 1 << 30);
-                if (mw) mw::k_decode_level<T, true><<<nb, 256, 0, st_>>>(hr_, sc_, L_, level, eps);
-                else mw::k_decode_level<T, false><<<nb, 256, 0, st_>>>(hr_, sc_, L_, level, eps);
-            }
+            mw::k_extra_sig_level<T><<<grid_for((int64_t)1 << (2 * level - 2), 256, 1 << 30), 256, 0, st_>>>(hr_.flags, sc_,
+                                                                                                            L_, level, eps);
             ++launches_;
         }
     }
     rec(3);
     if (remesh)
     {
+        const bool fork = L_ - 1 > mw::kBandMaxLevel;
+        if (fork)
+        {
+            CU(cudaEventRecord(ev_dec_fork_, st_));
+            CU(cudaStreamWaitEvent(st_dec_, ev_dec_fork_, 0));
+            for (int level = mw::kBandMaxLevel + 1; level < L_; ++level)
+            {
+                if (sparse_level(level))
+                {
+                    const int nb = grid_for(((int64_t)1 << (2 * level)) / 8, 256, 1 << 30);
+                    if (mw) mw::k_level_sparse<T, true, 2><<<nb, 256, 0, st_dec_>>>(hr_, sc_, L_, level, eps);
+                    else mw::k_level_sparse<T, false, 2><<<nb, 256, 0, st_dec_>>>(hr_, sc_, L_, level, eps);
+                }
+                else
+                {
+                    const int nb = grid_for((int64_t)1 << (2 * level), 256, 1 << 30);
+                    if (mw) mw::k_decode_level<T, true><<<nb, 256, 0, st_dec_>>>(hr_, sc_, L_, level, eps);
+                    else mw::k_decode_level<T, false><<<nb, 256, 0, st_dec_>>>(hr_, sc_, L_, level, eps);
+                }
+                ++launches_;
+            }
+        }
         // 96 threads: the count reads 85 flag words of the tile's subtree
         mw::k_tile_count<<<ntiles_, 96, 0, st_>>>(hr_.flags, L_, tile_counts_);
         ++launches_;
@@ -588,6 +613,11 @@ template <typename T> mwdg2_status Sim<T>::enqueue_device()
         ++launches_;
         mw::k_tile_emit<T, false><<<ntiles_, mw::kTileThreads, 0, st_>>>(lf_, hr_.flags, tile_counts_, L_, M_, cs_.xsz, cs_.ysz);
         ++launches_;
+        if (fork)
+        {
+            CU(cudaEventRecord(ev_dec_join_, st_dec_));
+            CU(cudaStreamWaitEvent(st_, ev_dec_join_, 0));
+        }
     }
     rec(4);
     const bool fric = cs_.manning > T(0);
