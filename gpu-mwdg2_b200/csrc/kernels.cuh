@@ -133,7 +133,7 @@ __device__ __forceinline__ void block_max_atomic(T (&v)[N], T* const (&dst)[N])
 // ---------------------------------------------------------------- step bookkeeping
 // carry: the maxima come from the previous step's final RK stage (MWDG2 after its first
 // step); otherwise k_maxes_reinsert computes them.
-template <typename T> __global__ void k_step_begin(Scalars<T>* sc, bool carry)
+template <typename T> __device__ __forceinline__ void step_begin(Scalars<T>* sc, bool carry)
 {
     sc->max_eta = carry ? sc->next_max[0] : T(0);
     sc->max_h = carry ? sc->next_max[1] : T(0);
@@ -150,6 +150,40 @@ template <typename T> __global__ void k_step_begin(Scalars<T>* sc, bool carry)
     sc->xs_factor = pow(T(2.0), T(1.5) + 1);
 #pragma unroll
     for (int l = 0; l < 16; ++l) sc->sig_level[l] = 0;
+}
+template <typename T> __global__ void k_step_begin(Scalars<T>* sc, bool carry) { step_begin(sc, carry); }
+
+// Point source i into the finest level (mra/reinsert_point_srcs.cu:3-29).
+template <typename T> __device__ __forceinline__ void point_source(const Hier<T>& hr, const Src<T>& src, T dt, T dx, int L)
+{
+    const int h = lvl_idx(L) + src.code;
+    const int t = src.type;
+    if (t == HFIX || t == HVAR) hr.s[0][0][h] = src.value;
+    else if (t == QFIX || t == QVAR) hr.s[0][0][h] += src.value * dt / dx;
+}
+
+// A step's first kernel (one block): resets the step's scalars, copies the step's
+// arguments (dt, boundary values), which it reads straight from pinned host memory, to
+// device memory for the later kernels, and applies the point sources, whose values it also
+// reads from pinned host memory. One launch in place of two copies and two kernels.
+template <typename T>
+__global__ void k_step_open(Scalars<T>* sc, bool carry, const StepArgs<T>* h_args, StepArgs<T>* d_args, const Src<T>* h_src,
+                            int nsrc, Hier<T> hr, T dx, int L)
+{
+    __shared__ T s_dt;
+    // the first source of each thread is read before the barrier, beside the arguments
+    Src<T> first{};
+    if ((int)threadIdx.x < nsrc) first = h_src[threadIdx.x];
+    if (threadIdx.x == 0)
+    {
+        const StepArgs<T> a = *h_args;
+        *d_args = a;
+        s_dt = a.dt;
+        step_begin(sc, carry);
+    }
+    __syncthreads();
+    if ((int)threadIdx.x < nsrc) point_source(hr, first, s_dt, dx, L);
+    for (int i = threadIdx.x + blockDim.x; i < nsrc; i += blockDim.x) point_source(hr, h_src[i], s_dt, dx, L);
 }
 
 // Maxima of the leaf state (mra/get_max_scale_coeffs.cu:3-27, with the reference's
@@ -191,17 +225,12 @@ __global__ void __launch_bounds__(256) k_maxes_reinsert(Leaves<T> lf, Hier<T> hr
     block_max_atomic<T, 4>(v, dst);
 }
 
-// Point sources into the finest level (mra/reinsert_point_srcs.cu:3-29).
+// Point sources into the finest level, from device copies of the step's arguments.
 template <typename T>
 __global__ void k_point_sources(Hier<T> hr, const Src<T>* src, int n, const StepArgs<T>* args, T dx, int L)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const T dt = args->dt;
-    const int h = lvl_idx(L) + src[i].code;
-    const int t = src[i].type;
-    if (t == HFIX || t == HVAR) hr.s[0][0][h] = src[i].value;
-    else if (t == QFIX || t == QVAR) hr.s[0][0][h] += src[i].value * dt / dx;
+    if (i < n) point_source(hr, src[i], args->dt, dx, L);
 }
 
 // ---------------------------------------------------------------- multiresolution analysis

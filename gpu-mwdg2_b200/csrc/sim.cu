@@ -130,6 +130,10 @@ private:
     int32_t* wet_list_ = nullptr;       // leaves that are not dry in an RK stage
     mw::StepArgs<T>* d_args_ = nullptr; // this step's dt and boundary values (device)
     mw::StepArgs<T>* h_args_ = nullptr; // pinned; copied to d_args_ by the step's first operation
+    // device addresses of the pinned h_args_ / h_src_ (mapped host memory), read directly by
+    // k_step_open; null where the mapping is not available (then copies and two kernels)
+    const mw::StepArgs<T>* m_args_ = nullptr;
+    const mw::Src<T>* m_src_ = nullptr;
     // Per-leaf kernels run persistent grids (grid-stride loops): SMs x resident blocks of each
     // kernel, so a step's launches do not depend on the leaf count and can be replayed.
     int grid_leaf_ = 0, grid_wet_ = 0, grid_dry_ = 0, grid_stage_ = 0;
@@ -392,6 +396,11 @@ template <typename T> mwdg2_status Sim<T>::init(const char* par, const mwdg2_opt
     if (mwdg2_status s = dalloc(d_args_, 1)) return s;
     CU(cudaMallocHost(&h_args_, sizeof(mw::StepArgs<T>)));
     {
+        void* m = nullptr;
+        if (cudaHostGetDevicePointer(&m, h_args_, 0) == cudaSuccess) m_args_ = static_cast<const mw::StepArgs<T>*>(m);
+        cudaGetLastError();
+    }
+    {
         // persistent grids: SMs x resident blocks of the kernel
         auto resident = [&](auto kernel, int threads) {
             int b = 0;
@@ -409,6 +418,9 @@ template <typename T> mwdg2_status Sim<T>::init(const char* par, const mwdg2_opt
     {
         if (mwdg2_status s = dalloc(d_src_, nsrc)) return s;
         CU(cudaMallocHost(&h_src_, sizeof(mw::Src<T>) * nsrc));
+        void* m = nullptr;
+        if (cudaHostGetDevicePointer(&m, h_src_, 0) == cudaSuccess) m_src_ = static_cast<const mw::Src<T>*>(m);
+        cudaGetLastError();
     }
     if (nst > 0)
     {
@@ -542,22 +554,32 @@ template <typename T> mwdg2_status Sim<T>::enqueue_device()
     };
     launches_ = 0;
     rec(0);
-    CU(cudaMemcpyAsync(d_args_, h_args_, sizeof(mw::StepArgs<T>), cudaMemcpyHostToDevice, st_));
     // MWDG2 after its first step: the previous step's stage 2 re-inserted the state into
     // the hierarchy and reduced its maxima, so only the point sources remain here
     const bool carry = mw && !first_;
-    mw::k_step_begin<T><<<1, 1, 0, st_>>>(sc_, carry);
-    ++launches_;
-    const int nfix = first_ ? (int)F_ : -1;
-    if (mw) { if (!carry) { mw::k_maxes_reinsert<T, true><<<grid_leaf_, 256, 0, st_>>>(lf_, hr_, sc_, nfix, false); ++launches_; } }
-    else { mw::k_maxes_reinsert<T, false><<<grid_leaf_, 256, 0, st_>>>(lf_, hr_, sc_, nfix, !first_); ++launches_; }
-    // point sources
     const int nsrc = (int)cs_.srcs.size();
-    if (nsrc > 0)
+    // one kernel where nothing runs between the scalar reset and the point sources (MWDG2
+    // after its first step) and the pinned buffers are mapped; else copies and two kernels
+    const bool open = carry && m_args_ && (nsrc == 0 || m_src_);
+    if (open)
     {
-        CU(cudaMemcpyAsync(d_src_, h_src_, sizeof(mw::Src<T>) * nsrc, cudaMemcpyHostToDevice, st_));
-        mw::k_point_sources<T><<<(nsrc + 127) / 128, 128, 0, st_>>>(hr_, d_src_, nsrc, d_args_, cs_.dx, L_);
+        mw::k_step_open<T><<<1, 128, 0, st_>>>(sc_, carry, m_args_, d_args_, m_src_, nsrc, hr_, cs_.dx, L_);
         ++launches_;
+    }
+    else
+    {
+        CU(cudaMemcpyAsync(d_args_, h_args_, sizeof(mw::StepArgs<T>), cudaMemcpyHostToDevice, st_));
+        mw::k_step_begin<T><<<1, 1, 0, st_>>>(sc_, carry);
+        ++launches_;
+        const int nfix = first_ ? (int)F_ : -1;
+        if (mw) { if (!carry) { mw::k_maxes_reinsert<T, true><<<grid_leaf_, 256, 0, st_>>>(lf_, hr_, sc_, nfix, false); ++launches_; } }
+        else { mw::k_maxes_reinsert<T, false><<<grid_leaf_, 256, 0, st_>>>(lf_, hr_, sc_, nfix, !first_); ++launches_; }
+        if (nsrc > 0)
+        {
+            CU(cudaMemcpyAsync(d_src_, h_src_, sizeof(mw::Src<T>) * nsrc, cudaMemcpyHostToDevice, st_));
+            mw::k_point_sources<T><<<(nsrc + 127) / 128, 128, 0, st_>>>(hr_, d_src_, nsrc, d_args_, cs_.dx, L_);
+            ++launches_;
+        }
     }
     rec(1);
     const bool remesh = (eps > T(0) || first_);
