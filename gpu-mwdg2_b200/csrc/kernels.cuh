@@ -47,6 +47,7 @@ template <typename T> struct Scalars
     int32_t wet[2];                   // leaves not dry in RK stage 1 / stage 2 (wet-list lengths)
     T next_max[4];                    // maxima of the state at the end of the step (eta, h, qx, z)
     T xs_factor;                      // 2^(M_BAR+1) of the extra-significance threshold (extra_eps)
+    int32_t min_leaf;                 // lowest leaf level of this step's tree (k_tile_emit)
 };
 
 template <typename T> struct Params
@@ -145,6 +146,7 @@ template <typename T> __device__ __forceinline__ void step_begin(Scalars<T>* sc,
     sc->dt_min = (sizeof(T) == 8) ? T(1.0e308) : T(3.0e38);
     sc->enc = 0; sc->enc2 = 0; sc->dec = 0;
     sc->wet[0] = 0; sc->wet[1] = 0;
+    sc->min_leaf = 1 << 30;
     // the expression of mra/extra_significance_kernel.cu, evaluated once per step instead of
     // once per parent (the same expression on the device gives the same bits everywhere)
     sc->xs_factor = pow(T(2.0), T(1.5) + 1);
@@ -279,6 +281,14 @@ template <typename T> __device__ __forceinline__ T extra_eps(T eps, int L, int l
     return eps_local * sc->xs_factor;
 }
 
+// scale_only_needed: the scale-only re-encode of the stage hierarchy (U*) produces the
+// values RK stage 2 reads where a leaf's neighbour id is a significant parent (the leaf's
+// neighbours across that face are finer). A neighbour id sits at level min(own leaf level,
+// adjacent leaf's level), so never at a level coarser than the step's coarsest leaf
+// (Scalars::min_leaf, set by k_tile_emit), and nothing else reads the stage hierarchy's
+// parents. The scale-only kernels therefore skip parent levels below min_leaf, whose
+// values nothing would read; every output is the same bits.
+
 // Encode one parent (mra/encode_flow_kernel_{mw,hw}.cu), threshold it and OR in the
 // children's significance (mra/regularisation_kernel.cu). FULL = false re-encodes scale
 // coefficients of significant parents only (run_simulation.cu:573-588).
@@ -371,6 +381,7 @@ constexpr int kBandMaxLevel = 9;
 template <typename T, bool MW, bool FULL>
 __global__ void __launch_bounds__(256) k_encode_level(Hier<T> hr, Scalars<T>* sc, int L, int level, T eps)
 {
+    if (!FULL && sc->min_leaf > level) return;   // see scale_only_needed
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned done = 0;
     if (idx < (1 << (2 * level))) encode_parent<T, MW, FULL>(hr, sc, L, level, idx, eps, done);
@@ -383,6 +394,7 @@ __global__ void __launch_bounds__(256) k_encode_level(Hier<T> hr, Scalars<T>* sc
 template <typename T, bool MW, bool FULL>
 __global__ void __launch_bounds__(256) k_encode_band(Hier<T> hr, Scalars<T>* sc, int L, int lo, int depth, T eps)
 {
+    if (!FULL && sc->min_leaf > lo + depth - 1) return;   // see scale_only_needed
     unsigned done = 0;
     for (int l = lo + depth - 1; l >= lo; --l)
     {
@@ -542,6 +554,7 @@ __global__ void __launch_bounds__(256) k_decode_level(Hier<T> hr, Scalars<T>* sc
 template <typename T, bool MW, int OP>
 __global__ void __launch_bounds__(256) k_level_sparse(Hier<T> hr, Scalars<T>* sc, int L, int level, T eps)
 {
+    if (OP == 1 && sc->min_leaf > level) return;   // see scale_only_needed
     __shared__ int list[8][256];   // per warp: up to 32 lanes x 8 parents
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t first = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * 8;
@@ -819,7 +832,7 @@ __device__ __forceinline__ void emit_single_leaf(const Leaves<T>& lf, const uint
 // is not -1 (-1: the leaf's own level).
 template <typename T, bool NBL>
 __global__ void __launch_bounds__(kTileThreads) k_tile_emit(Leaves<T> lf, const uint8_t* flags, const int32_t* offsets,
-                                                            int L, int M, int xsz, int ysz)
+                                                            int L, int M, int xsz, int ysz, int32_t* min_leaf)
 {
     constexpr int D = kTileDepth, kCells = 1 << (2 * D);
     const int Tl = L - D;
@@ -832,6 +845,7 @@ __global__ void __launch_bounds__(kTileThreads) k_tile_emit(Leaves<T> lf, const 
     __shared__ uint8_t node_lvl[kCells / 4];
     __shared__ uint16_t start_of[kCells];             // tile-local start cell of the leaf of each rank
     __shared__ int32_t warp_starts[kTileThreads / 32];
+    __shared__ int32_t warp_min[kTileThreads / 32];
     // leaf levels of the cells just outside the tile (N, E, S, W), indexed by the dilated
     // tile-local coordinate along the side (x bits for N/S, y bits shifted down for E/W)
     __shared__ uint8_t halo[4][(kXBits & (kCells - 1)) + 1];
@@ -839,11 +853,15 @@ __global__ void __launch_bounds__(kTileThreads) k_tile_emit(Leaves<T> lf, const 
     if (k < Tl)
     {
         if ((tcode & ((1 << (2 * (Tl - k))) - 1)) == 0)
+        {
+            if (min_leaf && threadIdx.x == 0) atomicMin(min_leaf, k);
             emit_single_leaf<T, NBL>(lf, flags, L, M, xsz, ysz, off, lvl_idx(k) + (tcode >> (2 * (Tl - k))), k);
+        }
         return;
     }
     if (k == Tl)
     {
+        if (min_leaf && threadIdx.x == 0) atomicMin(min_leaf, Tl);
         emit_single_leaf<T, NBL>(lf, flags, L, M, xsz, ysz, off, lvl_idx(Tl) + tcode, Tl);
         return;
     }
@@ -906,7 +924,9 @@ __global__ void __launch_bounds__(kTileThreads) k_tile_emit(Leaves<T> lf, const 
         const int v = __shfl_up_sync(0xffffffffu, incl, o);
         if (lane >= o) incl += v;
     }
+    const int wmin = __reduce_min_sync(0xffffffffu, qlev);
     if (lane == 31) warp_starts[warp] = incl;
+    if (lane == 0) warp_min[warp] = wmin;
     __syncthreads();
     int rank = incl - nstart, total = 0;
 #pragma unroll
@@ -915,6 +935,14 @@ __global__ void __launch_bounds__(kTileThreads) k_tile_emit(Leaves<T> lf, const 
         const int c = warp_starts[w];
         rank += (w < warp) ? c : 0;
         total += c;
+    }
+    // the tree's coarsest leaf level (Scalars::min_leaf), one atomic per tile that lowers it
+    if (min_leaf && threadIdx.x == 0)
+    {
+        int bmin = warp_min[0];
+#pragma unroll
+        for (int w = 1; w < kTileThreads / 32; ++w) bmin = min(bmin, warp_min[w]);
+        if (bmin < *min_leaf) atomicMin(min_leaf, bmin);
     }
     if (nstart == 4)
     {

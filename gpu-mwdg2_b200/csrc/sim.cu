@@ -633,7 +633,8 @@ template <typename T> mwdg2_status Sim<T>::enqueue_device()
         ++launches_;
         mw::k_tile_scan<T><<<1, 1024, 0, st_>>>(tile_counts_, ntiles_, sc_);
         ++launches_;
-        mw::k_tile_emit<T, false><<<ntiles_, mw::kTileThreads, 0, st_>>>(lf_, hr_.flags, tile_counts_, L_, M_, cs_.xsz, cs_.ysz);
+        mw::k_tile_emit<T, false><<<ntiles_, mw::kTileThreads, 0, st_>>>(lf_, hr_.flags, tile_counts_, L_, M_, cs_.xsz, cs_.ysz,
+                                                                        &sc_->min_leaf);
         ++launches_;
         if (fork)
         {
