@@ -831,7 +831,7 @@ __device__ __forceinline__ void emit_single_leaf(const Leaves<T>& lf, const uint
 // NBL: also write the neighbours' levels (lf.nbl), which level_of(id) gives wherever the id
 // is not -1 (-1: the leaf's own level).
 template <typename T, bool NBL>
-__global__ void __launch_bounds__(kTileThreads) k_tile_emit(Leaves<T> lf, const uint8_t* flags, const int32_t* offsets,
+__global__ void __launch_bounds__(kTileThreads, 8) k_tile_emit(Leaves<T> lf, const uint8_t* flags, const int32_t* offsets,
                                                             int L, int M, int xsz, int ysz, int32_t* min_leaf)
 {
     constexpr int D = kTileDepth, kCells = 1 << (2 * D);
