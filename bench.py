@@ -147,7 +147,7 @@ class Clocks:
 # summed, divided by the step's leaves) from a one-pass ncu launch list of this workload
 # (4096^2, FP32, 3.0 M leaves). Keyed by (solver, P, timing phase).
 TRAFFIC_SOURCE = "ncu launch list (dram bytes, 1 pass) of the same workload, per leaf x leaves"
-TRAFFIC_B_PER_LEAF: dict = {("mwdg2", 4, 3): 10.8, ("mwdg2", 4, 4): 224.9, ("mwdg2", 4, 6): 184.0}
+TRAFFIC_B_PER_LEAF: dict = {("mwdg2", 4, 3): 6.0, ("mwdg2", 4, 4): 224.4, ("mwdg2", 4, 6): 183.9}
 
 
 def peaks() -> tuple[float, str]:
