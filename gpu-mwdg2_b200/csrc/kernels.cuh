@@ -569,7 +569,9 @@ __global__ void __launch_bounds__(256) k_level_sparse(Hier<T> hr, Scalars<T>* sc
         {
             const uint32_t f = ((j < 4 ? w.x : w.y) >> (8 * (j & 3))) & 0xffu;
             if (f & F_SIG) sig |= 1u << j;
-            else if (OP == 0) encode_parent<T, MW, true>(hr, sc, L, level, (int)(first + j), eps, done);
+            // FULL encode of a parent that was not significant: only its flag changes (its
+            // encode / extra-significance bits from the last step clear, the preflag stays)
+            else if (OP == 0 && (f & ~(uint32_t)F_PRE)) hr.flags[lvl_idx(level) + first + j] = (uint8_t)(f & F_PRE);
         }
     }
     const int c = __popc(sig);
