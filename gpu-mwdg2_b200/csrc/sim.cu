@@ -74,6 +74,7 @@ struct SimBase
     virtual mwdg2_status hierarchy(int f, int m, double* out, int64_t cap) = 0;
     virtual mwdg2_status stage(double* out, int n) = 0;
     virtual mwdg2_status timing(double* out, int n) = 0;
+    virtual mwdg2_status set_timing(int mode) = 0;
     virtual mwdg2_status counters(int64_t* out, int n) = 0;
 };
 
@@ -102,6 +103,7 @@ public:
     mwdg2_status hierarchy(int f, int m, double* out, int64_t cap) override;
     mwdg2_status stage(double* out, int n) override;
     mwdg2_status timing(double* out, int n) override;
+    mwdg2_status set_timing(int mode) override;
     mwdg2_status counters(int64_t* out, int n) override;
 
 private:
@@ -159,7 +161,7 @@ private:
     }
     int variant_key() const
     {
-        int key = (mw_ && use_list(1) ? 1 : 0) | (mw_ && use_list(2) ? 2 : 0);
+        int key = (mw_ && use_list(1) ? 1 : 0) | (mw_ && use_list(2) ? 2 : 0) | (timed_ ? 1 << 24 : 0);
         for (int level = mw::kBandMaxLevel + 1; level < L_; ++level)
             if (sparse_level(level)) key |= 4 << (level - mw::kBandMaxLevel - 1);
         return key;
@@ -177,8 +179,13 @@ private:
     T* d_raster_ = nullptr;             // raster rows (saveint raster maps)
     mw::Params<T> P_{};
     // timing
-    bool timed_ = false;
+    // timing_mode_ 2 (phases): events between the step's phases, captured into the step's
+    // graph as event nodes (each breaks the launch pipelining of the graph, ~10 us);
+    // 1 (step): two stream events around the step, outside any graph; 0: none
+    int timing_mode_ = 0;
+    bool timed_ = false;                // timing_mode_ == 2
     cudaEvent_t ev_[9] = {};
+    cudaEvent_t ev_step_[2] = {};
     double last_ms_[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     int64_t last_cnt_[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     int launches_ = 0;
@@ -278,6 +285,7 @@ template <typename T> void Sim<T>::release()
 {
     if (device_ >= 0) cudaSetDevice(device_);
     for (auto& e : ev_) if (e) { cudaEventDestroy(e); e = nullptr; }
+    for (auto& e : ev_step_) if (e) { cudaEventDestroy(e); e = nullptr; }
     for (auto& g : graphs_) cudaGraphExecDestroy(g.second.exec);
     graphs_.clear();
     if (h_args_) { cudaFreeHost(h_args_); h_args_ = nullptr; }
@@ -495,8 +503,7 @@ template <typename T> mwdg2_status Sim<T>::init(const char* par, const mwdg2_opt
         int32_t zero = 0;
         CU(cudaMemcpy(&sc_->status, &zero, sizeof(zero), cudaMemcpyHostToDevice));
     }
-    timed_ = (o.verbose >= 2);
-    if (timed_) for (auto& e : ev_) CU(cudaEventCreate(&e));
+    if (mwdg2_status st = set_timing(o.verbose >= 2 ? 2 : 0)) return st;
     t_start_ = std::chrono::steady_clock::now();
     return MWDG2_OK;
 }
@@ -513,9 +520,17 @@ template <typename T> mwdg2_status Sim<T>::launch_step()
         if (cs_.bnd[d].varying) cs_.bnd[d].inlet = cs_.bnd[d].series.at(time_);
     h_args_->dt = dt_;
     h_args_->B = bnd_now();
+    // step timing: stream events right around the step's device work (after any capture)
+    auto rec_step = [&](int k) { if (timing_mode_ == 1) cudaEventRecord(ev_step_[k], st_); };
+    auto direct = [&]() {
+        rec_step(0);
+        const mwdg2_status st = enqueue_device();
+        rec_step(1);
+        return st;
+    };
     // the first step has its own kernels (initial maxima, full encode); later steps differ
     // only in which RK stages take the wet list
-    if (!use_graphs_ || first_) return enqueue_device();
+    if (!use_graphs_ || first_) return direct();
     const int key = variant_key();
     if (!graphs_.count(key))
     {
@@ -533,12 +548,14 @@ template <typename T> mwdg2_status Sim<T>::launch_step()
         {
             if (ge) cudaGraphExecDestroy(ge);
             use_graphs_ = false;
-            return enqueue_device();
+            return direct();
         }
         graphs_[key] = Captured{ge, launches_};
     }
     launches_ = graphs_[key].launches;
+    rec_step(0);
     CU(cudaGraphLaunch(graphs_[key].exec, st_));
+    rec_step(1);
     return MWDG2_OK;
 }
 
@@ -690,6 +707,12 @@ template <typename T> mwdg2_status Sim<T>::collect_step()
             cudaEventElapsedTime(&ms, ev_[pairs[k][0]], ev_[pairs[k][1]]);
             last_ms_[k] = ms;
         }
+    }
+    else if (timing_mode_ == 1)
+    {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ev_step_[0], ev_step_[1]);
+        last_ms_[7] = ms;
     }
     if (mw)
         for (int s = 0; s < 2; ++s) wet_prev_[s] = sc_host_->wet[s];
@@ -1193,6 +1216,20 @@ template <typename T> mwdg2_status Sim<T>::timing(double* out, int n)
     return MWDG2_OK;
 }
 
+template <typename T> mwdg2_status Sim<T>::set_timing(int mode)
+{
+    if (mode < 0 || mode > 2) return set_err(MWDG2_ERR_ARG, "set_timing: mode 0, 1 or 2");
+    CU(cudaSetDevice(device_));
+    if (mode == 2 && !ev_[0])
+        for (auto& e : ev_) CU(cudaEventCreate(&e));
+    if (mode == 1 && !ev_step_[0])
+        for (auto& e : ev_step_) CU(cudaEventCreate(&e));
+    timing_mode_ = mode;
+    timed_ = (mode == 2);
+    for (auto& v : last_ms_) v = 0.0;
+    return MWDG2_OK;
+}
+
 template <typename T> mwdg2_status Sim<T>::counters(int64_t* out, int n)
 {
     for (int i = 0; i < n && i < 10; ++i) out[i] = last_cnt_[i];
@@ -1339,6 +1376,12 @@ mwdg2_status mwdg2_last_step_timing(mwdg2_sim* s, double* out, int n)
 {
     if (!s || !out) return set_err(MWDG2_ERR_ARG, "null argument");
     return s->impl->timing(out, n);
+}
+
+mwdg2_status mwdg2_set_timing(mwdg2_sim* s, int mode)
+{
+    if (!s) return set_err(MWDG2_ERR_ARG, "null handle");
+    return s->impl->set_timing(mode);
 }
 
 mwdg2_status mwdg2_last_step_counters(mwdg2_sim* s, int64_t* out, int n)

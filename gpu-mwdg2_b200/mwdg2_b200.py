@@ -78,6 +78,7 @@ def lib():
         L.mwdg2_get_hierarchy.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp, ctypes.c_int64]
         L.mwdg2_read_stage.argtypes = [vp, dp, ctypes.c_int]
         L.mwdg2_last_step_timing.argtypes = [vp, dp, ctypes.c_int]
+        L.mwdg2_set_timing.argtypes = [vp, ctypes.c_int]
         L.mwdg2_last_step_counters.argtypes = [vp, i64p, ctypes.c_int]
         L.mwdg2_destroy.argtypes = [vp]
         L.mwdg2_batch_create.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(Opts),
@@ -88,7 +89,8 @@ def lib():
         L.mwdg2_batch_destroy.argtypes = [vp]
         for name in ("mwdg2_create", "mwdg2_step", "mwdg2_run", "mwdg2_run_simulation", "mwdg2_info",
                      "mwdg2_get_leaves", "mwdg2_get_state", "mwdg2_get_sig", "mwdg2_get_hierarchy",
-                     "mwdg2_read_stage", "mwdg2_last_step_timing", "mwdg2_last_step_counters", "mwdg2_batch_create",
+                     "mwdg2_read_stage", "mwdg2_last_step_timing", "mwdg2_set_timing", "mwdg2_last_step_counters",
+                     "mwdg2_batch_create",
                      "mwdg2_batch_step", "mwdg2_batch_run", "mwdg2_batch_member"):
             getattr(L, name).restype = ctypes.c_int
         _lib = L
@@ -124,10 +126,10 @@ class Simulation:
 
     def __init__(self, par: str, precision: int = 64, epsilon: float | None = None,
                  solver: str | None = None, dirroot: str | None = None, write_outputs: bool = False,
-                 device: int = -1, timing: bool = False):
+                 device: int = -1, timing: bool | str = False):
         self.par = os.path.abspath(par)
         self.dir = os.path.dirname(self.par)
-        o = _opts(precision, epsilon, solver, dirroot, write_outputs, device, timing)
+        o = _opts(precision, epsilon, solver, dirroot, write_outputs, device, timing is True or timing == "phases")
         self._dirroot = o.dirroot
         h = ctypes.c_void_p()
         with _cwd(self.dir):
@@ -135,6 +137,8 @@ class Simulation:
         self._h = h
         self._owned = True
         self.precision = precision
+        if timing == "step":
+            self.set_timing("step")
 
     @classmethod
     def _view(cls, handle: ctypes.c_void_p, par: str, precision: int, owner) -> "Simulation":
@@ -217,6 +221,13 @@ class Simulation:
         out = np.zeros(max(1, n_points))
         _check(lib().mwdg2_read_stage(self._h, _p(out, ctypes.c_double), n_points))
         return out[:n_points]
+
+    def set_timing(self, mode: str | bool):
+        """Timing of the following steps (mwdg2_set_timing): "step" (two events around each
+        step, no cost to it: last_step_timing()[7]), "phases" or True (events between the
+        phases inside the step's graph, ~10 us each: all eight values), None or False (none)."""
+        code = {None: 0, False: 0, "step": 1, "phases": 2, True: 2}[mode]
+        _check(lib().mwdg2_set_timing(self._h, code))
 
     def last_step_timing(self) -> np.ndarray:
         out = np.zeros(8)

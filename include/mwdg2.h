@@ -110,12 +110,19 @@ mwdg2_status mwdg2_read_stage(mwdg2_sim* sim, double* out, int n);
 /* Device timing of the last step's kernels, in milliseconds, by phase:
  * [0] maxima + re-insertion (HWFV1, and MWDG2's first step; later MWDG2 steps take both
  * from the previous stage 2) + point sources, [1] encode + threshold + regularisation,
- * [2] decode + extra significance, [3] leaf topology (tile counts, scan, leaf list and
- * neighbours),
+ * [2] decode bands + extra significance of the upper levels, [3] leaf topology (tile
+ * counts, scan, leaf list and neighbours) beside the value decode of the upper levels,
  * [4] MWDG2 stage 1 (or the HWFV1 update), [5] scale re-encode of the stage-1 result +
  * stage-2 maximum depth, [6] MWDG2 stage 2, [7] whole step including the scalar read-back.
- * Requires opts.verbose >= 2 at create (CUDA events per phase); otherwise zeros. n <= 8. */
+ * Timing mode 2 (phases; opts.verbose >= 2 at create) fills all; mode 1 (step) fills [7];
+ * otherwise zeros. n <= 8. */
 mwdg2_status mwdg2_last_step_timing(mwdg2_sim* sim, double* out, int n);
+
+/* Timing of the following steps: 0 none; 1 step (two CUDA events around each step's device
+ * work, outside its captured graph: no effect on the step); 2 phases (events between the
+ * step's phases, captured into the step's graph, which costs ~10 us per phase boundary).
+ * No counterpart in the reference (its timing is host wall time around the loop). */
+mwdg2_status mwdg2_set_timing(mwdg2_sim* sim, int mode);
 
 /* Counters of the last step used for the algorithmic-bytes roofline:
  * [0] parents encoded (E), [1] parents re-encoded scale-only (E2), [2] parents decoded (D),
