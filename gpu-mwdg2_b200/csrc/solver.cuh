@@ -376,12 +376,16 @@ __global__ void __launch_bounds__(256) k_stage_wet(Leaves<T> lf, Hier<T> hin, Sc
         if (i < n)
         {
             const int a = lf.act[i];
-            const int level = lf.lvl[i];
             int32_t nid[4];
 #pragma unroll
             for (int d = 0; d < 4; ++d) nid[d] = lf.nb[d][i];
-            // own and neighbour loads issued together (almost every leaf is dry here)
-            const T e0 = hin.s[0][0][a], z0 = hin.s[3][0][a], qx0 = hin.s[1][0][a], qy0 = hin.s[2][0][a];
+            // own and neighbour loads issued together (almost every leaf is dry here); the
+            // level and the discharges only enter the ghost cells of faces on the border
+            // (ghost_pass)
+            const bool border = (nid[0] == -1) | (nid[1] == -1) | (nid[2] == -1) | (nid[3] == -1);
+            const int level = border ? lf.lvl[i] : 0;
+            const T e0 = hin.s[0][0][a], z0 = hin.s[3][0][a];
+            const T qx0 = border ? hin.s[1][0][a] : T(0.0), qy0 = border ? hin.s[2][0][a] : T(0.0);
             T nbh[4];
 #pragma unroll
             for (int d = 0; d < 4; ++d)
