@@ -389,18 +389,99 @@ __global__ void __launch_bounds__(256) k_encode_level(Hier<T> hr, Scalars<T>* sc
     if ((threadIdx.x & 31) == 0 && tot) atomicAdd(FULL ? &sc->enc : &sc->enc2, (unsigned long long)tot);
 }
 
+// One field of one significant parent's encode: its scale coefficients (stored) and, for
+// FULL, the normalised maximum |detail| of that field (returned; 0 otherwise). The same
+// helper calls in the same order as one field of encode_parent.
+template <typename T, bool MW, bool FULL>
+__device__ __forceinline__ T encode_field(const Hier<T>& hr, const Scalars<T>* sc, int level, int idx, int fld)
+{
+    const int p = lvl_idx(level) + idx;
+    const int c = lvl_idx(level + 1) + 4 * idx;
+    // the field's arrays, chosen without indexing the parameter block by a runtime value
+    T* const a0 = fld == 0 ? hr.s[0][0] : fld == 1 ? hr.s[1][0] : hr.s[2][0];
+    T* const a1 = fld == 0 ? hr.s[0][1] : fld == 1 ? hr.s[1][1] : hr.s[2][1];
+    T* const a2 = fld == 0 ? hr.s[0][2] : fld == 1 ? hr.s[1][2] : hr.s[2][2];
+    T nd = T(0.0);
+    if (MW)
+    {
+        T k[3][4];
+        load4(a0 + c, k[0]); load4(a1 + c, k[1]); load4(a2 + c, k[2]);
+        T s[3];
+        mw_encode_scale(k, s);
+        a0[p] = s[0]; a1[p] = s[1]; a2[p] = s[2];
+        if (FULL)
+        {
+            const T mx = fld == 0 ? fmax(T(1.0), sc->max_eta) : fmax(T(1.0), sc->max_qx);
+            T d[3][3];
+            mw_encode_details(k, d);
+            nd = mw_detail_max(d) / mx;
+        }
+    }
+    else
+    {
+        T k[4];
+        load4(a0 + c, k);
+        a0[p] = hw_scale(k);
+        if (FULL)
+        {
+            const T mx = fld == 0 ? fmax(T(1.0), sc->max_eta) : fmax(T(1.0), sc->max_qx);
+            const T a = hw_alpha(k), b = hw_beta(k), g = hw_gamma(k);
+            T m1 = fmax(fabs(a), fabs(b));
+            m1 = fmax(fabs(g), m1);
+            nd = m1 / mx;
+        }
+    }
+    return nd;
+}
+
 // Encode (FULL: + threshold + regularise; else scale-only re-encode) levels
-// lo + depth - 1 .. lo bottom-up (mra/encode_flow.cu, mra/regularisation.cu).
+// lo + depth - 1 .. lo bottom-up (mra/encode_flow.cu, mra/regularisation.cu). One thread per
+// parent and field (the fields of a parent are independent; one thread doing them in turn
+// waits on three dependent round trips, as a field's stores may alias the next one's
+// loads); the fields' detail norms meet in shared memory and are combined in field order,
+// as encode_parent combines them, before the flags.
 template <typename T, bool MW, bool FULL>
 __global__ void __launch_bounds__(256) k_encode_band(Hier<T> hr, Scalars<T>* sc, int L, int lo, int depth, T eps)
 {
     if (!FULL && sc->min_leaf > lo + depth - 1) return;   // see scale_only_needed
+    static_assert(kBandDepth <= 5, "a band level has at most 4^(kBandDepth - 1) <= 256 parents");
+    __shared__ T s_nd[3][256];
     unsigned done = 0;
     for (int l = lo + depth - 1; l >= lo; --l)
     {
-        const int n = 1 << (2 * (l - lo)), base = (int)blockIdx.x << (2 * (l - lo));
-        for (int k = threadIdx.x; k < n; k += blockDim.x) encode_parent<T, MW, FULL>(hr, sc, L, l, base + k, eps, done);
-        if (l > lo) __syncthreads();
+        const int sh = 2 * (l - lo), n = 1 << sh, base = (int)blockIdx.x << sh, first = lvl_idx(l) + base;
+        for (int t = threadIdx.x; t < 3 * n; t += blockDim.x)
+        {
+            const int fld = t >> sh, j = t & (n - 1);
+            if (!(hr.flags[first + j] & F_SIG)) continue;
+            s_nd[fld][j] = encode_field<T, MW, FULL>(hr, sc, l, base + j, fld);
+        }
+        __syncthreads();
+        for (int j = threadIdx.x; j < n; j += blockDim.x)
+        {
+            const uint8_t f = hr.flags[first + j];
+            const bool was_sig = (f & F_SIG) != 0;
+            if (was_sig) ++done;
+            if (!FULL) continue;
+            uint8_t nf = f & F_PRE;
+            if (was_sig)
+            {
+                nf |= F_ENC;
+                T nd = T(0.0);
+                nd = fmax(nd, s_nd[0][j]);
+                nd = fmax(nd, s_nd[1][j]);
+                nd = fmax(nd, s_nd[2][j]);
+                if (nd >= encode_eps(eps, L, l) || (f & F_PRE)) nf |= F_SIG;
+                if (l <= L - 2 && nd >= extra_eps(eps, L, l, sc)) nf |= F_XS;
+                if (!(nf & F_SIG) && l <= L - 2)
+                {
+                    const uint32_t ch = *reinterpret_cast<const uint32_t*>(hr.flags + lvl_idx(l + 1) + 4 * (base + j));
+                    if (ch & 0x01010101u) nf |= F_SIG;
+                }
+            }
+            if (nf != f) hr.flags[first + j] = nf;
+        }
+        __syncthreads();
     }
     const unsigned tot = __reduce_add_sync(0xffffffffu, done);
     if ((threadIdx.x & 31) == 0 && tot) atomicAdd(FULL ? &sc->enc : &sc->enc2, (unsigned long long)tot);
@@ -489,16 +570,99 @@ __device__ __forceinline__ int path_leaf_level_warp(const uint8_t* flags, int Tl
     return m ? __ffs(m) - 1 : Tl + 1;
 }
 
-// Decode levels lo .. lo + depth - 1 top-down (mra/decoding.cu, mra/extra_significance.cu).
+// One field of one significant parent's decode: its four children (stored) from its scale
+// coefficients and details (recomputed from the children for an encoded parent, zero
+// otherwise); returns the normalised maximum |detail| of that field (0 when not encoded).
+// The same helper calls in the same order as one field of decode_parent.
+template <typename T, bool MW>
+__device__ __forceinline__ T decode_field(const Hier<T>& hr, const Scalars<T>* sc, int level, int idx, int fld, bool enc)
+{
+    const int p = lvl_idx(level) + idx;
+    const int c = lvl_idx(level + 1) + 4 * idx;
+    // the field's arrays, chosen without indexing the parameter block by a runtime value
+    T* const a0 = fld == 0 ? hr.s[0][0] : fld == 1 ? hr.s[1][0] : hr.s[2][0];
+    T* const a1 = fld == 0 ? hr.s[0][1] : fld == 1 ? hr.s[1][1] : hr.s[2][1];
+    T* const a2 = fld == 0 ? hr.s[0][2] : fld == 1 ? hr.s[1][2] : hr.s[2][2];
+    T nd = T(0.0);
+    if (MW)
+    {
+        const T s[3] = {a0[p], a1[p], a2[p]};
+        T d[3][3];
+        if (enc)
+        {
+            const T mx = fld == 0 ? fmax(T(1.0), sc->max_eta) : fmax(T(1.0), sc->max_qx);
+            T k[3][4];
+            load4(a0 + c, k[0]); load4(a1 + c, k[1]); load4(a2 + c, k[2]);
+            mw_encode_details(k, d);
+            nd = mw_detail_max(d) / mx;
+        }
+        else
+        {
+#pragma unroll
+            for (int t = 0; t < 3; ++t)
+#pragma unroll
+                for (int m = 0; m < 3; ++m) d[t][m] = T(0.0);
+        }
+        T k[3][4];
+        mw_decode(s, d, k);
+        store4(a0 + c, k[0]); store4(a1 + c, k[1]); store4(a2 + c, k[2]);
+    }
+    else
+    {
+        const T u = a0[p];
+        T a = T(0.0), b = T(0.0), g = T(0.0);
+        if (enc)
+        {
+            const T mx = fld == 0 ? fmax(T(1.0), sc->max_eta) : fmax(T(1.0), sc->max_qx);
+            T k[4];
+            load4(a0 + c, k);
+            a = hw_alpha(k); b = hw_beta(k); g = hw_gamma(k);
+            T m1 = fmax(fabs(a), fabs(b));
+            m1 = fmax(fabs(g), m1);
+            nd = m1 / mx;
+        }
+        T k[4];
+        hw_decode(u, a, b, g, k);
+        store4(a0 + c, k);
+    }
+    return nd;
+}
+
+// Decode levels lo .. lo + depth - 1 top-down (mra/decoding.cu, mra/extra_significance.cu),
+// one thread per parent and field (see k_encode_band); the fields' detail norms are combined
+// in field order, as decode_parent combines them, for extra significance.
 template <typename T, bool MW>
 __global__ void __launch_bounds__(256) k_decode_band(Hier<T> hr, Scalars<T>* sc, int L, int lo, int depth, T eps)
 {
+    static_assert(kBandDepth <= 5, "a band level has at most 4^(kBandDepth - 1) <= 256 parents");
+    __shared__ T s_nd[3][256];
     unsigned done = 0;
     for (int l = lo; l < lo + depth; ++l)
     {
-        const int n = 1 << (2 * (l - lo)), base = (int)blockIdx.x << (2 * (l - lo));
-        for (int k = threadIdx.x; k < n; k += blockDim.x) decode_parent<T, MW>(hr, sc, L, l, base + k, eps, done);
-        if (l + 1 < lo + depth) __syncthreads();
+        const int sh = 2 * (l - lo), n = 1 << sh, base = (int)blockIdx.x << sh, first = lvl_idx(l) + base;
+        for (int t = threadIdx.x; t < 3 * n; t += blockDim.x)
+        {
+            const int fld = t >> sh, j = t & (n - 1);
+            const uint8_t f = hr.flags[first + j];
+            if (!(f & F_SIG)) continue;
+            s_nd[fld][j] = decode_field<T, MW>(hr, sc, l, base + j, fld, (f & F_ENC) != 0);
+        }
+        __syncthreads();
+        for (int j = threadIdx.x; j < n; j += blockDim.x)
+        {
+            if (!(hr.flags[first + j] & F_SIG)) continue;
+            ++done;
+            if (l <= L - 2)
+            {
+                T nd = T(0.0);
+                nd = fmax(nd, s_nd[0][j]);
+                nd = fmax(nd, s_nd[1][j]);
+                nd = fmax(nd, s_nd[2][j]);
+                if (nd >= extra_eps(eps, L, l, sc))
+                    *reinterpret_cast<uint32_t*>(hr.flags + lvl_idx(l + 1) + 4 * (base + j)) |= 0x01010101u;
+            }
+        }
+        __syncthreads();
     }
     const unsigned tot = __reduce_add_sync(0xffffffffu, done);
     if ((threadIdx.x & 31) == 0 && tot) atomicAdd(&sc->dec, (unsigned long long)tot);
