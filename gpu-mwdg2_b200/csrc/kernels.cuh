@@ -377,14 +377,33 @@ __device__ __forceinline__ void encode_parent(const Hier<T>& hr, const Scalars<T
 constexpr int kBandDepth = 5;
 constexpr int kBandMaxLevel = 9;
 
-// One level of parents (levels above kBandMaxLevel).
-template <typename T, bool MW, bool FULL>
+// One level of parents (levels above kBandMaxLevel). FOLD: the level below it (level + 1)
+// is sparse, and each thread first encodes its own parent's children there that need it
+// (significant ones; FULL also clears the stale flag bits of the others, as k_level_sparse
+// does) before the parent itself: a child's data is touched by its parent's thread only,
+// and the sparse level needs no launch (and no scan of its flags) of its own.
+template <typename T, bool MW, bool FULL, bool FOLD = false>
 __global__ void __launch_bounds__(256) k_encode_level(Hier<T> hr, Scalars<T>* sc, int L, int level, T eps)
 {
-    if (!FULL && sc->min_leaf > level) return;   // see scale_only_needed
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool in = idx < (1 << (2 * level));
     unsigned done = 0;
-    if (idx < (1 << (2 * level))) encode_parent<T, MW, FULL>(hr, sc, L, level, idx, eps, done);
+    if (FOLD && in && (FULL || sc->min_leaf <= level + 1))   // see scale_only_needed
+    {
+        const int cb = 4 * idx, first = lvl_idx(level + 1);
+        const uint32_t cw = *reinterpret_cast<const uint32_t*>(hr.flags + first + cb);
+        if (cw)
+        {
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+            {
+                const uint32_t f = (cw >> (8 * j)) & 0xffu;
+                if (f & F_SIG) encode_parent<T, MW, FULL>(hr, sc, L, level + 1, cb + j, eps, done);
+                else if (FULL && (f & ~(uint32_t)F_PRE)) hr.flags[first + cb + j] = (uint8_t)(f & F_PRE);
+            }
+        }
+    }
+    if (in && (FULL || sc->min_leaf <= level)) encode_parent<T, MW, FULL>(hr, sc, L, level, idx, eps, done);
     const unsigned tot = __reduce_add_sync(0xffffffffu, done);
     if ((threadIdx.x & 31) == 0 && tot) atomicAdd(FULL ? &sc->enc : &sc->enc2, (unsigned long long)tot);
 }

@@ -240,10 +240,18 @@ private:
     }
     // Bottom-up walk of the tree: one launch per level above kBandMaxLevel, then the bands.
     // FULL: encode + threshold + regularise; else scale-only re-encode.
+    // a sparse level right below a dense one (both above the bands) is walked inside the
+    // dense level's kernel (FOLD): each parent's thread takes its own children there
+    bool folded_below(int level) const
+    {
+        return level - 1 > mw::kBandMaxLevel && level <= L_ - 1 && sparse_level(level) && !sparse_level(level - 1);
+    }
     template <bool FULL> void encode_tree(const mw::Hier<T>& h, T eps)
     {
         for (int level = L_ - 1; level > mw::kBandMaxLevel; --level)
         {
+            if (folded_below(level)) continue;
+            const bool fold = folded_below(level + 1);
             if (sparse_level(level))
             {
                 const int nb = grid_for(((int64_t)1 << (2 * level)) / 8, 256, 1 << 30);
@@ -253,7 +261,9 @@ private:
             else
             {
                 const int nb = grid_for((int64_t)1 << (2 * level), 256, 1 << 30);
-                if (mw_) mw::k_encode_level<T, true, FULL><<<nb, 256, 0, st_>>>(h, sc_, L_, level, eps);
+                if (mw_ && fold) mw::k_encode_level<T, true, FULL, true><<<nb, 256, 0, st_>>>(h, sc_, L_, level, eps);
+                else if (mw_) mw::k_encode_level<T, true, FULL><<<nb, 256, 0, st_>>>(h, sc_, L_, level, eps);
+                else if (fold) mw::k_encode_level<T, false, FULL, true><<<nb, 256, 0, st_>>>(h, sc_, L_, level, eps);
                 else mw::k_encode_level<T, false, FULL><<<nb, 256, 0, st_>>>(h, sc_, L_, level, eps);
             }
             ++launches_;
@@ -628,6 +638,8 @@ template <typename T> mwdg2_status Sim<T>::enqueue_device()
         {
             CU(cudaEventRecord(ev_dec_fork_, st_));
             CU(cudaStreamWaitEvent(st_dec_, ev_dec_fork_, 0));
+            // (no folding here: a thread decoding a child after its parent lengthens the
+            // kernel's tail, while the sparse level's own kernel overlaps the topology)
             for (int level = mw::kBandMaxLevel + 1; level < L_; ++level)
             {
                 if (sparse_level(level))
