@@ -695,7 +695,7 @@ template <typename T> mwdg2_status Sim<T>::enqueue_device()
     const int np = (int)cs_.stage_codes.size();
     if (np > 0)
     {
-        mw::k_sample_points<T><<<(np + 127) / 128, 128, 0, st_>>>(lf_, hr_, sc_, L_, d_stage_codes_, np, tile_counts_,
+        mw::k_sample_points<T><<<(32 * np + 127) / 128, 128, 0, st_>>>(lf_, hr_, sc_, L_, d_stage_codes_, np, tile_counts_,
                                                                   ntiles_, d_stage_out_);
         ++launches_;
     }
@@ -801,7 +801,7 @@ template <typename T> mwdg2_status Sim<T>::sample_stage(std::vector<T>& vals)
         return MWDG2_OK;
     }
     // before the first step: the leaf list is every finest cell and no tile offsets exist
-    mw::k_sample_points<T><<<(np + 127) / 128, 128, 0, st_>>>(lf_, hr_, sc_, L_, d_stage_codes_, np, nullptr, 0,
+    mw::k_sample_points<T><<<(32 * np + 127) / 128, 128, 0, st_>>>(lf_, hr_, sc_, L_, d_stage_codes_, np, nullptr, 0,
                                                               d_stage_out_);
     CU(cudaGetLastError());
     CU(cudaMemcpyAsync(vals.data(), d_stage_out_, sizeof(T) * 4 * np, cudaMemcpyDeviceToHost, st_));

@@ -803,18 +803,21 @@ __global__ void __launch_bounds__(kSolverThreads) k_hwfv1(Leaves<T> lf, Hier<T> 
     if (__syncthreads_or(nan_seen) && threadIdx.x == 0) atomicOr(&sc->status, 1);
 }
 
-// Leaf containing each finest cell code (binary search over the leaves' Z-order starts)
-// and its depth eta0 - z0, discharges and bed (output/project_assem_sol.cu:3-77).
-template <typename T>
+// Leaf containing each finest cell code (search over the leaves' Z-order starts) and its
+// depth eta0 - z0, discharges and bed (output/project_assem_sol.cu:3-77). One warp per
+// point: lane j probes position lo + (j + 1) * step of the range [lo, hi] that holds the
+// answer (the last leaf whose start is <= c; starts increase along the leaf list), and the
+// ballot of the probes narrows the range 32-fold per round (two rounds for a tile's leaves).
 // tile_offsets (the scanned leaf counts of the 4^5-cell tiles, ntiles of them; null before
-// the first step) narrow the search: leaves are in Z order, so the leaf holding finest cell
+// the first step) narrow the start: leaves are in Z order, so the leaf holding finest cell
 // c is among the leaves of tile c >> 10, or is the last leaf before them when a coarser leaf
 // covers the whole tile.
+template <typename T>
 __global__ void k_sample_points(Leaves<T> lf, Hier<T> hr, Scalars<T>* sc, int L, const int32_t* codes, int np,
                                 const int32_t* tile_offsets, int ntiles, T* out)
 {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= np) return;
+    const int k = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (k >= np) return;   // the whole warp
     const int n = sc->n_leaves;
     const int c = codes[k];
     int lo = 0, hi = n - 1;
@@ -827,11 +830,17 @@ __global__ void k_sample_points(Leaves<T> lf, Hier<T> hr, Scalars<T>* sc, int L,
     }
     while (lo < hi)
     {
-        const int mid = (lo + hi + 1) >> 1;
-        const int l = lf.lvl[mid];
-        const int start = (lf.act[mid] - lvl_idx(l)) << (2 * (L - l));
-        if (start <= c) lo = mid; else hi = mid - 1;
+        const int step = (hi - lo + 31) / 32;
+        const int pos = min(hi, lo + (lane + 1) * step);
+        const int l = lf.lvl[pos];
+        const bool le = ((lf.act[pos] - lvl_idx(l)) << (2 * (L - l))) <= c;
+        const int t = __popc(__ballot_sync(0xffffffffu, le));   // probes 0..t-1 start at or before c
+        const int nlo = t == 0 ? lo : min(hi, lo + t * step);
+        const int nhi = t == 32 ? hi : min(hi, lo + (t + 1) * step) - 1;
+        lo = nlo;
+        hi = nhi;
     }
+    if (lane != 0) return;
     const int a = lf.act[lo];
     const T z0 = hr.s[3][0][a];
     const T eta = lf.un[0][lo] + z0;
