@@ -148,7 +148,7 @@ class Clocks:
 # (4096^2, FP32, 3.0 M leaves). Keyed by (solver, P, timing phase).
 TRAFFIC_SOURCE = "ncu launch list (dram bytes, 1 pass) of the same workload, per leaf x leaves"
 PHASE_STEPS = 5
-TRAFFIC_B_PER_LEAF: dict = {("mwdg2", 4, 3): 6.0, ("mwdg2", 4, 4): 224.4, ("mwdg2", 4, 6): 183.9}
+TRAFFIC_B_PER_LEAF: dict = {("mwdg2", 4, 3): 6.0, ("mwdg2", 4, 4): 208.8, ("mwdg2", 4, 6): 169.0}
 
 
 def peaks() -> tuple[float, str]:
