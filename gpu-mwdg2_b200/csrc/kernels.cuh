@@ -388,22 +388,32 @@ __global__ void __launch_bounds__(256) k_encode_level(Hier<T> hr, Scalars<T>* sc
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
     const bool in = idx < (1 << (2 * level));
     unsigned done = 0;
-    if (FOLD && in && (FULL || sc->min_leaf <= level + 1))   // see scale_only_needed
+    // FOLD: up to four children (level + 1) first, then the parent, through one call site of
+    // encode_parent (one inlined copy keeps the plain kernel's register count and occupancy)
+    const bool fold = FOLD && in && (FULL || sc->min_leaf <= level + 1);   // see scale_only_needed
+    const int cb = 4 * idx, cfirst = lvl_idx(level + 1);
+    const uint32_t cw = fold ? *reinterpret_cast<const uint32_t*>(hr.flags + cfirst + cb) : 0u;
+#pragma unroll 1
+    for (int j = (FOLD && cw) ? 0 : 4; j < 5; ++j)
     {
-        const int cb = 4 * idx, first = lvl_idx(level + 1);
-        const uint32_t cw = *reinterpret_cast<const uint32_t*>(hr.flags + first + cb);
-        if (cw)
+        bool go;
+        int lv, id;
+        if (j < 4)
         {
-#pragma unroll
-            for (int j = 0; j < 4; ++j)
-            {
-                const uint32_t f = (cw >> (8 * j)) & 0xffu;
-                if (f & F_SIG) encode_parent<T, MW, FULL>(hr, sc, L, level + 1, cb + j, eps, done);
-                else if (FULL && (f & ~(uint32_t)F_PRE)) hr.flags[first + cb + j] = (uint8_t)(f & F_PRE);
-            }
+            const uint32_t f = (cw >> (8 * j)) & 0xffu;
+            go = (f & F_SIG) != 0;
+            if (FULL && !go && (f & ~(uint32_t)F_PRE)) hr.flags[cfirst + cb + j] = (uint8_t)(f & F_PRE);
+            lv = level + 1;
+            id = cb + j;
         }
+        else
+        {
+            go = in && (FULL || sc->min_leaf <= level);
+            lv = level;
+            id = idx;
+        }
+        if (go) encode_parent<T, MW, FULL>(hr, sc, L, lv, id, eps, done);
     }
-    if (in && (FULL || sc->min_leaf <= level)) encode_parent<T, MW, FULL>(hr, sc, L, level, idx, eps, done);
     const unsigned tot = __reduce_add_sync(0xffffffffu, done);
     if ((threadIdx.x & 31) == 0 && tot) atomicAdd(FULL ? &sc->enc : &sc->enc2, (unsigned long long)tot);
 }
