@@ -383,7 +383,7 @@ constexpr int kBandMaxLevel = 9;
 // does) before the parent itself: a child's data is touched by its parent's thread only,
 // and the sparse level needs no launch (and no scan of its flags) of its own.
 template <typename T, bool MW, bool FULL, bool FOLD = false>
-__global__ void __launch_bounds__(256) k_encode_level(Hier<T> hr, Scalars<T>* sc, int L, int level, T eps)
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 6 : 4) k_encode_level(Hier<T> hr, Scalars<T>* sc, int L, int level, T eps)
 {
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
     const bool in = idx < (1 << (2 * level));
@@ -723,7 +723,7 @@ __global__ void __launch_bounds__(256) k_extra_sig_level(uint8_t* flags, const S
 // One level of parents (levels above kBandMaxLevel), values only (k_extra_sig_level set the
 // children's flags).
 template <typename T, bool MW>
-__global__ void __launch_bounds__(256) k_decode_level(Hier<T> hr, Scalars<T>* sc, int L, int level, T eps)
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4) k_decode_level(Hier<T> hr, Scalars<T>* sc, int L, int level, T eps)
 {
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned done = 0;

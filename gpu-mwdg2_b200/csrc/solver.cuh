@@ -362,7 +362,7 @@ template <typename T> struct StateMax
 // leaves). Stage 1 also keeps a dry leaf's depth after ghost cells in U^n (un[0]); stage 2
 // reports initial_tstep as the CFL step of dry leaves (dg2_update.cu:61).
 template <typename T, int STAGE>
-__global__ void __launch_bounds__(256) k_stage_wet(Leaves<T> lf, Hier<T> hin, Scalars<T>* sc, Params<T> P,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4) k_stage_wet(Leaves<T> lf, Hier<T> hin, Scalars<T>* sc, Params<T> P,
                                                    const StepArgs<T>* args, uint8_t* dry, int32_t* wet)
 {
     const T dt = args->dt;
