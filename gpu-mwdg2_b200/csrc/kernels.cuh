@@ -661,7 +661,7 @@ __device__ __forceinline__ T decode_field(const Hier<T>& hr, const Scalars<T>* s
 // one thread per parent and field (see k_encode_band); the fields' detail norms are combined
 // in field order, as decode_parent combines them, for extra significance.
 template <typename T, bool MW>
-__global__ void __launch_bounds__(256) k_decode_band(Hier<T> hr, Scalars<T>* sc, int L, int lo, int depth, T eps)
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4) k_decode_band(Hier<T> hr, Scalars<T>* sc, int L, int lo, int depth, T eps)
 {
     static_assert(kBandDepth <= 5, "a band level has at most 4^(kBandDepth - 1) <= 256 parents");
     __shared__ T s_nd[3][256];
