@@ -243,7 +243,9 @@ bool Case<T>::read(const std::string& par, double eps_override, int solver_overr
     bool has_cfl = false;
     const T cfl = kf.real<T>("CFL", &has_cfl);  // extension: the reference's CFL is fixed
     if (has_cfl && cfl > T(0)) CFL = cfl;
-    if (L < 6 || L > 15) return fail(2, "max_ref_lvl must be between 6 and 15");
+    // 14 at most: the hierarchy's slot count (4^(L+1) - 1) / 3 + 3 is formed in 32-bit ints,
+    // and a level-15 mesh would not fit in one GPU's memory anyway
+    if (L < 6 || L > 14) return fail(2, "max_ref_lvl must be between 6 and 14");
     // classes/SimulationParams.cpp:15-33
     const std::string dem = kf.str("DEMfile");
     if (dem.empty()) return fail(2, "no DEMfile in " + par);

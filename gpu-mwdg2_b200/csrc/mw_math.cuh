@@ -28,6 +28,7 @@ enum : uint8_t {
 
 // ---------------------------------------------------------------- indexing
 // utilities/get_lvl_idx.cuh:11-24 -- first slot of level n (3 padding slots)
+// (level <= 15: the library allows max_ref_lvl <= 14 and indexes levels up to L + 1)
 MW_HD int lvl_idx(int level) { return ((1 << (2 * level)) - 1) / 3 + 3; }
 
 // Level of a hierarchy index h >= 3 (inverse of lvl_idx): 3 (h - 3) + 1 lies in

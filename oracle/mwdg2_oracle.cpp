@@ -160,7 +160,7 @@ bool Sim<T>::read_params(double eps_override, int solver_override)
     bool has_cfl = false;
     T cfl = read_kw_real<T>(p, "CFL", &has_cfl);
     if (has_cfl && cfl > T(0)) CFL = cfl;
-    if (L < 6 || L > 15) { error = "max_ref_lvl must be in [6, 15]"; return false; }
+    if (L < 6 || L > 14) { error = "max_ref_lvl must be in [6, 14]"; return false; }
     // classes/SimulationParams.cpp:15-33
     std::string dem = read_kw_str(p, "DEMfile");
     if (dem.empty()) { error = "no DEMfile"; return false; }

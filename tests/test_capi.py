@@ -47,6 +47,17 @@ def test_unsupported_solver_keyword_is_parse_error(tmp_path):
     assert e.value.status == 2
 
 
+@pytest.mark.parametrize("level", [5, 15])
+def test_max_ref_lvl_outside_6_to_14_is_parse_error(tmp_path, level):
+    """Level 15 would overflow the 32-bit slot count of level L + 1 (and not fit in memory)."""
+    p = tmp_path / "x.par"
+    p.write_text(f"mwdg2\ncuda\nmax_ref_lvl {level}\nepsilon 1e-3\nDEMfile a.dem\n")
+    with pytest.raises(mwdg2_b200.MWDG2Error) as e:
+        mwdg2_b200.Simulation(str(p))
+    assert e.value.status == 2
+    assert "max_ref_lvl" in str(e.value)
+
+
 def test_null_handle_calls_are_rejected():
     lib = mwdg2_b200.lib()
     assert lib.mwdg2_step(None, None, None) == 6
