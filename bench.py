@@ -43,18 +43,30 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", type=int, default=32, choices=[32, 64])
     ap.add_argument("--solver", default="mwdg2", choices=["mwdg2", "hwfv1"])
-    ap.add_argument("--level", type=int, default=12)
+    ap.add_argument("--level", type=int, default=None, help="max_ref_lvl (catchment 12, urban 13)")
     ap.add_argument("--cpu-steps", type=int, default=2, help="timed oracle steps for cpu_baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--case-dir", default=None)
-    ap.add_argument("--workload", default="catchment", choices=["catchment", "ensemble"],
-                    help="ensemble: a batch of seeded uneven scenarios (mwdg2_batch_*) against the same "
-                         "members stepped one after another; prints its own line")
+    ap.add_argument("--workload", default="catchment", choices=["catchment", "urban", "ensemble"],
+                    help="urban: 8192^2 fBm base with building blocks, lake at rest at 1 m, rising point "
+                         "inflow; ensemble: a batch of seeded uneven scenarios (mwdg2_batch_*) against the "
+                         "same members stepped one after another; prints its own line")
     ap.add_argument("--members", type=int, default=64)
-    return ap.parse_args()
+    a = ap.parse_args()
+    if a.level is None:
+        a.level = 13 if a.workload == "urban" else 12
+    return a
 
 
 def workload(a) -> dict:
+    if a.workload == "urban":
+        return {"workload": f"urban catchment {1 << a.level}^2 finest cells (max_ref_lvl {a.level}), 1 m cells, "
+                            "fBm base Hurst 0.8 relief 0-3 m plus axis-aligned blocks 8-30 cells wide and "
+                            "5-20 m tall on ~30 % of the area, lake at rest at 1 m, Manning 0.03, west point "
+                            "inflow rising 0-100 m3/s over 15 min, epsilon 1e-3",
+                "solver": a.solver, "precision": f"fp{a.precision}", "max_ref_lvl": a.level,
+                "steps_from": "simulation start (steps W+1..W+K of the run)",
+                "l2": "inputs larger than L2 (hierarchy arrays >= 4 GB)"}
     return {"workload": f"fBm catchment {1 << a.level}^2 finest cells (max_ref_lvl {a.level}), 2 m cells, "
                         "Hurst 0.8, relief 0-30 m, Manning 0.03, dry start, west point inflow 50 m3/s peak at 30 min, "
                         "epsilon 1e-3",
@@ -65,15 +77,19 @@ def workload(a) -> dict:
 
 def make_case(a, rank: int) -> str:
     import cases
-    key = hashlib.sha1(f"{a.level}-{a.solver}-v1".encode()).hexdigest()[:10]
+    key = hashlib.sha1(f"{a.workload}-{a.level}-{a.solver}-v1".encode()).hexdigest()[:10]
     base = a.case_dir or os.path.join(tempfile.gettempdir(), "mwdg2_bench_cases")
     d = os.path.join(base, f"{key}-r{rank}")
     par = os.path.join(d, "case.par")
     if os.path.exists(os.path.join(d, "READY")):
         return par
     os.makedirs(d, exist_ok=True)
-    cases.fbm_catchment(d, L=a.level, solver=a.solver, eps=1e-3, sim_time=7200.0, cellsize=2.0, hurst=0.8,
-                        relief=30.0, manning=0.03, peak_q=50.0, t_peak=1800.0, seed=20261203)
+    if a.workload == "urban":
+        cases.urban_catchment(d, L=a.level, solver=a.solver, eps=1e-3, sim_time=3600.0, cellsize=1.0,
+                              lake_level=1.0, peak_q=100.0, t_rise=900.0, manning=0.03, seed=20261203)
+    else:
+        cases.fbm_catchment(d, L=a.level, solver=a.solver, eps=1e-3, sim_time=7200.0, cellsize=2.0, hurst=0.8,
+                            relief=30.0, manning=0.03, peak_q=50.0, t_peak=1800.0, seed=20261203)
     open(os.path.join(d, "READY"), "w").write("ok\n")
     return par
 
@@ -378,7 +394,7 @@ def main():
                 "k_hwfv1 (gather, friction, FV1 update, CFL)": (4, 7 * P + 16)}
     kname, (kph, per_leaf) = max(cand.items(), key=lambda kv: mean_ph[kv[1][0]])
     kms = float(mean_ph[kph])
-    traffic = TRAFFIC_B_PER_LEAF.get((a.solver, P, kph))
+    traffic = TRAFFIC_B_PER_LEAF.get((a.solver, P, kph)) if (a.workload, a.level) == ("catchment", 12) else None
     achieved = per_leaf * n_mean_ph / (kms / 1e3) / 1e9
     # Algorithmic bytes per step of the reference-layout model, from each step's device
     # counters: E parents encoded, E2 re-encoded (scale only), D decoded, T detail slots,

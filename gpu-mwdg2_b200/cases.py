@@ -15,6 +15,8 @@ implementation sees byte-identical inputs. Generators:
 * lake_at_rest        - still water over an fBm bed (well-balancing checks).
 * ensemble            - seeded mix of fBm catchments with dam breaks or point inflows
                         of uneven sizes (batched-ensemble benchmark).
+* urban_catchment     - fBm base with axis-aligned building blocks, a lake at rest and a
+                        rising west-edge point inflow (8192^2 urban benchmark case).
 
 Reference quirks the generators respect (they would otherwise change the physics):
 * `wall_height` is set above every bed value, because `operators/dg2_update.cu:46`
@@ -319,3 +321,84 @@ def ensemble(root: str, n: int = 64, seed: int = 20261203, levels: tuple[int, ..
         out.append(case)
     return out
 
+
+
+def urban_surface(n: int, seed: int, hurst: float = 0.8, relief: float = 3.0, cover: float = 0.3,
+                  block_height: tuple[float, float] = (5.0, 20.0), tile: int = 32,
+                  block_side: tuple[int, int] = (8, 30)) -> np.ndarray:
+    """fBm base (`relief` m) plus axis-aligned building blocks covering ~`cover` of the area.
+
+    The domain is cut into `tile` x `tile` cell lots; a lot holds one block with the
+    probability that makes the expected built fraction `cover`. A block's sides are drawn
+    uniformly from `block_side` cells, its position uniformly inside the lot and its height
+    uniformly from `block_height` m above the base (PCG64 stream `seed` + 1).
+    """
+    z = fbm_surface(n, hurst, seed, relief)
+    t = min(tile, n)
+    lo, hi = block_side
+    hi = min(hi, t)
+    lo = min(lo, hi)
+    nt = n // t
+    rng = np.random.Generator(np.random.PCG64(seed + 1))
+    w = rng.integers(lo, hi + 1, size=(nt, nt))
+    d = rng.integers(lo, hi + 1, size=(nt, nt))
+    x0 = (rng.random((nt, nt)) * (t - w + 1)).astype(np.int64)
+    y0 = (rng.random((nt, nt)) * (t - d + 1)).astype(np.int64)
+    mean_side = 0.5 * (lo + hi)
+    p = min(1.0, cover * t * t / (mean_side * mean_side))
+    on = rng.random((nt, nt)) < p
+    height = rng.uniform(block_height[0], block_height[1], size=(nt, nt))
+    li = np.arange(t)
+    in_x = (li >= x0[..., None]) & (li < (x0 + w)[..., None])        # (lot row, lot col, cell col)
+    in_y = (li >= y0[..., None]) & (li < (y0 + d)[..., None])        # (lot row, lot col, cell row)
+    mask = in_y[:, :, :, None] & in_x[:, :, None, :] & on[:, :, None, None]
+    add = np.where(mask, height[:, :, None, None], 0.0)              # (lot row, lot col, row, col)
+    z[: nt * t, : nt * t] += add.transpose(0, 2, 1, 3).reshape(nt * t, nt * t)
+    return z
+
+
+def urban_catchment(directory: str, L: int = 13, solver: str = "mwdg2", eps: float = 1e-3,
+                    sim_time: float = 3600.0, cellsize: float = 1.0, lake_level: float | None = 1.0,
+                    peak_q: float = 100.0, t_rise: float = 900.0, manning: float = 0.03,
+                    seed: int = 20261203, relief: float = 3.0, cover: float = 0.3,
+                    limitslopes: bool = False, tol_krivo: float = 10.0, massint: float | None = None,
+                    cfl: float | None = None) -> Case:
+    """Urban catchment: `urban_surface` DEM, a lake at rest at `lake_level` (h =
+    max(0, level - z) on the DEM as written, so h + z equals the level wherever water
+    stands), and a west-edge point inflow rising linearly from 0 to `peak_q` m^3/s over
+    `t_rise` seconds and held (unit-width value peak_q/cellsize). `lake_level` None is a
+    dry start; `peak_q` 0 leaves the lake at rest.
+    """
+    os.makedirs(directory, exist_ok=True)
+    n = 1 << L
+    dem = np.round(urban_surface(n, seed, relief=relief, cover=cover), 3)
+    write_esri_ascii(os.path.join(directory, "case.dem"), dem[::-1], cellsize, decimals=3)
+    extra = ["DEMfile       case.dem", "bcifile       case.bci", "bdyfile       case.bdy"]
+    start = None
+    if lake_level is not None:
+        start = np.maximum(0.0, np.round(lake_level - dem, 6))
+        write_esri_ascii(os.path.join(directory, "case.start"), start[::-1], cellsize, decimals=6)
+        extra.append("startfile     case.start")
+    y_src = (n // 2) * cellsize + cellsize / 2
+    with open(os.path.join(directory, "case.bci"), "w") as fp:
+        fp.write(f"P {cellsize / 2!r} {y_src!r} QVAR HYD\n")
+    t_end = 2.0 * max(sim_time, t_rise) + 2.0 * t_rise
+    rows = [(0.0, 0.0), (peak_q / cellsize, t_rise), (peak_q / cellsize, t_end),
+            (peak_q / cellsize, t_end + t_rise)]
+    with open(os.path.join(directory, "case.bdy"), "w") as fp:
+        fp.write("rising inflow\nHYD\n")
+        fp.write(f"{len(rows)} seconds\n")
+        for v, t in rows:
+            fp.write(f"{v!r} {t!r}\n")
+    ext = n * cellsize
+    _write_stage(os.path.join(directory, "case.stage"),
+                 [(ext * 0.25 + cellsize / 2, ext * 0.5 + cellsize / 2),
+                  (ext * 0.5 + cellsize / 2, ext * 0.5 + cellsize / 2)])
+    extra.append("stagefile     case.stage")
+    lines = _common_par(solver, L, eps, sim_time, 1000.0, manning, limitslopes, tol_krivo,
+                        massint, None, cfl, extra)
+    par = os.path.join(directory, "case.par")
+    _write_par(par, lines)
+    return Case(par=par, directory=directory, L=L, solver=solver, cellsize=cellsize,
+                sim_time=sim_time, dem=dem, start_h=start,
+                meta={"kind": "urban_catchment", "seed": seed, "cover": cover})
