@@ -136,6 +136,16 @@ __device__ __forceinline__ void ghost_pass(T& own_h0, T own_qx0, T own_qy0, T ow
 
 // operators/friction_implicit.cu:155-264 -- implicit friction on the mode-0 value and,
 // for MWDG2, on the four Gauss-point values, whose differences rebuild the slopes.
+// One out-of-line copy of the implicit Manning update of a point value (apply_friction);
+// a stage kernel applies it at 25 points per leaf (5 points of the leaf and of each of its
+// four neighbours) and would otherwise hold 25 inlined copies of its pow and divisions.
+template <typename T> struct Q2 { T qx, qy; };
+template <typename T> __device__ __noinline__ Q2<T> friction_point(T h, T qx, T qy, T tol_h, T tol_s, T n, T g, T dt)
+{
+    apply_friction(h, tol_h, tol_s, qx, qy, n, g, dt);
+    return {qx, qy};
+}
+
 template <typename T, bool MW> __device__ __forceinline__ void friction_cell(Cell<T>& c, const Params<T>& P, T dt)
 {
     if (!MW)
@@ -149,11 +159,16 @@ template <typename T, bool MW> __device__ __forceinline__ void friction_cell(Cel
     T qxly = c.qx[0] - c.qx[2], qxuy = c.qx[0] + c.qx[2];
     T qylx = c.qy[0] - c.qy[1], qyux = c.qy[0] + c.qy[1];
     T qyly = c.qy[0] - c.qy[2], qyuy = c.qy[0] + c.qy[2];
-    apply_friction(c.h[0], P.tol_h, P.tol_s, c.qx[0], c.qy[0], P.manning, P.g, dt);
-    apply_friction(hlx, P.tol_h, P.tol_s, qxlx, qylx, P.manning, P.g, dt);
-    apply_friction(hux, P.tol_h, P.tol_s, qxux, qyux, P.manning, P.g, dt);
-    apply_friction(hly, P.tol_h, P.tol_s, qxly, qyly, P.manning, P.g, dt);
-    apply_friction(huy, P.tol_h, P.tol_s, qxuy, qyuy, P.manning, P.g, dt);
+    Q2<T> r = friction_point(c.h[0], c.qx[0], c.qy[0], P.tol_h, P.tol_s, P.manning, P.g, dt);
+    c.qx[0] = r.qx; c.qy[0] = r.qy;
+    r = friction_point(hlx, qxlx, qylx, P.tol_h, P.tol_s, P.manning, P.g, dt);
+    qxlx = r.qx; qylx = r.qy;
+    r = friction_point(hux, qxux, qyux, P.tol_h, P.tol_s, P.manning, P.g, dt);
+    qxux = r.qx; qyux = r.qy;
+    r = friction_point(hly, qxly, qyly, P.tol_h, P.tol_s, P.manning, P.g, dt);
+    qxly = r.qx; qyly = r.qy;
+    r = friction_point(huy, qxuy, qyuy, P.tol_h, P.tol_s, P.manning, P.g, dt);
+    qxuy = r.qx; qyuy = r.qy;
     c.qx[1] = T(0.5) * (qxux - qxlx);
     c.qx[2] = T(0.5) * (qxuy - qxly);
     c.qy[1] = T(0.5) * (qyux - qylx);
@@ -465,7 +480,7 @@ __global__ void __launch_bounds__(256) k_stage_dry(Leaves<T> lf, Hier<T> hin, Hi
 // mra/reinsert_assem_sol.cu), the next step's maxima, CFL dt. LIST: only the leaves in
 // the wet list built by k_stage_wet; otherwise every leaf.
 template <typename T, int STAGE, bool LIST>
-__global__ void __launch_bounds__(kSolverThreads) k_mwdg2_stage(Leaves<T> lf, Hier<T> hin, Hier<T> hout, Scalars<T>* sc,
+__global__ void __launch_bounds__(kSolverThreads, sizeof(T) == 4 ? 5 : 2) k_mwdg2_stage(Leaves<T> lf, Hier<T> hin, Hier<T> hout, Scalars<T>* sc,
                                                                 Params<T> P, const StepArgs<T>* args, bool friction,
                                                                 const int32_t* wet)
 {
