@@ -437,11 +437,23 @@ __global__ void __launch_bounds__(256) k_stage_dry(Leaves<T> lf, Hier<T> hin, Hi
                                                    bool friction, const uint8_t* dry)
 {
     const int n = sc->n_leaves;
+    const int stride = gridDim.x * blockDim.x;
     StateMax<T> mx;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    // software pipeline: the next leaf's mark and hierarchy index are loaded while this
+    // leaf's gathers at its index are in flight (one dependent round trip per leaf, not two)
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    bool dry_next = i < n && dry[i];
+    int a_next = i < n ? lf.act[i] : 0;
+    for (; i < n; i += stride)
     {
-        if (!dry[i]) continue;
-        const int a = lf.act[i];
+        const bool is_dry = dry_next;
+        const int a = a_next;
+        if (i + stride < n)
+        {
+            dry_next = dry[i + stride];
+            a_next = lf.act[i + stride];
+        }
+        if (!is_dry) continue;
         const T z[3] = {hin.s[3][0][a], hin.s[3][1][a], hin.s[3][2][a]};
         T u[9];
         if (STAGE == 1)
