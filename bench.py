@@ -164,7 +164,7 @@ class Clocks:
 # (4096^2, FP32, 3.0 M leaves). Keyed by (solver, P, timing phase).
 TRAFFIC_SOURCE = "ncu launch list (dram bytes, 1 pass) of the same workload, per leaf x leaves"
 PHASE_STEPS = 5
-TRAFFIC_B_PER_LEAF: dict = {("mwdg2", 4, 3): 6.0, ("mwdg2", 4, 4): 208.8, ("mwdg2", 4, 6): 169.0}
+TRAFFIC_B_PER_LEAF: dict = {("mwdg2", 4, 3): 6.0, ("mwdg2", 4, 4): 208.6, ("mwdg2", 4, 6): 168.7}
 
 
 def peaks() -> tuple[float, str]:
