@@ -61,7 +61,9 @@ const char* mwdg2_last_error(void);
 
 /* Read the case and set up device state (replaces the initialisation part of
  * run_simulation, source/run_simulation.cu:9-222). Relative file names in the .par are
- * opened relative to the working directory, as the reference does. */
+ * opened relative to the working directory, as the reference does. max_ref_lvl must lie in
+ * 6..14 (MWDG2_ERR_PARSE otherwise: below 6 the reference itself indexes past its arrays,
+ * above 14 the hierarchy's slot count leaves 32-bit range and one GPU's memory). */
 mwdg2_status mwdg2_create(const char* par_path, const mwdg2_opts* opts, mwdg2_sim** out);
 
 /* Advance one adaptive time step (one iteration of run_simulation.cu:226-774).
