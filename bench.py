@@ -167,6 +167,24 @@ PHASE_STEPS = 5
 TRAFFIC_B_PER_LEAF: dict = {("mwdg2", 4, 3): 6.0, ("mwdg2", 4, 4): 208.6, ("mwdg2", 4, 6): 168.7}
 
 
+def max_over_ranks(x: float, dist, device: str) -> float:
+    """The largest per-rank value of x (the slowest replica's time) on every rank; x itself
+    without a process group. Every rank must call it at the same point."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(world: int, leaves_per_rank: int, max_ms: float) -> float:
+    """Whole-job active-cell updates/s of `world` replicas of the same workload: every rank
+    updates `leaves_per_rank` leaves over the timed steps, and the job takes as long as the
+    slowest rank (`max_ms`, milliseconds)."""
+    return world * leaves_per_rank / (max_ms / 1e3)
+
+
 def peaks() -> tuple[float, str]:
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -331,12 +349,8 @@ def main():
         leaves.append(n)
         counters.append(sim.last_step_counters())
     barrier()
-    tot_ms = float(sum(ms_step))
-    if dist:
-        tt = torch.tensor([tot_ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        tot_ms = float(tt.item())
-    value = world * sum(leaves) / (tot_ms / 1e3)
+    tot_ms = max_over_ranks(float(sum(ms_step)), dist, "cuda")
+    value = replica_throughput(world, sum(leaves), tot_ms)
 
     # end to end through the C ABI: each step's inputs (point-source values) go host->device
     # from pinned memory inside mwdg2_step, its scalars come back, and the stage-point
@@ -364,10 +378,7 @@ def main():
         ms_phase.append(sim.last_step_timing().tolist())
         leaves_ph.append(n)
     barrier()
-    if dist:
-        tt = torch.tensor([e2e_wall], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_wall = float(tt.item())
+    e2e_wall = max_over_ranks(e2e_wall, dist, "cuda")
     P = a.precision // 8
     # bytes the library copied per step (its counters): host->device the step's dt, boundary
     # and point-source values; device->host its scalars and the stage-point values
