@@ -121,7 +121,11 @@ private:
     cudaStream_t st_ = nullptr;
     std::vector<void*> allocs_;
     mw::Hier<T> hr_{};
-    mw::Hier<T> hs_{};                  // MWDG2 stage hierarchy (U*), bed and flags shared with hr_
+    mw::Hier<T> hs_{};                  // MWDG2 stage hierarchy (U*), bed and flags shared with hr_;
+                                        // HWFV1: the buffer the step's FV1 result goes into
+    // HWFV1 alternates hr_ and hs_ (eta, qx, qy) every step; a captured graph holds the
+    // pointers of one parity, so the parity is part of the graph's key
+    bool flip_ = false;
     mw::Leaves<T> lf_{};
     mw::Scalars<T>* sc_ = nullptr;      // device
     mw::Scalars<T>* sc_host_ = nullptr; // pinned
@@ -161,7 +165,8 @@ private:
     }
     int variant_key() const
     {
-        int key = (mw_ && use_list(1) ? 1 : 0) | (mw_ && use_list(2) ? 2 : 0) | (timed_ ? 1 << 24 : 0);
+        int key = (mw_ && use_list(1) ? 1 : 0) | (mw_ && use_list(2) ? 2 : 0) | (timed_ ? 1 << 24 : 0) |
+                  (!mw_ && flip_ ? 1 << 23 : 0);
         for (int level = mw::kBandMaxLevel + 1; level < L_; ++level)
             if (sparse_level(level)) key |= 4 << (level - mw::kBandMaxLevel - 1);
         return key;
@@ -204,6 +209,7 @@ private:
     }
     void release();
     mwdg2_status launch_step();    // enqueue only (graph replay or direct launches)
+    mwdg2_status launch_step_device();
     mwdg2_status enqueue_device(); // the step's device work, on st_
     mwdg2_status collect_step();   // wait, timing, counters
     // One MWDG2 RK stage. When fewer than half of the leaves were wet in this stage last
@@ -365,11 +371,14 @@ template <typename T> mwdg2_status Sim<T>::init(const char* par, const mwdg2_opt
         {
             hr_.s[f][m] = hs_.s[f][m] = nullptr;
             if (m < modes) { mwdg2_status s = dalloc(hr_.s[f][m], n_all_); if (s) return s; }
-            if (mw_ && f < 3) { mwdg2_status s = dalloc(hs_.s[f][m], n_all_); if (s) return s; }
+            if ((mw_ || m == 0) && f < 3) { mwdg2_status s = dalloc(hs_.s[f][m], n_all_); if (s) return s; }
         }
     if (mwdg2_status s = dalloc(hr_.flags, n_det_)) return s;
     for (int m = 0; m < 3; ++m) hs_.s[3][m] = hr_.s[3][m];
     hs_.flags = hr_.flags;
+    // HWFV1: the second buffer starts at zero (only slots that a step writes are ever read)
+    if (!mw_)
+        for (int f = 0; f < 3; ++f) CU(cudaMemset(hs_.s[f][0], 0, sizeof(T) * (size_t)n_all_));
     // leaves (capacity: every finest cell)
     if (mwdg2_status s = dalloc(lf_.act, F_)) return s;
     if (mwdg2_status s = dalloc(lf_.lvl, F_)) return s;
@@ -520,6 +529,18 @@ template <typename T> mwdg2_status Sim<T>::init(const char* par, const mwdg2_opt
 
 template <typename T> mwdg2_status Sim<T>::launch_step()
 {
+    const mwdg2_status st = launch_step_device();
+    // HWFV1: the step wrote its result into hs_, which the next step reads as its hierarchy
+    if (st == MWDG2_OK && !mw_)
+    {
+        for (int f = 0; f < 3; ++f) std::swap(hr_.s[f][0], hs_.s[f][0]);
+        flip_ = !flip_;
+    }
+    return st;
+}
+
+template <typename T> mwdg2_status Sim<T>::launch_step_device()
+{
     // host-side values of this step: point-source values (classes/PointSources.h:453-472)
     // and boundary inlets (classes/Boundaries.h:28-39) at the current time, and dt
     for (auto& src : cs_.srcs)
@@ -581,9 +602,10 @@ template <typename T> mwdg2_status Sim<T>::enqueue_device()
     };
     launches_ = 0;
     rec(0);
-    // MWDG2 after its first step: the previous step's stage 2 re-inserted the state into
-    // the hierarchy and reduced its maxima, so only the point sources remain here
-    const bool carry = mw && !first_;
+    // after the first step: the previous step's last solver kernel (MWDG2 stage 2, or the
+    // FV1 kernel into the other buffer) re-inserted the state into the hierarchy and reduced
+    // its maxima, so only the point sources remain here
+    const bool carry = !first_;
     const int nsrc = (int)cs_.srcs.size();
     // one kernel where nothing runs between the scalar reset and the point sources (MWDG2
     // after its first step) and the pinned buffers are mapped; else copies and two kernels
@@ -599,8 +621,12 @@ template <typename T> mwdg2_status Sim<T>::enqueue_device()
         mw::k_step_begin<T><<<1, 1, 0, st_>>>(sc_, carry);
         ++launches_;
         const int nfix = first_ ? (int)F_ : -1;
-        if (mw) { if (!carry) { mw::k_maxes_reinsert<T, true><<<grid_leaf_, 256, 0, st_>>>(lf_, hr_, sc_, nfix, false); ++launches_; } }
-        else { mw::k_maxes_reinsert<T, false><<<grid_leaf_, 256, 0, st_>>>(lf_, hr_, sc_, nfix, !first_); ++launches_; }
+        if (!carry)
+        {
+            if (mw) mw::k_maxes_reinsert<T, true><<<grid_leaf_, 256, 0, st_>>>(lf_, hr_, sc_, nfix, false);
+            else mw::k_maxes_reinsert<T, false><<<grid_leaf_, 256, 0, st_>>>(lf_, hr_, sc_, nfix, false);
+            ++launches_;
+        }
         if (nsrc > 0)
         {
             CU(cudaMemcpyAsync(d_src_, h_src_, sizeof(mw::Src<T>) * nsrc, cudaMemcpyHostToDevice, st_));
@@ -675,7 +701,7 @@ template <typename T> mwdg2_status Sim<T>::enqueue_device()
     const bool fric = cs_.manning > T(0);
     if (!mw)
     {
-        mw::k_hwfv1<T><<<grid_stage_, mw::kSolverThreads, 0, st_>>>(lf_, hr_, sc_, P_, d_args_, fric);
+        mw::k_hwfv1<T><<<grid_stage_, mw::kSolverThreads, 0, st_>>>(lf_, hr_, hs_, sc_, P_, d_args_, fric);
         ++launches_;
         rec(5);
         rec(6);

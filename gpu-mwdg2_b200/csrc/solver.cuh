@@ -371,6 +371,19 @@ template <typename T> struct StateMax
     }
 };
 
+// The FV1 result of a leaf into the other of the two alternating hierarchy buffers at the
+// leaf's own index (the re-insertion of mra/reinsert_assem_sol.cu:3-32, eta = h + z), and
+// into the maxima the next step's thresholds use (mra/get_max_scale_coeffs.cu:3-27).
+template <typename T>
+__device__ __forceinline__ void put_leaf_fv1(const Hier<T>& hout, int a, T h, T qx, T qy, T z, StateMax<T>& mx)
+{
+    hout.s[0][0][a] = h + z;
+    hout.s[1][0][a] = qx;
+    hout.s[2][0][a] = qy;
+    const T u[9] = {h, T(0), T(0), qx, T(0), T(0), qy, T(0), T(0)};
+    mx.add(u, z);
+}
+
 // Wet test of one RK stage (the rule of leaf_is_dry, after ghost cells): wet leaves are
 // appended to `wet` (warp-aggregated) for k_mwdg2_stage<.., LIST=true>, dry ones marked in
 // `dry` for k_stage_dry, which then runs beside the wet-list kernel (the two touch disjoint
@@ -709,16 +722,20 @@ __global__ void __launch_bounds__(256) k_stage2_maxh(Leaves<T> lf, Hier<T> hr, S
     block_max_atomic<T, 1>(v, dst);
 }
 
-// operators/fv1_update.cu:3-243 with friction and ghost cells fused; in-place update.
+// operators/fv1_update.cu:3-243 with friction and ghost cells fused. Reads the leaf and its
+// neighbours from `hr` and writes the result into the leaf arrays and, at the leaf's own
+// index, into `hout`, the other of two alternating hierarchy buffers (no leaf reads `hout`
+// in this kernel), with the next step's maxima: the next step needs no re-insertion pass.
 template <typename T>
-__global__ void __launch_bounds__(kSolverThreads) k_hwfv1(Leaves<T> lf, Hier<T> hr, Scalars<T>* sc, Params<T> P,
-                                                          const StepArgs<T>* args, bool friction)
+__global__ void __launch_bounds__(kSolverThreads) k_hwfv1(Leaves<T> lf, Hier<T> hr, Hier<T> hout, Scalars<T>* sc,
+                                                          Params<T> P, const StepArgs<T>* args, bool friction)
 {
     const T dt = args->dt;
     const Bnd<T>& B = args->B;
     const int n = sc->n_leaves;
     T dt_loc = (sizeof(T) == 8) ? T(1.0e308) : T(3.0e38);
     bool nan_seen = false;
+    StateMax<T> mx;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     {
         const int a = lf.act[i];
@@ -751,6 +768,7 @@ __global__ void __launch_bounds__(kSolverThreads) k_hwfv1(Leaves<T> lf, Hier<T> 
             lf.un[0][i] = own.h[0];
             lf.un[3][i] = own.qx[0];
             lf.un[6][i] = own.qy[0];
+            put_leaf_fv1(hout, a, own.h[0], own.qx[0], own.qy[0], own.z[0], mx);
             if (P.dt_leaf) P.dt_leaf[i] = P.initial_tstep;
             dt_loc = fmin(dt_loc, P.initial_tstep);
             continue;
@@ -813,9 +831,11 @@ __global__ void __launch_bounds__(kSolverThreads) k_hwfv1(Leaves<T> lf, Hier<T> 
         lf.un[0][i] = h;
         lf.un[3][i] = qx;
         lf.un[6][i] = qy;
+        put_leaf_fv1(hout, a, h, qx, qy, own.z[0], mx);
         if (P.dt_leaf) P.dt_leaf[i] = leaf_dt;
         dt_loc = fmin(dt_loc, leaf_dt);
     }
+    mx.flush(sc);
     dt_loc = warp_min(dt_loc);
     __shared__ T red[kSolverThreads / 32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
