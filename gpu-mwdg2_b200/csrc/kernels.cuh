@@ -132,8 +132,8 @@ __device__ __forceinline__ void block_max_atomic(T (&v)[N], T* const (&dst)[N])
 }
 
 // ---------------------------------------------------------------- step bookkeeping
-// carry: the maxima come from the previous step's final RK stage (MWDG2 after its first
-// step); otherwise k_maxes_reinsert computes them.
+// carry: the maxima come from the previous step's last solver kernel (every step after the
+// first); otherwise k_leaf_maxima computes them.
 template <typename T> __device__ __forceinline__ void step_begin(Scalars<T>* sc, bool carry)
 {
     sc->max_eta = carry ? sc->next_max[0] : T(0);
@@ -189,10 +189,11 @@ __global__ void k_step_open(Scalars<T>* sc, bool carry, const StepArgs<T>* h_arg
 }
 
 // Maxima of the leaf state (mra/get_max_scale_coeffs.cu:3-27, with the reference's
-// use of qx0 for the qy maximum) and re-insertion of the leaf state into the hierarchy
+// use of qx0 for the qy maximum), for the first step; later steps take them from the
+// previous step's last solver kernel, which also re-inserts the state into the hierarchy
 // (mra/reinsert_assem_sol.cu:3-32).
-template <typename T, bool MW>
-__global__ void __launch_bounds__(256) k_maxes_reinsert(Leaves<T> lf, Hier<T> hr, Scalars<T>* sc, int n_fixed, bool reinsert)
+template <typename T>
+__global__ void __launch_bounds__(256) k_leaf_maxima(Leaves<T> lf, Hier<T> hr, Scalars<T>* sc, int n_fixed)
 {
     const int n = n_fixed >= 0 ? n_fixed : sc->n_leaves;
     T me = T(0), mh = T(0), mq = T(0), mz = T(0);
@@ -206,21 +207,6 @@ __global__ void __launch_bounds__(256) k_maxes_reinsert(Leaves<T> lf, Hier<T> hr
         mh = fmax(mh, fabs(h0));
         mq = fmax(mq, fabs(qx0));
         mz = fmax(mz, fabs(z0));
-        if (reinsert)
-        {
-            hr.s[0][0][a] = h0 + z0;
-            hr.s[1][0][a] = qx0;
-            hr.s[2][0][a] = lf.un[6][i];
-            if (MW)
-            {
-                hr.s[0][1][a] = lf.un[1][i] + hr.s[3][1][a];
-                hr.s[1][1][a] = lf.un[4][i];
-                hr.s[2][1][a] = lf.un[7][i];
-                hr.s[0][2][a] = lf.un[2][i] + hr.s[3][2][a];
-                hr.s[1][2][a] = lf.un[5][i];
-                hr.s[2][2][a] = lf.un[8][i];
-            }
-        }
     }
     T v[4] = {me, mh, mq, mz};
     T* const dst[4] = {&sc->max_eta, &sc->max_h, &sc->max_qx, &sc->max_z};

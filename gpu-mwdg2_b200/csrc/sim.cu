@@ -434,7 +434,7 @@ template <typename T> mwdg2_status Sim<T>::init(const char* par, const mwdg2_opt
             if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, threads, 0) != cudaSuccess || b < 1) b = 1;
             return b;
         };
-        grid_leaf_ = sms * resident(mw::k_maxes_reinsert<T, true>, 256);
+        grid_leaf_ = sms * resident(mw::k_leaf_maxima<T>, 256);
         grid_wet_ = sms * resident(mw::k_stage_wet<T, 1>, 256);
         grid_dry_ = sms * resident(mw::k_stage_dry<T, 1>, 256);
         grid_stage_ = sms * (mw_ ? resident(mw::k_mwdg2_stage<T, 1, false>, mw::kSolverThreads)
@@ -506,8 +506,7 @@ template <typename T> mwdg2_status Sim<T>::init(const char* par, const mwdg2_opt
     // maxima of the initial state (run_simulation.cu:190) then bed encoding with preflags
     // (mra/preflag_topo.cu:3-43)
     mw::k_step_begin<T><<<1, 1, 0, st_>>>(sc_, false);
-    if (mw_) mw::k_maxes_reinsert<T, true><<<red_blocks_, 256, 0, st_>>>(lf_, hr_, sc_, (int)F_, false);
-    else mw::k_maxes_reinsert<T, false><<<red_blocks_, 256, 0, st_>>>(lf_, hr_, sc_, (int)F_, false);
+    mw::k_leaf_maxima<T><<<red_blocks_, 256, 0, st_>>>(lf_, hr_, sc_, (int)F_);
     for (int level = L_ - 1; level >= 0; --level)
     {
         const int nb = grid_for((int64_t)1 << (2 * level), 256, 1 << 24);
@@ -623,8 +622,7 @@ template <typename T> mwdg2_status Sim<T>::enqueue_device()
         const int nfix = first_ ? (int)F_ : -1;
         if (!carry)
         {
-            if (mw) mw::k_maxes_reinsert<T, true><<<grid_leaf_, 256, 0, st_>>>(lf_, hr_, sc_, nfix, false);
-            else mw::k_maxes_reinsert<T, false><<<grid_leaf_, 256, 0, st_>>>(lf_, hr_, sc_, nfix, false);
+            mw::k_leaf_maxima<T><<<grid_leaf_, 256, 0, st_>>>(lf_, hr_, sc_, nfix);
             ++launches_;
         }
         if (nsrc > 0)

@@ -102,7 +102,9 @@ mwdg2_status mwdg2_get_sig(mwdg2_sim* sim, uint8_t* out, int64_t cap);
 
 /* One hierarchy array: field 0 eta, 1 qx, 2 qy, 3 z; mode 0, 1 (1x), 2 (1y);
  * n_hierarchy values. After an MWDG2 step the leaves' entries hold the new state and the
- * significant parents the scale coefficients encoded at the start of that step. */
+ * significant parents the scale coefficients encoded at the start of that step. After an
+ * HWFV1 step the leaves' entries of eta, qx and qy hold the new state (the step wrote them
+ * into the second of two alternating buffers); the other entries are not current. */
 mwdg2_status mwdg2_get_hierarchy(mwdg2_sim* sim, int field, int mode, double* out, int64_t cap);
 
 /* Depth h = eta - z of the leaf containing each stage point, in .stage file order
@@ -110,8 +112,9 @@ mwdg2_status mwdg2_get_hierarchy(mwdg2_sim* sim, int field, int mode, double* ou
 mwdg2_status mwdg2_read_stage(mwdg2_sim* sim, double* out, int n);
 
 /* Device timing of the last step's kernels, in milliseconds, by phase:
- * [0] maxima + re-insertion (HWFV1, and MWDG2's first step; later MWDG2 steps take both
- * from the previous stage 2) + point sources, [1] encode + threshold + regularisation,
+ * [0] step open: maxima (first step only; later steps take them, and the re-inserted state,
+ * from the previous step's last solver kernel) + point sources, [1] encode + threshold +
+ * regularisation,
  * [2] decode bands + extra significance of the upper levels, [3] leaf topology (tile
  * counts, scan, leaf list and neighbours) beside the value decode of the upper levels,
  * [4] MWDG2 stage 1 (or the HWFV1 update), [5] scale re-encode of the stage-1 result +
