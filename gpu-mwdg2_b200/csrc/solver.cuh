@@ -727,7 +727,7 @@ __global__ void __launch_bounds__(256) k_stage2_maxh(Leaves<T> lf, Hier<T> hr, S
 // index, into `hout`, the other of two alternating hierarchy buffers (no leaf reads `hout`
 // in this kernel), with the next step's maxima: the next step needs no re-insertion pass.
 template <typename T>
-__global__ void __launch_bounds__(kSolverThreads) k_hwfv1(Leaves<T> lf, Hier<T> hr, Hier<T> hout, Scalars<T>* sc,
+__global__ void __launch_bounds__(kSolverThreads, sizeof(T) == 4 ? 6 : 3) k_hwfv1(Leaves<T> lf, Hier<T> hr, Hier<T> hout, Scalars<T>* sc,
                                                           Params<T> P, const StepArgs<T>* args, bool friction)
 {
     const T dt = args->dt;
