@@ -81,3 +81,37 @@ def test_multiwavelet_round_trip_fp64(kat_lib):
         kat_lib.kat_mw_encode(64, _p(ch), _p(s), _p(d))
         kat_lib.kat_mw_decode(64, _p(s), _p(d), _p(back))
         assert np.max(np.abs(back - ch)) <= 1e-12 * 50.0
+
+
+@pytest.fixture(scope="module")
+def oracle_kat_lib(tmp_path_factory):
+    gxx = shutil.which("g++")
+    if not gxx:
+        pytest.skip("g++ not available")
+    out = str(tmp_path_factory.mktemp("kato") / "libkato.so")
+    subprocess.run([gxx, "-std=c++17", "-O2", "-fPIC", "-shared", "-ffp-contract=off", "-o", out,
+                    os.path.join(HERE, "filter_kat_oracle.cpp")], check=True, timeout=300)
+    lib = ctypes.CDLL(out)
+    dp = ctypes.POINTER(ctypes.c_double)
+    for f, n in (("kat_oracle_mw_encode", 3), ("kat_oracle_mw_decode", 3), ("kat_oracle_hw_encode", 2)):
+        getattr(lib, f).argtypes = [dp] * n
+        getattr(lib, f).restype = None
+    return lib
+
+
+def test_oracle_filters_pass_the_same_known_answers(oracle_kat_lib):
+    """The CPU oracle's filters (compiled as the oracle is: no fused multiply-adds)."""
+    k = KAT["hw_encode"]
+    out = np.zeros(4)
+    oracle_kat_lib.kat_oracle_hw_encode(_p(np.array(k["children"], np.float64)), _p(out))
+    _close(out, [k["scale"], k["alpha"], k["beta"], k["gamma"]], "oracle haar")
+    k = KAT["mw_encode"]
+    s, d = np.zeros(3), np.zeros(9)
+    oracle_kat_lib.kat_oracle_mw_encode(_p(np.array(k["children"], np.float64).ravel()), _p(s), _p(d))
+    _close(s, k["scale"], "oracle scale")
+    _close(d, np.array(k["details"]).ravel(), "oracle details")
+    k = KAT["mw_decode"]
+    c = np.zeros(12)
+    oracle_kat_lib.kat_oracle_mw_decode(_p(np.array(k["scale"], np.float64)),
+                                        _p(np.array(k["details"], np.float64).ravel()), _p(c))
+    _close(c, np.array(k["children"]).ravel(), "oracle children")
