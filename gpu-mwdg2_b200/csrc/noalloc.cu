@@ -11,7 +11,6 @@
 #include "../../include/mwdg2.h"
 #include "kernels.cuh"
 
-#include <mutex>
 #include <string>
 
 // Records the text returned by mwdg2_last_error (defined with the other entry points).
@@ -32,35 +31,24 @@ struct TopologyScratch
 // Shared by every call on this device; see the synchronisation note in include/mwdg2.h.
 static __device__ __align__(256) TopologyScratch g_topology_scratch;
 
-constexpr int kMaxDevices = 64;
-std::mutex g_setup_mutex;
-TopologyScratch* g_scratch_ptr[kMaxDevices] = {};
-
 mwdg2_status fail(mwdg2_status st, const std::string& msg)
 {
     mwdg2_detail_set_last_error(msg.c_str());
     return st;
 }
 
-// Device address of g_topology_scratch on the current device, looked up once per device.
-// In host code the symbol itself is only a host-side stand-in and must never be passed
-// to a kernel.
+// Device address of g_topology_scratch on the current device. In host code the symbol
+// itself is only a host-side stand-in and must never be passed to a kernel. The address is
+// looked up on every call rather than cached: the lookup is cheap, and a cached address
+// would go stale if the caller reset the device (the module, and the array with it, is
+// loaded again afterwards and may land elsewhere).
 mwdg2_status scratch_on_current_device(TopologyScratch** out)
 {
-    int dev = -1;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return fail(MWDG2_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
-    if (dev < 0 || dev >= kMaxDevices) return fail(MWDG2_ERR_CUDA, "device ordinal out of range");
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_ptr[dev])
-    {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_topology_scratch);
-        if (e != cudaSuccess || p == nullptr)
-            return fail(MWDG2_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-        g_scratch_ptr[dev] = static_cast<TopologyScratch*>(p);
-    }
-    *out = g_scratch_ptr[dev];
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_topology_scratch);
+    if (e != cudaSuccess || p == nullptr)
+        return fail(MWDG2_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    *out = static_cast<TopologyScratch*>(p);
     return MWDG2_OK;
 }
 

@@ -195,12 +195,12 @@ void mwdg2_batch_destroy(mwdg2_batch* b);
  *   d_nb_ids     device int32[4*cap]; d_nb_levels device uint8[4*cap] ([4][cap] layout)
  *   cap          at least 4^max_ref_lvl (every finest cell a leaf)
  *   n_leaves_out host; number of leaves written
- *   stream       cudaStream_t to run on (NULL: the default stream); the call returns
- *                after the outputs are complete
- * The first call on a device looks up the scratch array's device address
- * (cudaGetSymbolAddress) with that device current; make that first call before any
- * stream capture. Every call on a device shares the one scratch array, so calls whose
- * work overlaps on the GPU (different host threads or streams) race: serialise them. */
+ *   stream       cudaStream_t to run on (NULL: the default stream)
+ * The call blocks until the outputs are complete: it waits for `stream` and copies the leaf
+ * count into host memory. Each call looks up the scratch array's device address on the
+ * current device (cudaGetSymbolAddress), so a device reset between calls is harmless. Every
+ * call on a device shares the one scratch array, so calls whose work overlaps on the GPU
+ * (different host threads or streams) race: serialise them. */
 mwdg2_status mwdg2_leaf_topology_static(const uint8_t* d_sig, int max_ref_lvl, int xsz, int ysz,
                                         int32_t* d_act, uint8_t* d_levels, int32_t* d_nb_ids,
                                         uint8_t* d_nb_levels, int64_t cap, int64_t* n_leaves_out,

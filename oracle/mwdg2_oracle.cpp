@@ -91,6 +91,11 @@ public:
 
     bool init(const char* par_path, double eps_override, int solver_override);
     bool step();
+    // Leaf list and neighbours of the tree given by significance flags `s` (get_lvl_idx(L)
+    // bytes), with no simulation around it: the traversal and neighbour/compaction passes of
+    // a step (mra/traverse_tree_of_sig_details.cu, neighbours/find_neighbours.cu,
+    // neighbours/compaction.cu) on an MWDG2 grid of 2^L x 2^L cells whose DEM is xsz x ysz.
+    int topology_from_sig(const unsigned char* s, int L_, int xsz_, int ysz_);
 
     T* hier(int field, int mode)
     {
@@ -866,6 +871,35 @@ void Sim<T>::neighbours_and_compaction()
 }
 
 template <typename T>
+int Sim<T>::topology_from_sig(const unsigned char* s, int L_, int xsz_, int ysz_)
+{
+    L = L_;
+    M = 1 << L;
+    F = M * M;
+    xsz = xsz_;
+    ysz = ysz_;
+    solver = MWDG2;
+    n_det = lvl_idx(L);
+    sig.assign(s, s + n_det);
+    assem.alloc(F, false);
+    buf.alloc(F, false);
+    for (int d = 0; d < 4; ++d) { nb[d].alloc(F, false); buf_nb[d].alloc(F, false); }
+    flag_ne.assign(F, 0);
+    flag_sw.assign(F, 0);
+    rev_z_order.assign(F, 0);
+    rev_row_major.assign(F, 0);
+    for (int idx = 0; idx < F; ++idx)
+    {
+        const int code = morton(idx % M, idx / M);
+        rev_z_order[code] = idx;
+        rev_row_major[idx] = code;
+    }
+    traverse();
+    neighbours_and_compaction();
+    return assem.length;
+}
+
+template <typename T>
 void Sim<T>::load_soln(LeafArrays<T>& s)
 {
     // neighbours/load_soln_and_nghbr_coeffs.cu:3-104
@@ -1606,6 +1640,27 @@ int oracle_get_hier(void* p, int field, int mode, double* out)
         return 1;
     };
     return h->f ? get(*h->f) : get(*h->d);
+}
+
+// Leaf list and neighbours of a flag tree alone (Sim::topology_from_sig). Outputs hold up to
+// 4^L leaves (nb_ids / nb_lvls laid out [4][4^L]); returns the number of leaves.
+int oracle_leaf_topology(const unsigned char* sig, int L, int xsz, int ysz, int* act, int* lvl, int* nb_ids,
+                         int* nb_lvls)
+{
+    Sim<double> s;
+    const int n = s.topology_from_sig(sig, L, xsz, ysz);
+    const size_t cap = (size_t)1 << (2 * L);
+    for (int i = 0; i < n; ++i)
+    {
+        act[i] = s.assem.act[i];
+        lvl[i] = s.assem.lvl[i];
+        for (int d = 0; d < 4; ++d)
+        {
+            nb_ids[d * cap + i] = s.nb[d].act[i];
+            nb_lvls[d * cap + i] = s.nb[d].lvl[i];
+        }
+    }
+    return n;
 }
 
 void oracle_get_maxes(void* p, double* out)

@@ -43,6 +43,9 @@ def lib():
         L.oracle_get_hier.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp]
         L.oracle_get_maxes.argtypes = [vp, dp]
         L.oracle_num_threads.restype = ctypes.c_int
+        L.oracle_leaf_topology.restype = ctypes.c_int
+        L.oracle_leaf_topology.argtypes = [ctypes.POINTER(ctypes.c_ubyte), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                           ip, ip, ip, ip]
         _lib = L
     return _lib
 
@@ -141,6 +144,21 @@ class Oracle:
         out = np.zeros(5)
         lib().oracle_get_maxes(self._h, _p(out, ctypes.c_double))
         return out
+
+
+def leaf_topology(sig: np.ndarray, L: int, xsz: int, ysz: int) -> dict:
+    """Leaf list and neighbours (north, east, south, west) of the tree whose significance
+    flags are `sig` (get_lvl_idx(L) bytes), as a step's traversal and compaction give them."""
+    sig = np.ascontiguousarray(sig, dtype=np.uint8)
+    cap = 4 ** L
+    act = np.zeros(cap, np.int32)
+    lvl = np.zeros(cap, np.int32)
+    ids = np.zeros(4 * cap, np.int32)
+    lvls = np.zeros(4 * cap, np.int32)
+    n = lib().oracle_leaf_topology(_p(sig, ctypes.c_ubyte), L, xsz, ysz, _p(act, ctypes.c_int), _p(lvl, ctypes.c_int),
+                                   _p(ids, ctypes.c_int), _p(lvls, ctypes.c_int))
+    return {"act": act[:n], "lvl": lvl[:n], "nb_ids": ids.reshape(4, cap)[:, :n],
+            "nb_lvls": lvls.reshape(4, cap)[:, :n]}
 
 
 def num_threads() -> int:

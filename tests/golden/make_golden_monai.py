@@ -84,7 +84,7 @@ def golden_series(solver: str, eps: str, fixture=None) -> np.ndarray:
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref-cases", default="/root/reference/cases")
+    ap.add_argument("--ref-cases", default=os.path.join(os.environ.get("MWDG2_REFERENCE", "/root/reference"), "cases"))
     pack(ap.parse_args().ref_cases)
 
 
