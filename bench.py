@@ -44,7 +44,7 @@ def parse():
     ap.add_argument("--precision", type=int, default=32, choices=[32, 64])
     ap.add_argument("--solver", default="mwdg2", choices=["mwdg2", "hwfv1"])
     ap.add_argument("--level", type=int, default=None, help="max_ref_lvl (catchment 12, urban 13)")
-    ap.add_argument("--cpu-steps", type=int, default=2, help="timed oracle steps for cpu_baseline")
+    ap.add_argument("--cpu-steps", type=int, default=16, help="timed FP64 oracle steps for cpu_baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--case-dir", default=None)
     ap.add_argument("--workload", default="catchment", choices=["catchment", "urban", "ensemble"],
@@ -193,48 +193,74 @@ def peaks() -> tuple[float, str]:
         return 6650.0, "fallback"
 
 
-def cpu_baseline(par: str, a, steps: int) -> dict:
-    """The oracle (CPU restatement of the reference algorithm) on this machine's host cores."""
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def oracle_timing(par: str, steps: int, warmup: int) -> dict:
+    """The oracle (the reference algorithm restated in C++ with OpenMP) in FP64 -- the
+    plain stepper the CPU baseline is defined on -- on this machine's host cores: `warmup`
+    untimed steps (the first is the full encode from the initial grid), then `steps` timed
+    ones: active-cell updates/s and wall seconds per simulated second."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle_py
-    o = oracle_py.Oracle(par, a.precision)
-    o.step()  # first step (full encode from the initial grid) is not timed
-    n_tot = 0
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        ok, dt, n = o.step()
-        n_tot += n
-    wall = time.perf_counter() - t0
-    o.close()
+    o = oracle_py.Oracle(par, 64)
+    try:
+        for _ in range(max(1, warmup)):
+            o.step()
+        t_sim0 = o.info()["current_time"]
+        n_tot = 0
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            ok, dt, n = o.step()
+            n_tot += n
+        wall = time.perf_counter() - t0
+        t_sim = o.info()["current_time"] - t_sim0
+    finally:
+        o.close()
     return {"value": n_tot / wall, "unit": UNIT, "cores": oracle_py.num_threads(), "kind": "port",
-            "sample": f"steps 2..{steps + 1} of the same case ({steps} full adaptive steps, {n_tot} leaf updates, "
-                      f"{wall:.1f} s)"}
+            "dtype": "f64", "cpu_model": cpu_model(), "wall_s": wall, "leaf_updates": n_tot,
+            "wall_s_per_sim_s": wall / t_sim if t_sim > 0 else None,
+            "sample": f"steps {max(1, warmup) + 1}..{max(1, warmup) + steps} of the same case in FP64 "
+                      f"({steps} full adaptive steps, {n_tot} leaf updates, {wall:.1f} s on "
+                      f"{oracle_py.num_threads()} OpenMP threads)"}
+
+
+def cpu_baseline(par: str, a, steps: int) -> dict:
+    """The FP64 oracle on the host cores, for the line of this build's own arm."""
+    return oracle_timing(par, steps, 1)
 
 
 def run_reference(a):
+    """The reference arm: the reference algorithm on the host cores (it has no CPU path of
+    its own, so its FP64 restatement, the oracle port, stands in), timed on this arm's
+    workload; beside it, the reference's own CUDA build (oracle/_ref, its unmodified sources
+    compiled for sm_100a) on the same case, steps and warm-up in the arm's precision."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     par = make_case(a, 0)
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle_py
-    o = oracle_py.Oracle(par, a.precision)
-    for _ in range(a.warmup):
-        o.step()
-    n_tot = 0
-    t0 = time.perf_counter()
-    for _ in range(a.steps):
-        ok, dt, n = o.step()
-        n_tot += n
-    wall = time.perf_counter() - t0
-    v = n_tot / wall
+    cpu = oracle_timing(par, a.steps, a.warmup)
+    v = cpu["value"]
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
-            "ms_per_step": 1e3 * wall / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": f"f{a.precision}", "data": "synthetic (seeded fBm DEM)", "config": workload(a),
+            "ms_per_step": 1e3 * cpu["wall_s"] / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded fBm DEM)", "config": workload(a),
             "impl": "reference",
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": oracle_py.num_threads(), "kind": "port",
-                             "sample": f"{a.steps} full adaptive steps after {a.warmup} warm-up steps"},
+            "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample", "cpu_model", "dtype")},
+            "wall_s_per_sim_s": cpu["wall_s_per_sim_s"],
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    try:
+        import time_reference_build
+        line["reference_cuda"] = time_reference_build.time_reference(par, a.precision, a.steps, a.warmup)
+    except Exception as e:   # the binary is missing or the run failed: say so, keep the CPU line
+        line["reference_cuda"] = {"unavailable": f"{type(e).__name__}: {str(e)[:300]}"}
     print(json.dumps(line), flush=True)
 
 
@@ -342,6 +368,7 @@ def main():
 
     # device-timed steps (replicas: every rank runs the same workload on its own GPU)
     barrier()
+    t_sim0 = sim.info()["time"]
     ms_step, leaves, counters = [], [], []
     for _ in range(a.steps):
         ok, dt, n = sim.step()
@@ -349,6 +376,7 @@ def main():
         leaves.append(n)
         counters.append(sim.last_step_counters())
     barrier()
+    sim_s = sim.info()["time"] - t_sim0
     tot_ms = max_over_ranks(float(sum(ms_step)), dist, "cuda")
     value = replica_throughput(world, sum(leaves), tot_ms)
 
@@ -442,6 +470,9 @@ def main():
             "phase_timing": f"{PHASE_STEPS} steps after the timed ones with events between the phases inside "
                             "the step's graph (the timed steps carry none; each adds ~10 us)",
             "leaves_mean": n_mean,
+            "wall_s_per_sim_s": {"value": (tot_ms / 1e3) / sim_s if sim_s > 0 else None, "sim_seconds": sim_s,
+                                 "window": f"steps {a.warmup + 1}..{a.warmup + a.steps} of the run (device time of "
+                                           "the timed steps over the simulated time they advanced)"},
             "init_s": t_init,
             "wet_fraction": [float(np.mean([cc[k] for cc in counters])) / n_mean for k in ("wet_stage1", "wet_stage2")]}
     if rank == 0 and world == 1 and not a.no_cpu_baseline:

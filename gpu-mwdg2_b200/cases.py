@@ -17,6 +17,10 @@ implementation sees byte-identical inputs. Generators:
                         of uneven sizes (batched-ensemble benchmark).
 * urban_catchment     - fBm base with axis-aligned building blocks, a lake at rest and a
                         rising west-edge point inflow (8192^2 urban benchmark case).
+* bc_edges            - a lake over an fBm bed with boundary segments of every type
+                        (FREE, HFIX, HVAR, QFIX, QVAR) on the four sides.
+* start_q_nodata      - a DEM narrower than the mesh with -9999 (no-data) cells, and an
+                        initial discharge read from .start.Qx/.Qy rasters (startq2d).
 
 Reference quirks the generators respect (they would otherwise change the physics):
 * `wall_height` is set above every bed value, because `operators/dg2_update.cu:46`
@@ -402,3 +406,105 @@ def urban_catchment(directory: str, L: int = 13, solver: str = "mwdg2", eps: flo
     return Case(par=par, directory=directory, L=L, solver=solver, cellsize=cellsize,
                 sim_time=sim_time, dem=dem, start_h=start,
                 meta={"kind": "urban_catchment", "seed": seed, "cover": cover})
+
+
+def _write_series(path: str, series: dict[str, list[tuple[float, float]]]) -> None:
+    """A .bdy file holding several named series (classes/Boundary.h:427-466): a comment
+    line, then per series its name, "<rows> seconds" and "value time" rows."""
+    with open(path, "w") as fp:
+        fp.write("boundary series\n")
+        for name, rows in series.items():
+            fp.write(f"{name}\n{len(rows)} seconds\n")
+            for v, t in rows:
+                fp.write(f"{v!r} {t!r}\n")
+
+
+# Boundary segments of each variant, one line per side (classes/Boundary.h:332-371 reads the
+# first line starting with the side's letter; lower and upper are coordinates along the side).
+BC_EDGE_VARIANTS = {
+    "a": ["N 0 {ext} FREE", "E {q1} {q3} HFIX 1.3", "S {q1} {q3} QVAR SQ", "W 0 {ext} HVAR WH"],
+    "b": ["N {q1} {q3} QFIX 0.4", "E 0 {ext} FREE", "S 0 {ext} HFIX 1.2", "W {q1} {q3} QVAR WQ"],
+}
+
+
+def bc_edges(directory: str, variant: str = "a", L: int = 7, solver: str = "mwdg2", eps: float = 1e-3,
+             sim_time: float = 600.0, cellsize: float = 1.0, level: float = 1.0, relief: float = 0.8,
+             seed: int = 11, manning: float = 0.02, limitslopes: bool = False) -> Case:
+    """Still water at `level` over an fBm bed, driven through boundary segments.
+
+    Variant "a": north FREE (whole side), east HFIX 1.3 m (middle half), south QVAR
+    (middle half, series SQ rising to 0.6 m^2/s), west HVAR (whole side, series WH rising
+    to 1.4 m). Variant "b": north QFIX 0.4 m^2/s (middle half), east FREE, south HFIX
+    1.2 m, west QVAR (middle half, series WQ rising to 0.5 m^2/s). The series are padded
+    far beyond `sim_time` (the reference reads one row past the current one).
+    """
+    os.makedirs(directory, exist_ok=True)
+    n = 1 << L
+    dem = fbm_surface(n, 0.8, seed, relief)
+    h = np.maximum(0.0, level - dem)
+    write_esri_ascii(os.path.join(directory, "case.dem"), dem[::-1], cellsize, decimals=4)
+    write_esri_ascii(os.path.join(directory, "case.start"), h[::-1], cellsize, decimals=4)
+    ext = n * cellsize
+    fmt = {"ext": repr(ext), "q1": repr(ext / 4), "q3": repr(3 * ext / 4)}
+    with open(os.path.join(directory, "case.bci"), "w") as fp:
+        for line in BC_EDGE_VARIANTS[variant]:
+            fp.write(line.format(**fmt) + "\n")
+    pad = 4.0 * sim_time + 100.0
+    _write_series(os.path.join(directory, "case.bdy"), {
+        "WH": [(1.0, 0.0), (1.4, 2.0), (1.4, pad), (1.4, pad + 10.0)],
+        "SQ": [(0.0, 0.0), (0.6, 2.0), (0.6, pad), (0.6, pad + 10.0)],
+        "WQ": [(0.0, 0.0), (0.5, 1.5), (0.5, pad), (0.5, pad + 10.0)],
+    })
+    _write_stage(os.path.join(directory, "case.stage"), [(ext / 2 + cellsize / 2, ext / 2 + cellsize / 2)])
+    lines = _common_par(solver, L, eps, sim_time, 1000.0, manning, limitslopes, 10.0, None, None, None,
+                        ["DEMfile       case.dem", "startfile     case.start", "bcifile       case.bci",
+                         "bdyfile       case.bdy", "stagefile     case.stage"])
+    par = os.path.join(directory, "case.par")
+    _write_par(par, lines)
+    return Case(par=par, directory=directory, L=L, solver=solver, cellsize=cellsize, sim_time=sim_time,
+                dem=dem, start_h=h, meta={"kind": "bc_edges", "variant": variant})
+
+
+def start_q_nodata(directory: str, L: int = 7, solver: str = "mwdg2", eps: float = 1e-3,
+                   sim_time: float = 600.0, cellsize: float = 1.0, xsz: int = 120, ysz: int = 100,
+                   level: float = 1.0, relief: float = 0.8, seed: int = 13, wall_height: float = 5.0,
+                   manning: float = 0.02, limitslopes: bool = True, nan_cell: bool = False) -> Case:
+    """A lake over an fBm bed on an xsz x ysz DEM (narrower than the 2^L mesh) with a
+    block of no-data (-9999) cells, which the reference reads as `wall_height`
+    (input/read_raster_file.cpp:26-46), and a swirling initial discharge read from
+    case.start.Qx / case.start.Qy (`startq2d`, input/read_and_project_modes_dg2.cu:42-49).
+    The mesh outside the DEM keeps the bed at `wall_height` as well. `nan_cell` writes one
+    depth of the start raster as "nan" (a corrupted input)."""
+    os.makedirs(directory, exist_ok=True)
+    n = 1 << L
+    if xsz > n or ysz > n:
+        raise ValueError("the DEM must fit the 2^L mesh")
+    dem = fbm_surface(n, 0.8, seed, relief)[:ysz, :xsz]
+    h = np.maximum(0.0, level - dem)
+    yc, xc = (np.arange(ysz) + 0.5) * cellsize, (np.arange(xsz) + 0.5) * cellsize
+    X, Y = np.meshgrid(xc, yc)
+    qx = 0.2 * h * np.sin(2 * np.pi * Y / (ysz * cellsize))
+    qy = -0.15 * h * np.sin(2 * np.pi * X / (xsz * cellsize))
+    dem_out = np.round(dem, 4)
+    block = (slice(ysz // 2 - 4, ysz // 2 + 4), slice(xsz // 3, xsz // 3 + 10))
+    dem_out[block] = -9999.0
+    h[block], qx[block], qy[block] = 0.0, 0.0, 0.0
+    write_esri_ascii(os.path.join(directory, "case.dem"), dem_out[::-1], cellsize, decimals=4)
+    write_esri_ascii(os.path.join(directory, "case.start"), h[::-1], cellsize, decimals=4)
+    write_esri_ascii(os.path.join(directory, "case.start.Qx"), qx[::-1], cellsize, decimals=5)
+    write_esri_ascii(os.path.join(directory, "case.start.Qy"), qy[::-1], cellsize, decimals=5)
+    if nan_cell:
+        path = os.path.join(directory, "case.start")
+        lines = open(path).read().split("\n")
+        row = lines[6 + ysz // 4].split(" ")
+        row[xsz // 4] = "nan"
+        lines[6 + ysz // 4] = " ".join(row)
+        open(path, "w").write("\n".join(lines))
+    _write_stage(os.path.join(directory, "case.stage"), [(xsz * cellsize / 4, ysz * cellsize / 4)])
+    lines = _common_par(solver, L, eps, sim_time, wall_height, manning, limitslopes, 10.0, None, None, None,
+                        ["DEMfile       case.dem", "startfile     case.start", "startq2d",
+                         "stagefile     case.stage"])
+    par = os.path.join(directory, "case.par")
+    _write_par(par, lines)
+    return Case(par=par, directory=directory, L=L, solver=solver, cellsize=cellsize, sim_time=sim_time,
+                dem=dem_out, start_h=h, meta={"kind": "start_q_nodata", "xsz": xsz, "ysz": ysz})

@@ -385,7 +385,8 @@ __device__ __forceinline__ void put_leaf_fv1(const Hier<T>& hout, int a, T h, T 
 }
 
 // Wet test of one RK stage (the rule of leaf_is_dry, after ghost cells): wet leaves are
-// appended to `wet` (warp-aggregated) for k_mwdg2_stage<.., LIST=true>, dry ones marked in
+// appended to `wet` (warp-aggregated) for k_mwdg2_stage<.., LIST=true> (a NaN depth is not
+// below tol_h, so a NaN leaf is listed and the stage kernel reports it), dry ones marked in
 // `dry` for k_stage_dry, which then runs beside the wet-list kernel (the two touch disjoint
 // leaves). Stage 1 also keeps a dry leaf's depth after ghost cells in U^n (un[0]); stage 2
 // reports initial_tstep as the CFL step of dry leaves (dg2_update.cu:61).
@@ -529,6 +530,8 @@ __global__ void __launch_bounds__(kSolverThreads, sizeof(T) == 4 ? 5 : 2) k_mwdg
         for (int d = 0; d < 4; ++d) { nid[d] = lf.nb[d][i]; nl[d] = nid[d] == -1 ? level : level_of(nid[d]); }
         Cell<T> own;
         load_cell<T, true>(hr, a, own);
+        // a NaN depth anywhere in the state (a dry-looking NaN leaf is never updated below)
+        nan_seen |= (own.h[0] != own.h[0]);
         T gh[4], gqx[4], gqy[4];
         ghost_pass(own.h[0], own.qx[0], own.qy[0], own.z[0], nid, level, a, P, B, dt, gh, gqx, gqy);
         // Depths of the four neighbours (after ghost cells). A leaf whose own depth and
@@ -745,6 +748,8 @@ __global__ void __launch_bounds__(kSolverThreads, sizeof(T) == 4 ? 6 : 3) k_hwfv
         for (int d = 0; d < 4; ++d) nid[d] = lf.nb[d][i];
         Cell<T> own;
         load_cell<T, false>(hr, a, own);
+        // a NaN depth anywhere in the state (a NaN leaf with NaN neighbours is never updated)
+        nan_seen |= (own.h[0] != own.h[0]);
         T gh[4], gqx[4], gqy[4];
         ghost_pass(own.h[0], own.qx[0], own.qy[0], own.z[0], nid, level, a, P, B, dt, gh, gqx, gqy);
         bool fric = false;

@@ -12,6 +12,18 @@
  *   MWDG2_REF_STOP_AFTER  stop the process (exit 0) after this many steps
  *   MWDG2_REF_STEPS_CSV   per-step log "step,dt,n_leaves,wall_s" (always written
  *                         when set)
+ *   MWDG2_REF_DIGEST_DIR  directory for per-step digests (unset: none): every step,
+ *                         digest.csv gets one row "step,name,n,hash" per leaf-list,
+ *                         neighbour and significance array (hash: below), and at the
+ *                         steps listed in MWDG2_REF_SAMPLE_STEPS sample_step<n>.bin gets
+ *                         the leaf state after step n at up to 2048 evenly spaced leaves
+ *                         (12 rows of `real`) followed by the float64 sums of the 12 rows
+ *
+ * Digest of n 8- or 32-bit values v_i (their bit patterns, zero-extended):
+ *     n * 0x9E3779B97F4A7C15 + sum_i (v_i + 1) * (splitmix64(i) | 1)   (mod 2^64)
+ * with splitmix64 Vigna's finaliser of x + 0x9E3779B97F4A7C15. Every multiplier is odd, so
+ * a change in any single value changes the digest; tests/golden/make_golden_digest.py
+ * computes the same function in numpy for the product's arrays.
  *
  * Dump points (step n counts from 1, as the reference's `timestep`):
  *   compaction (run_simulation.cu:457)  -> leaf list + neighbours of step n
@@ -23,6 +35,8 @@
 #include "run_simulation.cuh"
 
 #include <chrono>
+#include <cstdint>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <set>
@@ -40,6 +54,59 @@ std::set<int> g_dump_steps;
 std::string   g_dump_dir;
 FILE*         g_steps_csv = nullptr;
 std::chrono::steady_clock::time_point g_t0;
+std::string   g_digest_dir;
+FILE*         g_digest_csv = nullptr;
+std::set<int> g_sample_steps;
+constexpr int kSample = 2048;
+
+std::set<int> parse_steps(const char* steps)
+{
+    std::set<int> out;
+    if (!steps) return out;
+    std::string s(steps);
+    size_t pos = 0;
+    while (pos < s.size())
+    {
+        size_t end = s.find(',', pos);
+        if (end == std::string::npos) end = s.size();
+        if (end > pos) out.insert(atoi(s.substr(pos, end - pos).c_str()));
+        pos = end + 1;
+    }
+    return out;
+}
+
+uint64_t splitmix64(uint64_t x)
+{
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+template <typename T>
+uint64_t digest_host(const T* v, size_t n)
+{
+    static_assert(sizeof(T) == 1 || sizeof(T) == 4, "8- or 32-bit values");
+    uint64_t h = (uint64_t)n * 0x9E3779B97F4A7C15ull;
+    for (size_t i = 0; i < n; ++i)
+    {
+        uint64_t bits;
+        if (sizeof(T) == 1) bits = *reinterpret_cast<const uint8_t*>(v + i);
+        else bits = *reinterpret_cast<const uint32_t*>(v + i);
+        h += (bits + 1) * (splitmix64(i) | 1ull);
+    }
+    return h;
+}
+
+template <typename T>
+void digest_dev(int step, const char* name, const T* d_ptr, size_t count)
+{
+    if (!g_digest_csv || d_ptr == nullptr) return;
+    std::vector<T> h(count);
+    if (count) cudaMemcpy(h.data(), d_ptr, count * sizeof(T), cudaMemcpyDeviceToHost);
+    fprintf(g_digest_csv, "%d,%s,%zu,%llu\n", step, name, count,
+            (unsigned long long)digest_host(h.data(), count));
+}
 
 void load_cfg()
 {
@@ -67,6 +134,14 @@ void load_cfg()
     }
     const char* stop = getenv("MWDG2_REF_STOP_AFTER");
     if (stop) g_stop_after = atoi(stop);
+    const char* ddir = getenv("MWDG2_REF_DIGEST_DIR");
+    if (ddir)
+    {
+        g_digest_dir = ddir;
+        g_digest_csv = fopen((g_digest_dir + "/digest.csv").c_str(), "w");
+        if (g_digest_csv) fprintf(g_digest_csv, "step,name,n,hash\n");
+        g_sample_steps = parse_steps(getenv("MWDG2_REF_SAMPLE_STEPS"));
+    }
     const char* csv = getenv("MWDG2_REF_STEPS_CSV");
     if (csv)
     {
@@ -127,6 +202,33 @@ void dump_assem(int step, const AssembledSolution& s)
     dump_dev(step, "qy1y", s.qy1y, n);
     dump_dev(step, "z1y",  s.z1y,  n);
 }
+// State after `step` at up to kSample evenly spaced leaves (index j * n / S), then the
+// float64 sums of the 12 rows over all leaves.
+void sample_assem(int step, const AssembledSolution& s)
+{
+    const size_t n = (size_t)s.length;
+    const size_t S = n < (size_t)kSample ? n : (size_t)kSample;
+    const real* rows[12] = {s.h0, s.qx0, s.qy0, s.z0, s.h1x, s.qx1x, s.qy1x, s.z1x, s.h1y, s.qx1y, s.qy1y, s.z1y};
+    std::vector<real> out(12 * S, real(0));
+    double sums[12] = {0};
+    std::vector<real> h(n);
+    for (int r = 0; r < 12; ++r)
+    {
+        if (rows[r] == nullptr || n == 0) continue;
+        cudaMemcpy(h.data(), rows[r], n * sizeof(real), cudaMemcpyDeviceToHost);
+        for (size_t j = 0; j < S; ++j) out[r * S + j] = h[j * n / S];
+        double acc = 0;
+        for (size_t i = 0; i < n; ++i) acc += (double)h[i];
+        sums[r] = acc;
+    }
+    char path[1024];
+    snprintf(path, sizeof(path), "%s/sample_step%06d.bin", g_digest_dir.c_str(), step);
+    FILE* fp = fopen(path, "wb");
+    if (!fp) return;
+    fwrite(out.data(), sizeof(real), out.size(), fp);
+    fwrite(sums, sizeof(double), 12, fp);
+    fclose(fp);
+}
 } // namespace
 
 __host__
@@ -144,6 +246,24 @@ void ref_hook_compaction
     compaction(d_buf_assem_sol, d_assem_sol, d_buf_neighbours, d_neighbours,
                d_compaction_flags, num_finest_elems, solver_params);
     const int step = g_step_done + 1;
+    load_cfg();
+    if (g_digest_csv)
+    {
+        const size_t m = (size_t)d_assem_sol.length;
+        digest_dev(step, "leaf_act", d_assem_sol.act_idcs, m);
+        digest_dev(step, "leaf_lvl", d_assem_sol.levels, m);
+        digest_dev(step, "nb_n_ids", d_neighbours.north.act_idcs, m);
+        digest_dev(step, "nb_e_ids", d_neighbours.east.act_idcs, m);
+        digest_dev(step, "nb_s_ids", d_neighbours.south.act_idcs, m);
+        digest_dev(step, "nb_w_ids", d_neighbours.west.act_idcs, m);
+        if (solver_params.solver_type == MWDG2)
+        {
+            digest_dev(step, "nb_n_lvls", d_neighbours.north.levels, m);
+            digest_dev(step, "nb_e_lvls", d_neighbours.east.levels, m);
+            digest_dev(step, "nb_s_lvls", d_neighbours.south.levels, m);
+            digest_dev(step, "nb_w_lvls", d_neighbours.west.levels, m);
+        }
+    }
     if (!want(step)) return;
     const size_t n = (size_t)d_assem_sol.length;
     int len = d_assem_sol.length;
@@ -174,6 +294,8 @@ void ref_hook_decoding
 {
     decoding(d_sig_details, d_norm_details, d_details, d_scale_coeffs, solver_params);
     const int step = g_step_done + 1;
+    load_cfg();
+    digest_dev(step, "sig", reinterpret_cast<unsigned char*>(d_sig_details), (size_t)get_lvl_idx(solver_params.L));
     if (!want(step)) return;
     const size_t n_det = (size_t)get_lvl_idx(solver_params.L);
     const size_t n_all = (size_t)get_lvl_idx(solver_params.L + 1);
@@ -210,6 +332,7 @@ Maxes ref_hook_get_max_scale_coeffs
     const int prev_step = call - 1;
     const bool dump = (call >= 2) && want(prev_step);
     if (dump) dump_assem(prev_step, d_assem_sol);
+    if (call >= 2 && g_digest_csv && g_sample_steps.count(prev_step)) sample_assem(prev_step, d_assem_sol);
     Maxes m = get_max_scale_coeffs(d_assem_sol, d_eta_temp);
     if (call >= 1 && want(call))
     {
@@ -242,6 +365,7 @@ real ref_hook_get_dt_CFL
     if (g_stop_after > 0 && g_step_done >= g_stop_after)
     {
         if (g_steps_csv) fclose(g_steps_csv);
+        if (g_digest_csv) fclose(g_digest_csv);
         cudaDeviceSynchronize();
         fflush(stdout);
         _exit(0);
@@ -270,4 +394,5 @@ void ref_hook_project_assem_sol
 void ref_hooks_finish()
 {
     if (g_steps_csv) { fclose(g_steps_csv); g_steps_csv = nullptr; }
+    if (g_digest_csv) { fclose(g_digest_csv); g_digest_csv = nullptr; }
 }

@@ -23,6 +23,39 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 
 
+def time_reference(par: str, precision: int, steps: int, warmup: int, exe: str | None = None,
+                   timeout: float = 1800.0) -> dict:
+    """Runs the reference build on `par` (from its folder) for warmup + steps steps and times
+    steps warmup+1 .. warmup+steps from its per-step log: ms per step, active-cell updates/s
+    and wall seconds per simulated second (the simulated time of a step is the dt the step
+    before it logged)."""
+    work = os.path.dirname(os.path.abspath(par))
+    exe = os.path.abspath(exe) if exe else os.path.join(HERE, "_ref", f"gpu-mwdg2-ref-fp{precision}")
+    if not os.path.exists(exe):
+        raise FileNotFoundError(f"{exe} is missing: build it with `make -C oracle ref`")
+    log = os.path.join(work, f"ref_steps_{os.getpid()}.csv")
+    env = dict(os.environ, MWDG2_REF_STOP_AFTER=str(warmup + steps), MWDG2_REF_STEPS_CSV=log)
+    r = subprocess.run([exe, os.path.basename(par)], cwd=work, env=env, capture_output=True, text=True,
+                       timeout=timeout)
+    if r.returncode != 0:
+        raise RuntimeError(f"reference build exited {r.returncode}: {r.stderr[-2000:]}")
+    rows = list(csv.DictReader(open(log)))
+    os.remove(log)
+    if len(rows) < warmup + steps:
+        raise RuntimeError(f"reference build logged {len(rows)} steps, {warmup + steps} wanted")
+    t0 = float(rows[warmup - 1]["wall_s"]) if warmup > 0 else 0.0
+    t1 = float(rows[warmup + steps - 1]["wall_s"])
+    leaves = sum(int(rw["n_leaves"]) for rw in rows[warmup:warmup + steps])
+    # step k advances the clock by the dt logged at the end of step k - 1
+    sim = sum(float(rw["dt"]) for rw in rows[max(0, warmup - 1):warmup + steps - 1])
+    return {"impl": "reference CUDA build", "dtype": f"f{precision}", "steps": steps, "warmup": warmup,
+            "ms_per_step": 1e3 * (t1 - t0) / steps, "value": leaves / (t1 - t0), "unit": "cell-updates/s",
+            "leaves_mean": leaves / steps, "sim_seconds": sim,
+            "wall_s_per_sim_s": (t1 - t0) / sim if sim > 0 else None,
+            "timing": "host wall clock between the ends of steps W and W+K (each step ends with a "
+                      "device-to-host copy of dt)"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--precision", type=int, default=32, choices=[32, 64])
@@ -36,30 +69,14 @@ def main():
     sys.path.insert(0, ROOT)
     import bench
     case = argparse.Namespace(workload="catchment", level=a.level, solver=a.solver, precision=a.precision,
-                              case_dir=a.case_dir)
+                              case_dir=a.case_dir, window="start")
     par = bench.make_case(case, 0)
-    work = os.path.dirname(os.path.abspath(par))
-    exe = os.path.abspath(a.exe) if a.exe else os.path.join(HERE, "_ref", f"gpu-mwdg2-ref-fp{a.precision}")
-    if not os.path.exists(exe):
-        raise SystemExit(f"{exe} is missing: build it with `make -C oracle ref`")
-    log = os.path.join(work, f"ref_steps_{a.solver}_fp{a.precision}.csv")
-    env = dict(os.environ, MWDG2_REF_STOP_AFTER=str(a.warmup + a.steps), MWDG2_REF_STEPS_CSV=log)
-    r = subprocess.run([exe, os.path.basename(par)], cwd=work, env=env, capture_output=True, text=True,
-                       timeout=1800)
-    if r.returncode != 0:
-        raise SystemExit(f"reference build exited {r.returncode}: {r.stderr[-2000:]}")
-    rows = list(csv.DictReader(open(log)))
-    if len(rows) < a.warmup + a.steps:
-        raise SystemExit(f"reference build logged {len(rows)} steps, {a.warmup + a.steps} wanted")
-    t0 = float(rows[a.warmup - 1]["wall_s"]) if a.warmup > 0 else 0.0
-    t1 = float(rows[a.warmup + a.steps - 1]["wall_s"])
-    leaves = sum(int(rw["n_leaves"]) for rw in rows[a.warmup:a.warmup + a.steps])
-    print(json.dumps({"impl": "reference CUDA build", "solver": a.solver, "dtype": f"f{a.precision}",
-                      "workload": bench.workload(case)["workload"], "steps": a.steps, "warmup": a.warmup,
-                      "ms_per_step": 1e3 * (t1 - t0) / a.steps, "value": leaves / (t1 - t0),
-                      "unit": "cell-updates/s", "leaves_mean": leaves / a.steps,
-                      "timing": "host wall clock between the ends of steps W and W+K (each step ends with a "
-                                "device-to-host copy of dt)"}), flush=True)
+    try:
+        d = time_reference(par, a.precision, a.steps, a.warmup, a.exe)
+    except (FileNotFoundError, RuntimeError) as e:
+        raise SystemExit(str(e))
+    d.update({"solver": a.solver, "workload": bench.workload(case)["workload"]})
+    print(json.dumps(d), flush=True)
 
 
 if __name__ == "__main__":

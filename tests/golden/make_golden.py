@@ -45,6 +45,15 @@ def case_specs():
         "fbm_mw_l7_fp64": (dict(kind="fbm", L=7, solver="mwdg2"), 64),
         "fbm_hw_l7_fp64": (dict(kind="fbm", L=7, solver="hwfv1"), 64),
         "lake_mw_l7_fp64": (dict(kind="lake", L=7, solver="mwdg2"), 64),
+        # boundary segments of every type on the four sides (two layouts)
+        "edges_a_mw_l7_fp64": (dict(kind="edges_a", L=7, solver="mwdg2"), 64),
+        "edges_a_hw_l7_fp64": (dict(kind="edges_a", L=7, solver="hwfv1"), 64),
+        "edges_b_mw_l7_fp64": (dict(kind="edges_b", L=7, solver="mwdg2"), 64),
+        "edges_b_hw_l7_fp64": (dict(kind="edges_b", L=7, solver="hwfv1"), 64),
+        "edges_a_mw_l7_fp32": (dict(kind="edges_a", L=7, solver="mwdg2"), 32),
+        # a 120 x 100 DEM with no-data cells, initial discharge from .start.Qx/.Qy
+        "startq_mw_l7_fp64": (dict(kind="startq", L=7, solver="mwdg2"), 64),
+        "startq_hw_l7_fp64": (dict(kind="startq", L=7, solver="hwfv1"), 64),
     }
     return specs
 
@@ -61,6 +70,10 @@ def make_case(kind: str, directory: str, L: int, solver: str):
                                    limitslopes=(solver == "mwdg2"))
     if kind == "lake":
         return cases.lake_at_rest(directory, L=L, solver=solver, sim_time=10.0)
+    if kind in ("edges_a", "edges_b"):
+        return cases.bc_edges(directory, variant=kind[-1], L=L, solver=solver)
+    if kind == "startq":
+        return cases.start_q_nodata(directory, L=L, solver=solver)
     raise ValueError(kind)
 
 
@@ -166,6 +179,7 @@ def main():
     ap.add_argument("--ref-dir", default=os.path.join(ROOT, "oracle", "_ref"))
     ap.add_argument("--max-step", type=int, default=40)
     ap.add_argument("--only", default=None)
+    ap.add_argument("--append", action="store_true", help="keep the other entries of index.json")
     a = ap.parse_args()
     os.makedirs(a.out, exist_ok=True)
     if a.retrim:
@@ -178,13 +192,14 @@ def main():
         if os.path.exists(idx):
             shutil.copy(idx, os.path.join(a.out, "index.json"))
         return
-    index = []
+    index_path = os.path.join(a.out, "index.json")
+    index = json.load(open(index_path)) if a.append and os.path.exists(index_path) else []
     for name, spec in case_specs().items():
-        if a.only and a.only not in name:
+        if a.only and not any(o in name for o in a.only.split(",")):
             continue
         info = run_case(name, spec, a.ref_dir, a.out, a.max_step)
         print(json.dumps(info), flush=True)
-        index.append(info)
+        index = [e for e in index if e["name"] != name] + [info]
     with open(os.path.join(a.out, "index.json"), "w") as fp:
         json.dump(index, fp, indent=1)
 

@@ -1,0 +1,140 @@
+"""The benchmarked configurations and the full parity run against the reference build.
+
+Fixtures (tests/golden/digest_*.npz, written by tests/golden/make_golden_digest.py from the
+reference's own CUDA build) hold, for every step of
+
+* the 4096^2 fBm benchmark catchment (max_ref_lvl 12, 25 steps): MWDG2 and HWFV1, each in
+  FP32 and FP64 -- the levels-10-and-up kernels (dense, sparse and folded encodes, the
+  flag pass, the value decode beside the topology) in the precision the benchmark runs;
+* the 256^2 circular dam break (max_ref_lvl 8, MWDG2) over its whole 3.5 s (292 steps),
+  FP64 and FP32,
+
+a 64-bit digest of the leaf list, neighbour ids (and levels) and significance flags, the
+step's dt and leaf count, and at a few steps the state at 2048 evenly spaced leaves plus
+the float64 sums of the state rows. The product runs the same inputs through the C ABI.
+
+Bounds (every step unless noted):
+* leaf list, levels, neighbour ids and levels, significance flags: bit-exact (equal digests);
+* leaf count equal; dt within 1e-9 (FP64) / 2e-5 (FP32) relative;
+* FP64 state: sampled values within 1e-10 relative to max(1, |value|), row sums within
+  1e-10 of sum(max(1, |value|));
+* FP32 state: 2e-5 for the first 40 steps. Beyond them FP32 rounding grows through the
+  moving shock in any build: the reference's own FP32 build leaves its FP64 build by
+  3.4e-5 at step 50 of the dam break and their trees part at step 68. So a later sample
+  is held to twice the reference FP32 build's own distance from its FP64 build at that
+  step while the two reference trees agree, and is only reported once they have parted
+  (the topology stays checked bit for bit at every step).
+With MWDG2_TEST_REPORT set to a folder, every case writes its measured errors there."""
+import json
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+import make_golden_digest as mgd
+import mwdg2_b200
+from gpu_util import FIELDS
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLDEN = os.path.join(HERE, "golden")
+TOL = {64: 1e-10, 32: 2e-5}
+DT_TOL = {64: 1e-9, 32: 2e-5}
+FP32_STRICT_STEPS = 40
+CASES = sorted(mgd.case_specs().items())
+
+
+def _digests(dig: mgd.Digester, sim) -> dict:
+    lv = sim.leaves()
+    out = {"leaf_act": dig(lv["act"].astype(np.int32)), "leaf_lvl": dig(lv["lvl"].astype(np.int32))}
+    for k, d in enumerate("nesw"):
+        out[f"nb_{d}_ids"] = dig(lv["nb_ids"][k].astype(np.int32))
+        out[f"nb_{d}_lvls"] = dig(lv["nb_lvls"][k].astype(np.int32))
+    out["sig"] = dig(sim.sig(), 8)
+    return out
+
+
+def _rel(a, b) -> float:
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.max(np.abs(a - b) / np.maximum(1.0, np.abs(b)))) if a.size else 0.0
+
+
+def _fp32_own_drift(name: str, g32) -> dict:
+    """Step -> the reference FP32 build's largest sampled deviation from the reference FP64
+    build of the same case, at sample steps where the two reference runs have the same
+    tree (equal digests and leaf counts up to that step)."""
+    path = os.path.join(GOLDEN, f"digest_{name.replace('fp32', 'fp64')}.npz")
+    if not os.path.exists(path):
+        return {}
+    g64 = np.load(path)
+    n = min(g32["digest"].shape[0], g64["digest"].shape[0])
+    same = np.all(g32["digest"][:n] == g64["digest"][:n], axis=1) & (g32["steps_n"][:n] == g64["steps_n"][:n])
+    agree_to = n if same.all() else int(np.argmin(same))   # steps 1..agree_to agree
+    out = {}
+    for s in (int(x) for x in g32["sample_steps"]):
+        if s <= agree_to and f"sample_{s}" in g64.files:
+            out[s] = _rel(g32[f"sample_{s}"], g64[f"sample_{s}"])
+    return out
+
+
+def _state_tol(prec: int, s: int, drift: dict):
+    if prec == 64 or s <= FP32_STRICT_STEPS:
+        return TOL[prec]
+    return max(TOL[32], 2.0 * drift[s]) if s in drift else None
+
+
+@pytest.mark.parametrize("name,spec", CASES, ids=[n for n, _ in CASES])
+def test_every_step_matches_reference_build(name, spec):
+    g = np.load(os.path.join(GOLDEN, f"digest_{name}.npz"))
+    names = [str(n) for n in g["names"]]
+    present = g["present"]
+    table = g["digest"]
+    nsteps = table.shape[0]
+    prec = spec["precision"]
+    samples = set(int(s) for s in g["sample_steps"])
+    drift = _fp32_own_drift(name, g) if prec == 32 else {}
+    dig = mgd.Digester()
+    dts, report, failures = [], {"case": name, "steps": nsteps, "samples": {}}, []
+    with tempfile.TemporaryDirectory() as d:
+        c = mgd.make_case(spec, d)
+        sim = mwdg2_b200.Simulation(c.par, precision=prec)
+        try:
+            for s in range(1, nsteps + 1):
+                ok, dt, n = sim.step()
+                assert ok, f"{name}: run ended at step {s}, the reference took {nsteps}"
+                dts.append(dt)
+                assert n == int(g["steps_n"][s - 1]), f"{name} step {s}: {n} leaves, reference {g['steps_n'][s - 1]}"
+                mine = _digests(dig, sim)
+                bad = [k for i, k in enumerate(names) if present[i] and mine[k] != int(table[s - 1, i])]
+                assert not bad, f"{name} step {s}: differs from the reference build in {bad}"
+                if s not in samples:
+                    continue
+                st = sim.state()
+                ref = g[f"sample_{s}"]
+                S = ref.shape[1]
+                idx = (np.arange(S, dtype=np.int64) * n) // S
+                tol = _state_tol(prec, s, drift)
+                errs = {}
+                for r, f in enumerate(FIELDS):
+                    e = _rel(st[f][idx], ref[r])
+                    full = np.asarray(st[f], np.float64)
+                    ds = abs(float(np.sum(full)) - float(g[f"sums_{s}"][r])) / float(np.sum(np.maximum(1.0, np.abs(full))))
+                    errs[f] = (e, ds)
+                    if tol is not None and (e > tol or ds > tol):
+                        failures.append(f"step {s} {f}: sampled {e:.3e}, row sum {ds:.3e} (bound {tol:.1e})")
+                report["samples"][s] = {"bound": tol, "max_sampled": max(v[0] for v in errs.values()),
+                                        "max_row_sum": max(v[1] for v in errs.values()),
+                                        "reference_fp32_vs_fp64": drift.get(s)}
+        finally:
+            sim.close()
+    e = float(np.max(np.abs(np.array(dts) - g["steps_dt"]) / np.abs(g["steps_dt"])))
+    report["dt_max_rel"] = e
+    out = os.environ.get("MWDG2_TEST_REPORT")
+    if out:
+        os.makedirs(out, exist_ok=True)
+        with open(os.path.join(out, f"digest_{name}.json"), "w") as fp:
+            json.dump(report, fp, indent=1)
+    assert not failures, f"{name}: " + "; ".join(failures)
+    assert e <= DT_TOL[prec], f"{name}: dt differs by {e:.3e}"
