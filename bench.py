@@ -52,6 +52,9 @@ def parse():
                          "inflow; ensemble: a batch of seeded uneven scenarios (mwdg2_batch_*) against the "
                          "same members stepped one after another; prints its own line")
     ap.add_argument("--members", type=int, default=64)
+    ap.add_argument("--peak-time", type=float, default=1800.0,
+                    help="catchment: a second timing window starting at this simulated time (the hydrograph "
+                         "peak); <= 0 skips it")
     a = ap.parse_args()
     if a.level is None:
         a.level = 13 if a.workload == "urban" else 12
@@ -256,11 +259,17 @@ def run_reference(a):
             "wall_s_per_sim_s": cpu["wall_s_per_sim_s"],
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import time_reference_build
     try:
-        import time_reference_build
         line["reference_cuda"] = time_reference_build.time_reference(par, a.precision, a.steps, a.warmup)
     except Exception as e:   # the binary is missing or the run failed: say so, keep the CPU line
         line["reference_cuda"] = {"unavailable": f"{type(e).__name__}: {str(e)[:300]}"}
+    if a.workload == "catchment" and a.peak_time > 0:
+        try:
+            line["reference_cuda_peak"] = time_reference_build.time_reference(par, a.precision, a.steps, a.warmup,
+                                                                              window_time=a.peak_time)
+        except Exception as e:
+            line["reference_cuda_peak"] = {"unavailable": f"{type(e).__name__}: {str(e)[:300]}"}
     print(json.dumps(line), flush=True)
 
 
@@ -327,6 +336,43 @@ def run_ensemble(a):
             "sequential": {"value": upd_seq / t_seq, "seconds": t_seq, "leaf_updates": upd_seq},
             "batch_over_sequential": (upd / t_batch) / (upd_seq / t_seq)}
     print(json.dumps(line), flush=True)
+
+
+def peak_window(sim, a, dist) -> dict:
+    """The same run later on: steps (untimed) until the simulated time reaches a.peak_time,
+    then W warm-up steps and K steps timed as the first window (two CUDA events around each
+    step): active-cell updates/s, ms per step, wall seconds per simulated second and the
+    fraction of leaves that are wet in each RK stage."""
+    import numpy as np
+    sim.set_timing("step")
+    t0 = time.perf_counter()
+    advance = 0
+    while sim.info()["time"] < a.peak_time:
+        ok, dt, n = sim.step()
+        if not ok:
+            return {"unavailable": f"the run ended before t = {a.peak_time} s"}
+        advance += 1
+    advance_s = time.perf_counter() - t0
+    for _ in range(a.warmup):
+        sim.step()
+    t_sim0 = sim.info()["time"]
+    ms, leaves, wet = [], [], []
+    for _ in range(a.steps):
+        ok, dt, n = sim.step()
+        ms.append(float(sim.last_step_timing()[7]))
+        leaves.append(n)
+        c = sim.last_step_counters()
+        wet.append((c["wet_stage1"], c["wet_stage2"]))
+    sim_s = sim.info()["time"] - t_sim0
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    tot_ms = max_over_ranks(float(sum(ms)), dist, "cuda")
+    n_mean = float(np.mean(leaves))
+    return {"from_time": a.peak_time, "steps_to_reach": advance, "seconds_to_reach": advance_s,
+            "time_at_window": t_sim0, "value": replica_throughput(world, sum(leaves), tot_ms),
+            "ms_per_step": tot_ms / a.steps, "leaves_mean": n_mean,
+            "wet_fraction": [float(np.mean([w[k] for w in wet])) / n_mean for k in (0, 1)],
+            "wall_s_per_sim_s": (tot_ms / 1e3) / sim_s if sim_s > 0 else None, "sim_seconds": sim_s,
+            "timing": "device time of each step (CUDA events on the library's stream), max over ranks"}
 
 
 def main():
@@ -475,6 +521,8 @@ def main():
                                            "the timed steps over the simulated time they advanced)"},
             "init_s": t_init,
             "wet_fraction": [float(np.mean([cc[k] for cc in counters])) / n_mean for k in ("wet_stage1", "wet_stage2")]}
+    if a.workload == "catchment" and a.peak_time > 0:
+        line["window_peak"] = peak_window(sim, a, dist)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(par, a, a.cpu_steps)
     sim.close()

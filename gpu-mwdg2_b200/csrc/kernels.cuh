@@ -48,6 +48,19 @@ template <typename T> struct Scalars
     T next_max[4];                    // maxima of the state at the end of the step (eta, h, qx, z)
     T xs_factor;                      // 2^(M_BAR+1) of the extra-significance threshold (extra_eps)
     int32_t min_leaf;                 // lowest leaf level of this step's tree (k_tile_emit)
+    // learned refinement proposal (csrc/proposal.cuh): subtrees of the proposal level that
+    // were active in the step, active but not proposed, and proposed
+    uint32_t prop_active, prop_missed, prop_proposed;
+};
+
+// The subtrees below the nodes of level `level` (the proposal level) that a step's encode and
+// decode visit: prop[node] != 0 (null: all), and where the encode records a change of a
+// significance flag (act[node] = 1; null: nowhere).
+struct PropMask
+{
+    const uint8_t* prop;
+    uint8_t* act;
+    int level;
 };
 
 template <typename T> struct Params
@@ -55,6 +68,10 @@ template <typename T> struct Params
     int L, M, xsz, ysz, limit;
     T dx, tol_h, tol_q, tol_s, g, manning, CFL, initial_tstep, wall_height, tol_Krivo, eps;
     T* dt_leaf;   // per-leaf CFL step of the final stage (VTK output), or null
+    // learned refinement proposal: the RK stages mark the node of level act_level above every
+    // leaf they update (act[node] = 1); null: no marks
+    uint8_t* act;
+    int act_level;
 };
 
 template <typename T> struct Bnd
@@ -152,6 +169,9 @@ template <typename T> __device__ __forceinline__ void step_begin(Scalars<T>* sc,
     sc->xs_factor = pow(T(2.0), T(1.5) + 1);
 #pragma unroll
     for (int l = 0; l < 16; ++l) sc->sig_level[l] = 0;
+    sc->prop_active = 0;
+    sc->prop_missed = 0;
+    sc->prop_proposed = 0;
 }
 template <typename T> __global__ void k_step_begin(Scalars<T>* sc, bool carry) { step_begin(sc, carry); }
 
@@ -278,11 +298,14 @@ template <typename T> __device__ __forceinline__ T extra_eps(T eps, int L, int l
 // Encode one parent (mra/encode_flow_kernel_{mw,hw}.cu), threshold it and OR in the
 // children's significance (mra/regularisation_kernel.cu). FULL = false re-encodes scale
 // coefficients of significant parents only (run_simulation.cu:573-588).
-template <typename T, bool MW, bool FULL>
+template <typename T, bool MW, bool FULL, bool PM = false>
 __device__ __forceinline__ void encode_parent(const Hier<T>& hr, const Scalars<T>* sc, int L, int level, int idx, T eps,
-                                              unsigned& n_done)
+                                              unsigned& n_done, const PropMask& pm = PropMask{})
 {
     const int p = lvl_idx(level) + idx;
+    // PM: a parent in a subtree the proposal leaves out keeps its flags and values
+    const int anc = (PM && level >= pm.level) ? (idx >> (2 * (level - pm.level))) : -1;
+    if (PM && anc >= 0 && pm.prop && !pm.prop[anc]) return;
     const uint8_t f = hr.flags[p];
     const bool was_sig = (f & F_SIG) != 0;
     const int c = lvl_idx(level + 1) + 4 * idx;
@@ -351,6 +374,7 @@ __device__ __forceinline__ void encode_parent(const Hier<T>& hr, const Scalars<T
         ++n_done;
     }
     if (nf != f) hr.flags[p] = nf;   // most large-level parents keep their flags
+    if (PM && anc >= 0 && pm.act && ((nf ^ f) & F_SIG)) pm.act[anc] = 1;
 }
 
 // Small levels are processed in bands of up to kBandDepth levels, one CTA per node of the
@@ -368,8 +392,9 @@ constexpr int kBandMaxLevel = 9;
 // (significant ones; FULL also clears the stale flag bits of the others, as k_level_sparse
 // does) before the parent itself: a child's data is touched by its parent's thread only,
 // and the sparse level needs no launch (and no scan of its flags) of its own.
-template <typename T, bool MW, bool FULL, bool FOLD = false>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 6 : 4) k_encode_level(Hier<T> hr, Scalars<T>* sc, int L, int level, T eps)
+template <typename T, bool MW, bool FULL, bool FOLD = false, bool PM = false>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 6 : 4) k_encode_level(Hier<T> hr, Scalars<T>* sc, int L, int level, T eps,
+                                                                         PropMask pm = PropMask{})
 {
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
     const bool in = idx < (1 << (2 * level));
@@ -388,7 +413,9 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 6 : 4) k_encode_level(Hi
         {
             const uint32_t f = (cw >> (8 * j)) & 0xffu;
             go = (f & F_SIG) != 0;
-            if (FULL && !go && (f & ~(uint32_t)F_PRE)) hr.flags[cfirst + cb + j] = (uint8_t)(f & F_PRE);
+            const bool kept = PM && level + 1 >= pm.level && pm.prop &&
+                              !pm.prop[(cb + j) >> (2 * (level + 1 - pm.level))];
+            if (FULL && !go && !kept && (f & ~(uint32_t)F_PRE)) hr.flags[cfirst + cb + j] = (uint8_t)(f & F_PRE);
             lv = level + 1;
             id = cb + j;
         }
@@ -398,7 +425,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 6 : 4) k_encode_level(Hi
             lv = level;
             id = idx;
         }
-        if (go) encode_parent<T, MW, FULL>(hr, sc, L, lv, id, eps, done);
+        if (go) encode_parent<T, MW, FULL, PM>(hr, sc, L, lv, id, eps, done, pm);
     }
     const unsigned tot = __reduce_add_sync(0xffffffffu, done);
     if ((threadIdx.x & 31) == 0 && tot) atomicAdd(FULL ? &sc->enc : &sc->enc2, (unsigned long long)tot);
@@ -513,11 +540,13 @@ __global__ void __launch_bounds__(256) k_encode_band(Hier<T> hr, Scalars<T>* sc,
 // reference (mra/zero_details.cu).
 // FLAGS = false: values only; the flags of the children are then set by k_extra_sig_level
 // from F_XS, which the encode derived from the same details.
-template <typename T, bool MW, bool FLAGS = true>
+template <typename T, bool MW, bool FLAGS = true, bool PM = false>
 __device__ __forceinline__ void decode_parent(const Hier<T>& hr, const Scalars<T>* sc, int L, int level, int idx, T eps,
-                                              unsigned& n_done)
+                                              unsigned& n_done, const PropMask& pm = PropMask{})
 {
     const int p = lvl_idx(level) + idx;
+    // PM: the children of a parent in a subtree the proposal leaves out keep their values
+    if (PM && level >= pm.level && pm.prop && !pm.prop[idx >> (2 * (level - pm.level))]) return;
     const uint8_t f = hr.flags[p];
     if (!(f & F_SIG)) return;
     const bool enc = (f & F_ENC) != 0;
@@ -708,12 +737,13 @@ __global__ void __launch_bounds__(256) k_extra_sig_level(uint8_t* flags, const S
 
 // One level of parents (levels above kBandMaxLevel), values only (k_extra_sig_level set the
 // children's flags).
-template <typename T, bool MW>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4) k_decode_level(Hier<T> hr, Scalars<T>* sc, int L, int level, T eps)
+template <typename T, bool MW, bool PM = false>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4) k_decode_level(Hier<T> hr, Scalars<T>* sc, int L, int level, T eps,
+                                                                         PropMask pm = PropMask{})
 {
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned done = 0;
-    if (idx < (1 << (2 * level))) decode_parent<T, MW, false>(hr, sc, L, level, idx, eps, done);
+    if (idx < (1 << (2 * level))) decode_parent<T, MW, false, PM>(hr, sc, L, level, idx, eps, done, pm);
     const unsigned tot = __reduce_add_sync(0xffffffffu, done);
     if ((threadIdx.x & 31) == 0 && tot)
     {
@@ -730,8 +760,9 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4) k_decode_level(Hi
 // parents with a handful significant costs 512K threads that read 8 bytes each instead of
 // 4M threads. Op 0: FULL encode, 1: scale-only re-encode, 2: decode (values only, as
 // k_decode_level).
-template <typename T, bool MW, int OP>
-__global__ void __launch_bounds__(256) k_level_sparse(Hier<T> hr, Scalars<T>* sc, int L, int level, T eps)
+template <typename T, bool MW, int OP, bool PM = false>
+__global__ void __launch_bounds__(256) k_level_sparse(Hier<T> hr, Scalars<T>* sc, int L, int level, T eps,
+                                                      PropMask pm = PropMask{})
 {
     if (OP == 1 && sc->min_leaf > level) return;   // see scale_only_needed
     __shared__ int list[8][256];   // per warp: up to 32 lanes x 8 parents
@@ -747,10 +778,12 @@ __global__ void __launch_bounds__(256) k_level_sparse(Hier<T> hr, Scalars<T>* sc
         for (int j = 0; j < 8; ++j)
         {
             const uint32_t f = ((j < 4 ? w.x : w.y) >> (8 * (j & 3))) & 0xffu;
-            if (f & F_SIG) sig |= 1u << j;
+            const bool kept = PM && level >= pm.level && pm.prop &&
+                              !pm.prop[(int)((first + j) >> (2 * (level - pm.level)))];
+            if (f & F_SIG) sig |= kept ? 0u : 1u << j;
             // FULL encode of a parent that was not significant: only its flag changes (its
             // encode / extra-significance bits from the last step clear, the preflag stays)
-            else if (OP == 0 && (f & ~(uint32_t)F_PRE)) hr.flags[lvl_idx(level) + first + j] = (uint8_t)(f & F_PRE);
+            else if (OP == 0 && !kept && (f & ~(uint32_t)F_PRE)) hr.flags[lvl_idx(level) + first + j] = (uint8_t)(f & F_PRE);
         }
     }
     const int c = __popc(sig);
@@ -769,9 +802,9 @@ __global__ void __launch_bounds__(256) k_level_sparse(Hier<T> hr, Scalars<T>* sc
     for (int e = lane; e < total; e += 32)
     {
         const int idx = list[warp][e];
-        if (OP == 0) encode_parent<T, MW, true>(hr, sc, L, level, idx, eps, done);
-        else if (OP == 1) encode_parent<T, MW, false>(hr, sc, L, level, idx, eps, done);
-        else decode_parent<T, MW, false>(hr, sc, L, level, idx, eps, done);
+        if (OP == 0) encode_parent<T, MW, true, PM>(hr, sc, L, level, idx, eps, done, pm);
+        else if (OP == 1) encode_parent<T, MW, false, PM>(hr, sc, L, level, idx, eps, done, pm);
+        else decode_parent<T, MW, false, PM>(hr, sc, L, level, idx, eps, done, pm);
     }
     const unsigned tot = __reduce_add_sync(0xffffffffu, done);
     if (lane == 0 && tot)

@@ -14,6 +14,7 @@
 #include "case_io.hpp"
 #include "init.cuh"
 #include "outputs.cuh"
+#include "proposal_sim.cuh"
 #include "solver.cuh"
 
 #include <algorithm>
@@ -76,6 +77,12 @@ struct SimBase
     virtual mwdg2_status timing(double* out, int n) = 0;
     virtual mwdg2_status set_timing(int mode) = 0;
     virtual mwdg2_status counters(int64_t* out, int n) = 0;
+    // learned refinement proposal
+    virtual mwdg2_status proposal_record(bool on) = 0;
+    virtual mwdg2_status proposal_enable(const float* params, int judge_every, float threshold, float miss_bound) = 0;
+    virtual mwdg2_status proposal_stats(double* out, int n) = 0;
+    virtual mwdg2_status proposal_samples(const void** feats, const uint8_t** labels, int64_t* n, int* device) = 0;
+    virtual mwdg2_status proposal_samples_host(float* feats, uint8_t* labels, int64_t cap, int64_t* n) = 0;
 };
 
 template <typename T> class Sim final : public SimBase
@@ -105,6 +112,11 @@ public:
     mwdg2_status timing(double* out, int n) override;
     mwdg2_status set_timing(int mode) override;
     mwdg2_status counters(int64_t* out, int n) override;
+    mwdg2_status proposal_record(bool on) override;
+    mwdg2_status proposal_enable(const float* params, int judge_every, float threshold, float miss_bound) override;
+    mwdg2_status proposal_stats(double* out, int n) override;
+    mwdg2_status proposal_samples(const void** feats, const uint8_t** labels, int64_t* n, int* device) override;
+    mwdg2_status proposal_samples_host(float* feats, uint8_t* labels, int64_t cap, int64_t* n) override;
 
 private:
     mwio::Case<T> cs_;
@@ -166,7 +178,8 @@ private:
     int variant_key() const
     {
         int key = (mw_ && use_list(1) ? 1 : 0) | (mw_ && use_list(2) ? 2 : 0) | (timed_ ? 1 << 24 : 0) |
-                  (!mw_ && flip_ ? 1 << 23 : 0);
+                  (!mw_ && flip_ ? 1 << 23 : 0) | (prop_rec_ ? 1 << 22 : 0) | (prop_learned_ ? 1 << 21 : 0) |
+                  (prop_apply_ ? 1 << 20 : 0);
         for (int level = mw::kBandMaxLevel + 1; level < L_; ++level)
             if (sparse_level(level)) key |= 4 << (level - mw::kBandMaxLevel - 1);
         return key;
@@ -194,6 +207,25 @@ private:
     double last_ms_[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     int64_t last_cnt_[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     int launches_ = 0;
+    // learned refinement proposal (csrc/proposal_sim.cuh): record features and activity labels
+    // (prop_rec_), propose the subtrees the encode and decode visit (prop_learned_); every
+    // judge_every_-th step runs in full as the judge, and a step whose active subtrees the
+    // proposal missed beyond miss_bound_ makes the next judge_every_ steps run in full
+    bool prop_rec_ = false, prop_learned_ = false, prop_apply_ = false, prop_judge_ = false;
+    int prop_C_ = 0;
+    int64_t prop_nC_ = 0;
+    __nv_bfloat16* d_feat_ = nullptr;   // [4^C][128] features of the step's start
+    uint8_t* d_lab_ = nullptr;          // [4^C] activity bits of the children in the last step
+    uint8_t* d_act_ = nullptr;          // [4^(C+1)] activity marks of this step
+    uint8_t* d_prop_ = nullptr;         // [4^(C+1)] proposal of this step
+    float* d_mlp_ = nullptr;            // MLP parameters
+    int* d_mlp_err_ = nullptr;
+    float prop_thr_ = 0.0f, prop_bound_ = 0.0f;
+    int prop_judge_every_ = 0, prop_since_judge_ = 0, prop_fallback_left_ = 0;
+    int64_t prop_learned_steps_ = 0, prop_judge_steps_ = 0, prop_fallbacks_ = 0;
+    double prop_last_[4] = {0, 0, 0, 0};      // active, missed, proposed, applied (last step)
+    double prop_judge_rate_ = 0.0;            // missed / active at the last judge step
+    mwdg2_status prop_alloc();
     // outputs
     std::chrono::steady_clock::time_point t_start_;
     double time_mra_ = 0, time_solver_ = 0;
@@ -252,22 +284,34 @@ private:
     {
         return level - 1 > mw::kBandMaxLevel && level <= L_ - 1 && sparse_level(level) && !sparse_level(level - 1);
     }
+    // The proposal's mask of this step's encode / decode (prop_on_: the proposal records or
+    // applies; the masked kernels are used on the levels at and below its level C + 1).
+    bool prop_on() const { return prop_rec_ || prop_learned_; }
+    mw::PropMask prop_mask(bool record) const
+    {
+        return mw::PropMask{prop_apply_ ? d_prop_ : nullptr, record ? d_act_ : nullptr, prop_C_ + 1};
+    }
     template <bool FULL> void encode_tree(const mw::Hier<T>& h, T eps)
     {
+        const mw::PropMask pm = prop_mask(FULL);
         for (int level = L_ - 1; level > mw::kBandMaxLevel; --level)
         {
             if (folded_below(level)) continue;
             const bool fold = folded_below(level + 1);
+            const bool pmk = prop_on() && level + (fold ? 1 : 0) >= pm.level;
             if (sparse_level(level))
             {
                 const int nb = grid_for(((int64_t)1 << (2 * level)) / 8, 256, 1 << 30);
-                if (mw_) mw::k_level_sparse<T, true, FULL ? 0 : 1><<<nb, 256, 0, st_>>>(h, sc_, L_, level, eps);
+                if (pmk) mw::k_level_sparse<T, true, FULL ? 0 : 1, true><<<nb, 256, 0, st_>>>(h, sc_, L_, level, eps, pm);
+                else if (mw_) mw::k_level_sparse<T, true, FULL ? 0 : 1><<<nb, 256, 0, st_>>>(h, sc_, L_, level, eps);
                 else mw::k_level_sparse<T, false, FULL ? 0 : 1><<<nb, 256, 0, st_>>>(h, sc_, L_, level, eps);
             }
             else
             {
                 const int nb = grid_for((int64_t)1 << (2 * level), 256, 1 << 30);
-                if (mw_ && fold) mw::k_encode_level<T, true, FULL, true><<<nb, 256, 0, st_>>>(h, sc_, L_, level, eps);
+                if (pmk && fold) mw::k_encode_level<T, true, FULL, true, true><<<nb, 256, 0, st_>>>(h, sc_, L_, level, eps, pm);
+                else if (pmk) mw::k_encode_level<T, true, FULL, false, true><<<nb, 256, 0, st_>>>(h, sc_, L_, level, eps, pm);
+                else if (mw_ && fold) mw::k_encode_level<T, true, FULL, true><<<nb, 256, 0, st_>>>(h, sc_, L_, level, eps);
                 else if (mw_) mw::k_encode_level<T, true, FULL><<<nb, 256, 0, st_>>>(h, sc_, L_, level, eps);
                 else if (fold) mw::k_encode_level<T, false, FULL, true><<<nb, 256, 0, st_>>>(h, sc_, L_, level, eps);
                 else mw::k_encode_level<T, false, FULL><<<nb, 256, 0, st_>>>(h, sc_, L_, level, eps);
@@ -634,6 +678,22 @@ template <typename T> mwdg2_status Sim<T>::enqueue_device()
     }
     rec(1);
     const bool remesh = (eps > T(0) || first_);
+    if (prop_on() && remesh)
+    {
+        // features of the step's start; the MLP's proposal (applied or, on judge and fallback
+        // steps, only scored against the step's activity)
+        const int grid = grid_for(prop_nC_, 128, 148 * 16);
+        mw::k_prop_features<T><<<grid, 128, 0, st_>>>(hr_, prop_C_, d_lab_, d_feat_);
+        ++launches_;
+        if (prop_learned_)
+        {
+            const int64_t tiles = (prop_nC_ + mlp::kRows - 1) / mlp::kRows;
+            const int g = (int)std::min<int64_t>(tiles, 2 * (int64_t)(solver_blocks_ / 8));
+            mlp::k_mlp_forward<<<g, mlp::kRows, mlp::FwdSmem::Total + 1024, st_>>>(d_mlp_, d_feat_, prop_nC_, nullptr, d_prop_,
+                                                                                 prop_thr_, d_mlp_err_);
+            ++launches_;
+        }
+    }
     if (remesh) encode_tree<true>(hr_, eps);
     rec(2);
     if (remesh)
@@ -664,18 +724,22 @@ template <typename T> mwdg2_status Sim<T>::enqueue_device()
             CU(cudaStreamWaitEvent(st_dec_, ev_dec_fork_, 0));
             // (no folding here: a thread decoding a child after its parent lengthens the
             // kernel's tail, while the sparse level's own kernel overlaps the topology)
+            const mw::PropMask pm = prop_mask(false);
             for (int level = mw::kBandMaxLevel + 1; level < L_; ++level)
             {
+                const bool pmk = prop_on() && level >= pm.level;
                 if (sparse_level(level))
                 {
                     const int nb = grid_for(((int64_t)1 << (2 * level)) / 8, 256, 1 << 30);
-                    if (mw) mw::k_level_sparse<T, true, 2><<<nb, 256, 0, st_dec_>>>(hr_, sc_, L_, level, eps);
+                    if (pmk) mw::k_level_sparse<T, true, 2, true><<<nb, 256, 0, st_dec_>>>(hr_, sc_, L_, level, eps, pm);
+                    else if (mw) mw::k_level_sparse<T, true, 2><<<nb, 256, 0, st_dec_>>>(hr_, sc_, L_, level, eps);
                     else mw::k_level_sparse<T, false, 2><<<nb, 256, 0, st_dec_>>>(hr_, sc_, L_, level, eps);
                 }
                 else
                 {
                     const int nb = grid_for((int64_t)1 << (2 * level), 256, 1 << 30);
-                    if (mw) mw::k_decode_level<T, true><<<nb, 256, 0, st_dec_>>>(hr_, sc_, L_, level, eps);
+                    if (pmk) mw::k_decode_level<T, true, true><<<nb, 256, 0, st_dec_>>>(hr_, sc_, L_, level, eps, pm);
+                    else if (mw) mw::k_decode_level<T, true><<<nb, 256, 0, st_dec_>>>(hr_, sc_, L_, level, eps);
                     else mw::k_decode_level<T, false><<<nb, 256, 0, st_dec_>>>(hr_, sc_, L_, level, eps);
                 }
                 ++launches_;
@@ -714,6 +778,12 @@ template <typename T> mwdg2_status Sim<T>::enqueue_device()
         rec(6);
         stage<2>(hs_, hr_, false);
         rec(7);
+    }
+    if (prop_on() && remesh)
+    {
+        mw::k_prop_labels<<<grid_for(prop_nC_, 256, 148 * 8), 256, 0, st_>>>(d_act_, prop_learned_ ? d_prop_ : nullptr,
+                                                                           d_lab_, prop_nC_, &sc_->prop_active);
+        ++launches_;
     }
     // the stage points of the new state come back with the step's scalars
     const int np = (int)cs_.stage_codes.size();
@@ -775,6 +845,9 @@ template <typename T> mwdg2_status Sim<T>::begin_step()
         return MWDG2_DONE;
     }
     CU(cudaSetDevice(device_));
+    // the proposal: a judge step every prop_judge_every_ steps, full steps while a fallback lasts
+    prop_judge_ = prop_learned_ && !first_ && prop_judge_every_ > 0 && prop_since_judge_ >= prop_judge_every_;
+    prop_apply_ = prop_learned_ && !first_ && !prop_judge_ && prop_fallback_left_ == 0;
     // run_simulation.cu:228-235
     time_ += dt_;
     if ((time_ - cs_.sim_time) > T(0))
@@ -805,12 +878,141 @@ template <typename T> mwdg2_status Sim<T>::finish_step(double* dt_out, int64_t* 
     CU(cudaSetDevice(device_));
     if (mwdg2_status s = collect_step()) return s;
     if (sc_host_->status & 1) return set_err(MWDG2_ERR_NUMERIC, "NaN in the leaf state");
+    if (prop_on())
+    {
+        int mlp_err = 0;
+        if (prop_learned_) CU(cudaMemcpy(&mlp_err, d_mlp_err_, sizeof(int), cudaMemcpyDeviceToHost));
+        if (mlp_err) return set_err(MWDG2_ERR_TIMEOUT, "proposal MLP: a tensor-core wait ran out");
+        const double active = sc_host_->prop_active, missed = sc_host_->prop_missed;
+        prop_last_[0] = active;
+        prop_last_[1] = missed;
+        prop_last_[2] = sc_host_->prop_proposed;
+        prop_last_[3] = prop_apply_ ? 1.0 : 0.0;
+        if (prop_learned_ && !first_)
+        {
+            const double rate = active > 0 ? missed / active : 0.0;
+            ++prop_since_judge_;
+            if (prop_judge_)
+            {
+                ++prop_judge_steps_;
+                prop_judge_rate_ = rate;
+                prop_since_judge_ = 0;
+            }
+            else if (prop_apply_) ++prop_learned_steps_;
+            else if (prop_fallback_left_ > 0) --prop_fallback_left_;
+            if ((prop_judge_ || prop_apply_) && rate > prop_bound_)
+            {
+                prop_fallback_left_ = prop_judge_every_ > 0 ? prop_judge_every_ : 1;
+                ++prop_fallbacks_;
+            }
+        }
+    }
     n_leaves_ = sc_host_->n_leaves;
     dt_ = sc_host_->dt_min;
     first_ = false;
     timestep_++;
     if (dt_out) *dt_out = (double)dt_;
     if (n_out) *n_out = n_leaves_;
+    return MWDG2_OK;
+}
+
+template <typename T> mwdg2_status Sim<T>::prop_alloc()
+{
+    if (!mw_) return set_err(MWDG2_ERR_STATE, "the refinement proposal applies to MWDG2 only");
+    if (L_ < 4) return set_err(MWDG2_ERR_STATE, "the refinement proposal needs max_ref_lvl >= 4");
+    if (d_feat_) return MWDG2_OK;
+    prop_C_ = mw::proposal_level(L_);
+    prop_nC_ = (int64_t)1 << (2 * prop_C_);
+    if (mwdg2_status s = dalloc(d_feat_, (size_t)prop_nC_ * mlp::kIn)) return s;
+    if (mwdg2_status s = dalloc(d_lab_, (size_t)prop_nC_)) return s;
+    if (mwdg2_status s = dalloc(d_act_, (size_t)prop_nC_ * 4)) return s;
+    if (mwdg2_status s = dalloc(d_prop_, (size_t)prop_nC_ * 4)) return s;
+    if (mwdg2_status s = dalloc(d_mlp_, mlp::kParams)) return s;
+    if (mwdg2_status s = dalloc(d_mlp_err_, 1)) return s;
+    CU(cudaMemset(d_lab_, 0, (size_t)prop_nC_));
+    CU(cudaMemset(d_act_, 0, (size_t)prop_nC_ * 4));
+    CU(cudaMemset(d_prop_, 1, (size_t)prop_nC_ * 4));
+    CU(cudaMemset(d_mlp_err_, 0, sizeof(int)));
+    CU(cudaFuncSetAttribute(mlp::k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)(mlp::FwdSmem::Total + 1024)));
+    return MWDG2_OK;
+}
+
+template <typename T> mwdg2_status Sim<T>::proposal_record(bool on)
+{
+    CU(cudaSetDevice(device_));
+    if (on) { if (mwdg2_status s = prop_alloc()) return s; }
+    prop_rec_ = on;
+    P_.act = prop_on() ? d_act_ : nullptr;
+    P_.act_level = prop_C_ + 1;
+    for (auto& g : graphs_) cudaGraphExecDestroy(g.second.exec);   // they hold the old parameters
+    graphs_.clear();
+    return MWDG2_OK;
+}
+
+template <typename T>
+mwdg2_status Sim<T>::proposal_enable(const float* params, int judge_every, float threshold, float miss_bound)
+{
+    CU(cudaSetDevice(device_));
+    if (!params)
+    {
+        prop_learned_ = false;
+        return proposal_record(prop_rec_);
+    }
+    if (L_ < 11) return set_err(MWDG2_ERR_STATE, "the refinement proposal acts on max_ref_lvl >= 11 (levels 10 and up)");
+    if (mwdg2_status s = prop_alloc()) return s;
+    CU(cudaMemcpy(d_mlp_, params, sizeof(float) * mlp::kParams, cudaMemcpyHostToDevice));
+    prop_learned_ = true;
+    prop_judge_every_ = judge_every;
+    prop_thr_ = threshold;
+    prop_bound_ = miss_bound;
+    prop_since_judge_ = 0;
+    prop_fallback_left_ = 0;
+    return proposal_record(prop_rec_);
+}
+
+template <typename T> mwdg2_status Sim<T>::proposal_stats(double* out, int n)
+{
+    const double nodes = (double)(prop_nC_ * 4);
+    const double v[10] = {prop_last_[0], prop_last_[1], prop_last_[2], prop_last_[3], nodes, (double)prop_learned_steps_,
+                          (double)prop_judge_steps_, prop_judge_rate_, (double)prop_fallbacks_, (double)prop_fallback_left_};
+    for (int i = 0; i < n && i < 10; ++i) out[i] = v[i];
+    return MWDG2_OK;
+}
+
+template <typename T>
+mwdg2_status Sim<T>::proposal_samples(const void** feats, const uint8_t** labels, int64_t* n, int* device)
+{
+    if (!prop_on() || first_) return set_err(MWDG2_ERR_STATE, "no step recorded proposal features yet");
+    CU(cudaSetDevice(device_));
+    CU(cudaStreamSynchronize(st_));
+    *feats = d_feat_;
+    *labels = d_lab_;
+    *n = prop_nC_;
+    *device = device_;
+    return MWDG2_OK;
+}
+
+template <typename T> mwdg2_status Sim<T>::proposal_samples_host(float* feats, uint8_t* labels, int64_t cap, int64_t* n)
+{
+    const void* df = nullptr;
+    const uint8_t* dl = nullptr;
+    int64_t m = 0;
+    int dev = 0;
+    if (mwdg2_status s = proposal_samples(&df, &dl, &m, &dev)) return s;
+    if (n) *n = m;
+    if (cap < m) return set_err(MWDG2_ERR_ARG, "capacity below the number of coarse cells");
+    if (feats)
+    {
+        std::vector<uint16_t> h((size_t)m * mlp::kIn);
+        CU(cudaMemcpy(h.data(), df, h.size() * 2, cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < h.size(); ++i)
+        {
+            const uint32_t u = (uint32_t)h[i] << 16;
+            std::memcpy(feats + i, &u, 4);
+        }
+    }
+    if (labels) CU(cudaMemcpy(labels, dl, (size_t)m, cudaMemcpyDeviceToHost));
     return MWDG2_OK;
 }
 
@@ -1277,6 +1479,9 @@ template <typename T> mwdg2_status Sim<T>::counters(int64_t* out, int n)
 // Internal: lets other translation units of the library set the mwdg2_last_error text.
 void mwdg2_detail_set_last_error(const char* msg) { g_last_error = msg ? msg : ""; }
 
+mwdg2_status mwdg2_detail_proposal_samples(mwdg2_sim* sim, const void** feats, const uint8_t** labels, int64_t* n,
+                                           int* device);
+
 // ============================================================================ C ABI
 
 struct mwdg2_sim
@@ -1428,6 +1633,31 @@ mwdg2_status mwdg2_last_step_counters(mwdg2_sim* s, int64_t* out, int n)
 
 void mwdg2_destroy(mwdg2_sim* s) { delete s; }
 
+mwdg2_status mwdg2_proposal_record(mwdg2_sim* s, int on)
+{
+    if (!s) return set_err(MWDG2_ERR_ARG, "null handle");
+    return s->impl->proposal_record(on != 0);
+}
+
+mwdg2_status mwdg2_proposal_enable(mwdg2_sim* s, const float* params, int judge_every, float threshold, float miss_bound)
+{
+    if (!s) return set_err(MWDG2_ERR_ARG, "null handle");
+    if (judge_every < 0 || !(miss_bound >= 0.0f)) return set_err(MWDG2_ERR_ARG, "judge_every >= 0 and miss_bound >= 0");
+    return s->impl->proposal_enable(params, judge_every, threshold, miss_bound);
+}
+
+mwdg2_status mwdg2_proposal_samples(mwdg2_sim* s, float* feats, uint8_t* labels, int64_t cap, int64_t* n)
+{
+    if (!s) return set_err(MWDG2_ERR_ARG, "null handle");
+    return s->impl->proposal_samples_host(feats, labels, cap, n);
+}
+
+mwdg2_status mwdg2_proposal_stats(mwdg2_sim* s, double* out, int n)
+{
+    if (!s || !out) return set_err(MWDG2_ERR_ARG, "null argument");
+    return s->impl->proposal_stats(out, n);
+}
+
 mwdg2_status mwdg2_batch_create(int n, const char* const* par_paths, const mwdg2_opts* opts, mwdg2_batch** out)
 {
     if (!out || !par_paths || n < 1) return set_err(MWDG2_ERR_ARG, "mwdg2_batch_create: need n >= 1 paths and an output");
@@ -1573,3 +1803,9 @@ mwdg2_status mwdg2_run_simulation(int argc, char** argv)
 }
 
 } // extern "C"
+
+mwdg2_status mwdg2_detail_proposal_samples(mwdg2_sim* sim, const void** feats, const uint8_t** labels, int64_t* n,
+                                           int* device)
+{
+    return sim->impl->proposal_samples(feats, labels, n, device);
+}

@@ -632,6 +632,8 @@ __global__ void __launch_bounds__(kSolverThreads, sizeof(T) == 4 ? 5 : 2) k_mwdg
         T leaf_dt = P.initial_tstep;
         if (wet && geo.in_extent)
         {
+            // the leaf changes: the encode of the next step revisits its subtree
+            if (P.act && level >= P.act_level) P.act[(a - lvl_idx(level)) >> (2 * (level - P.act_level))] = 1;
             T u[9];
             dg2_rhs_update(P3<T>{own.h[0], own.h[1], own.h[2]}, P3<T>{own.qx[0], own.qx[1], own.qx[2]},
                            P3<T>{own.qy[0], own.qy[1], own.qy[2]}, P3<T>{own.z[0], own.z[1], own.z[2]}, nf, geo.dxl, P, dt, u);

@@ -87,6 +87,23 @@ def lib():
         L.mwdg2_batch_run.argtypes = [vp, ctypes.c_int64, i64p, i64p, i64p]
         L.mwdg2_batch_member.argtypes = [vp, ctypes.c_int, ctypes.POINTER(vp)]
         L.mwdg2_batch_destroy.argtypes = [vp]
+        fp = ctypes.POINTER(ctypes.c_float)
+        L.mwdg2_mlp_forward.argtypes = [fp, fp, ctypes.c_int, ctypes.c_int64, ctypes.c_float, fp, u8p]
+        L.mwdg2_mlp_grad.argtypes = [fp, fp, ctypes.c_int, u8p, ctypes.c_int64, ctypes.c_float, fp, fp]
+        L.mwdg2_trainer_create.argtypes = [fp, ctypes.c_float, ctypes.c_int, ctypes.POINTER(vp)]
+        L.mwdg2_trainer_step.argtypes = [vp, fp, ctypes.c_int, u8p, ctypes.c_int64, ctypes.c_float, fp]
+        L.mwdg2_trainer_observe.argtypes = [vp, vp, ctypes.c_float, fp]
+        L.mwdg2_trainer_params.argtypes = [vp, fp]
+        L.mwdg2_trainer_destroy.argtypes = [vp]
+        L.mwdg2_proposal_record.argtypes = [vp, ctypes.c_int]
+        L.mwdg2_proposal_enable.argtypes = [vp, fp, ctypes.c_int, ctypes.c_float, ctypes.c_float]
+        L.mwdg2_proposal_stats.argtypes = [vp, dp, ctypes.c_int]
+        L.mwdg2_proposal_samples.argtypes = [vp, fp, u8p, ctypes.c_int64, i64p]
+        L.mwdg2_proposal_samples.restype = ctypes.c_int
+        for name in ("mwdg2_mlp_forward", "mwdg2_mlp_grad", "mwdg2_trainer_create", "mwdg2_trainer_step",
+                     "mwdg2_trainer_observe", "mwdg2_trainer_params", "mwdg2_proposal_record", "mwdg2_proposal_enable",
+                     "mwdg2_proposal_stats"):
+            getattr(L, name).restype = ctypes.c_int
         for name in ("mwdg2_create", "mwdg2_step", "mwdg2_run", "mwdg2_run_simulation", "mwdg2_info",
                      "mwdg2_get_leaves", "mwdg2_get_state", "mwdg2_get_sig", "mwdg2_get_hierarchy",
                      "mwdg2_read_stage", "mwdg2_last_step_timing", "mwdg2_set_timing", "mwdg2_last_step_counters",
@@ -234,6 +251,36 @@ class Simulation:
         _check(lib().mwdg2_last_step_timing(self._h, _p(out, ctypes.c_double), 8))
         return out
 
+    def proposal_record(self, on: bool = True):
+        """Record the proposal's features (step start) and activity labels (step end)."""
+        _check(lib().mwdg2_proposal_record(self._h, 1 if on else 0))
+
+    def proposal_enable(self, params, judge_every: int = 20, threshold: float = 0.0, miss_bound: float = 0.01):
+        """Let the MLP with `params` choose the subtrees the encode and decode visit (None: off)."""
+        if params is None:
+            _check(lib().mwdg2_proposal_enable(self._h, None, 0, 0.0, 0.0))
+            return
+        p = np.ascontiguousarray(params, np.float32)
+        self._prop_params = p
+        _check(lib().mwdg2_proposal_enable(self._h, _p(p, ctypes.c_float), judge_every, threshold, miss_bound))
+
+    def proposal_samples(self) -> tuple[np.ndarray, np.ndarray]:
+        """Features [n][128] and labels [n] of the last recorded step (n coarse cells)."""
+        n = ctypes.c_int64()
+        lib().mwdg2_proposal_samples(self._h, None, None, 0, ctypes.byref(n))
+        feats = np.zeros((n.value, 128), np.float32)
+        labels = np.zeros(n.value, np.uint8)
+        _check(lib().mwdg2_proposal_samples(self._h, _p(feats, ctypes.c_float), _p(labels, ctypes.c_uint8), n.value,
+                                            ctypes.byref(n)))
+        return feats, labels
+
+    def proposal_stats(self) -> dict:
+        a = np.zeros(10)
+        _check(lib().mwdg2_proposal_stats(self._h, _p(a, ctypes.c_double), 10))
+        keys = ("active", "missed", "proposed", "applied", "subtrees", "learned_steps", "judge_steps", "judge_miss_rate",
+                "fallbacks", "fallback_left")
+        return dict(zip(keys, a.tolist()))
+
     def last_step_counters(self) -> dict:
         out = np.zeros(10, np.int64)
         _check(lib().mwdg2_last_step_counters(self._h, _p(out, ctypes.c_int64), 10))
@@ -302,6 +349,88 @@ class Batch:
 
     def __exit__(self, *a):
         self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------- learned refinement proposal
+MLP_PARAMS = 16836
+MLP_FEATURES = 113
+
+
+def mlp_init(seed: int = 0) -> np.ndarray:
+    """He-initialised parameter block (W1[64][128] b1 W2[64][64] b2 W3[64][64] b3 W4[4][64] b4)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    parts = []
+    for fan_out, fan_in in ((64, 128), (64, 64), (64, 64), (4, 64)):
+        parts.append(rng.normal(0.0, np.sqrt(2.0 / fan_in), size=fan_out * fan_in))
+        parts.append(np.zeros(fan_out))
+    p = np.concatenate(parts).astype(np.float32)
+    assert p.size == MLP_PARAMS
+    return p
+
+
+def mlp_forward(params: np.ndarray, feats: np.ndarray, threshold: float = 0.0) -> tuple[np.ndarray, np.ndarray]:
+    """Logits [n][4] and proposal bits [n][4] (logit > threshold) of the tensor-core MLP."""
+    params = np.ascontiguousarray(params, np.float32)
+    feats = np.ascontiguousarray(feats, np.float32)
+    n, nf = feats.shape
+    logits = np.zeros((n, 4), np.float32)
+    prop = np.zeros((n, 4), np.uint8)
+    fp = ctypes.POINTER(ctypes.c_float)
+    _check(lib().mwdg2_mlp_forward(_p(params, ctypes.c_float), _p(feats, ctypes.c_float), nf, n, threshold,
+                                   _p(logits, ctypes.c_float), _p(prop, ctypes.c_uint8)))
+    return logits, prop
+
+
+def mlp_grad(params: np.ndarray, feats: np.ndarray, labels: np.ndarray, pos_weight: float = 1.0):
+    """Gradient of the weighted logistic loss and the loss, from the tensor-core training kernel."""
+    params = np.ascontiguousarray(params, np.float32)
+    feats = np.ascontiguousarray(feats, np.float32)
+    labels = np.ascontiguousarray(labels, np.uint8)
+    n, nf = feats.shape
+    grad = np.zeros(MLP_PARAMS, np.float32)
+    loss = np.zeros(1, np.float32)
+    _check(lib().mwdg2_mlp_grad(_p(params, ctypes.c_float), _p(feats, ctypes.c_float), nf, _p(labels, ctypes.c_uint8), n,
+                                pos_weight, _p(grad, ctypes.c_float), _p(loss, ctypes.c_float)))
+    return grad, float(loss[0])
+
+
+class Trainer:
+    """Adam on the device for the proposal MLP."""
+
+    def __init__(self, params: np.ndarray, lr: float = 1e-3, device: int = -1):
+        params = np.ascontiguousarray(params, np.float32)
+        h = ctypes.c_void_p()
+        _check(lib().mwdg2_trainer_create(_p(params, ctypes.c_float), lr, device, ctypes.byref(h)))
+        self._h = h
+
+    def step(self, feats: np.ndarray, labels: np.ndarray, pos_weight: float = 1.0) -> float:
+        feats = np.ascontiguousarray(feats, np.float32)
+        labels = np.ascontiguousarray(labels, np.uint8)
+        loss = ctypes.c_float()
+        _check(lib().mwdg2_trainer_step(self._h, _p(feats, ctypes.c_float), feats.shape[1], _p(labels, ctypes.c_uint8),
+                                        feats.shape[0], pos_weight, ctypes.byref(loss)))
+        return loss.value
+
+    def observe(self, sim: "Simulation", pos_weight: float = 1.0) -> float:
+        loss = ctypes.c_float()
+        _check(lib().mwdg2_trainer_observe(self._h, sim._h, pos_weight, ctypes.byref(loss)))
+        return loss.value
+
+    def params(self) -> np.ndarray:
+        out = np.zeros(MLP_PARAMS, np.float32)
+        _check(lib().mwdg2_trainer_params(self._h, _p(out, ctypes.c_float)))
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().mwdg2_trainer_destroy(self._h)
+            self._h = None
 
     def __del__(self):
         try:

@@ -206,6 +206,69 @@ mwdg2_status mwdg2_leaf_topology_static(const uint8_t* d_sig, int max_ref_lvl, i
                                         uint8_t* d_nb_levels, int64_t cap, int64_t* n_leaves_out,
                                         void* stream);
 
+
+/* ---------------------------------------------------------------- learned refinement proposal
+ * No counterpart in the reference (which encodes every previously significant parent and
+ * decodes every significant one each step, source/mra/encode_flow.cu:14-92,
+ * source/mra/decoding.cu:3-67). A small MLP (128 -> 64 -> 64 -> 64 -> 4, ReLU, BF16 weights and
+ * activations, FP32 accumulation on the tensor cores) proposes, per node of a coarse level C
+ * (max(max_ref_lvl - 3, 9)), which of its four child subtrees the step's encode and decode
+ * visit. Parameters are one FP32 block of MWDG2_MLP_PARAMS values:
+ *   W1[64][128] b1[64] W2[64][64] b2[64] W3[64][64] b3[64] W4[4][64] b4[4]
+ * Features are rows of up to 128 values (MWDG2_MLP_FEATURES used, the rest zero); labels are
+ * one byte per row, bit j = child j active. */
+#define MWDG2_MLP_PARAMS 16836
+#define MWDG2_MLP_FEATURES 113
+
+/* Logits [n][4] (may be NULL) and proposal bytes [n][4] (1 where the logit exceeds
+ * `threshold`; may be NULL) of n feature rows of `nfeat` floats (host arrays). */
+mwdg2_status mwdg2_mlp_forward(const float* params, const float* feats, int nfeat, int64_t n, float threshold,
+                               float* logits, uint8_t* proposal);
+
+/* Gradient [MWDG2_MLP_PARAMS] of the weighted logistic loss
+ * sum over rows and outputs of w (softplus(z) - y z) / n, w = pos_weight where y = 1 else 1,
+ * and that loss (may be NULL), for n rows (host arrays). */
+mwdg2_status mwdg2_mlp_grad(const float* params, const float* feats, int nfeat, const uint8_t* labels, int64_t n,
+                            float pos_weight, float* grad, float* loss);
+
+/* Trainer: FP32 parameters and Adam moments (beta 0.9 / 0.999) on the device. */
+typedef struct mwdg2_trainer mwdg2_trainer;
+mwdg2_status mwdg2_trainer_create(const float* init_params, float lr, int device, mwdg2_trainer** out);
+/* One Adam step on n host rows. */
+mwdg2_status mwdg2_trainer_step(mwdg2_trainer* t, const float* feats, int nfeat, const uint8_t* labels, int64_t n,
+                                float pos_weight, float* loss_out);
+/* One Adam step on the features and labels a simulation recorded on the device for its last
+ * step (mwdg2_proposal_record); every node of the coarse level is one row. */
+mwdg2_status mwdg2_trainer_observe(mwdg2_trainer* t, mwdg2_sim* sim, float pos_weight, float* loss_out);
+mwdg2_status mwdg2_trainer_params(mwdg2_trainer* t, float* out);
+void mwdg2_trainer_destroy(mwdg2_trainer* t);
+
+/* Record, from the next step on, the proposal's features at each step's start and the
+ * activity of each child subtree over the step (its leaves updated by the RK stages or its
+ * significance flags changed by the encode), for mwdg2_trainer_observe. MWDG2 only; results
+ * are unchanged. on = 0 stops recording. */
+mwdg2_status mwdg2_proposal_record(mwdg2_sim* sim, int on);
+
+/* Let the MLP with `params` (MWDG2_MLP_PARAMS floats, copied) choose, from the next step on,
+ * the child subtrees of the coarse level that the encode, decode and scale re-encode visit
+ * (logit > threshold); subtrees left out keep their flags and values. Every judge_every-th
+ * step (0: never) runs in full as the judge; a step whose active subtrees the proposal left
+ * out exceed the fraction miss_bound makes the next judge_every steps run in full. params =
+ * NULL switches the proposal off. MWDG2 with max_ref_lvl >= 11 only (MWDG2_ERR_STATE). */
+mwdg2_status mwdg2_proposal_enable(mwdg2_sim* sim, const float* params, int judge_every, float threshold,
+                                   float miss_bound);
+
+/* The features ([n][128] floats, the BF16 values the MLP reads; may be NULL) and labels ([n]
+ * bytes; may be NULL) the last recorded step left for its n coarse cells (cap: rows the
+ * arrays hold; n is written in any case). */
+mwdg2_status mwdg2_proposal_samples(mwdg2_sim* sim, float* feats, uint8_t* labels, int64_t cap, int64_t* n);
+
+/* [0] active subtrees in the last step, [1] of them left out by the proposal, [2] subtrees
+ * proposed, [3] 1 if the last step applied the proposal, [4] subtrees in all, [5] steps that
+ * applied it, [6] judge steps, [7] missed fraction at the last judge step, [8] fallbacks,
+ * [9] full steps left in the current fallback. n <= 10. */
+mwdg2_status mwdg2_proposal_stats(mwdg2_sim* sim, double* out, int n);
+
 #ifdef __cplusplus
 }
 #endif

@@ -10,8 +10,12 @@
  *   MWDG2_REF_DUMP_DIR    directory for dumps (unset: no array dumps)
  *   MWDG2_REF_DUMP_STEPS  comma separated step numbers, or "all"
  *   MWDG2_REF_STOP_AFTER  stop the process (exit 0) after this many steps
- *   MWDG2_REF_STEPS_CSV   per-step log "step,dt,n_leaves,wall_s" (always written
- *                         when set)
+ *   MWDG2_REF_STEPS_CSV   per-step log "step,dt,n_leaves,wall_s,time" (always written
+ *                         when set; time: simulated time at the end of the step)
+ *   MWDG2_REF_WINDOW_TIME, MWDG2_REF_WINDOW_STEPS
+ *                         when both are set, stop (exit 0) once WINDOW_STEPS steps have
+ *                         ended at or after the first step that ended at a simulated time
+ *                         >= WINDOW_TIME (a timing window later in the run)
  *   MWDG2_REF_DIGEST_DIR  directory for per-step digests (unset: none): every step,
  *                         digest.csv gets one row "step,name,n,hash" per leaf-list,
  *                         neighbour and significance array (hash: below), and at the
@@ -50,6 +54,11 @@ int  g_max_calls  = 0;     // number of get_max_scale_coeffs calls
 bool g_cfg_loaded = false;
 bool g_dump_all   = false;
 int  g_stop_after = -1;
+double g_window_time = -1.0;   // MWDG2_REF_WINDOW_TIME
+int    g_window_steps = 0;     // MWDG2_REF_WINDOW_STEPS
+int    g_window_first = -1;    // first step that ended at or after g_window_time
+double g_sim_time = 0.0;       // simulated time at the end of the last step
+double g_dt_next = 0.001;      // dt of the next step (the reference starts with 0.001)
 std::set<int> g_dump_steps;
 std::string   g_dump_dir;
 FILE*         g_steps_csv = nullptr;
@@ -134,6 +143,9 @@ void load_cfg()
     }
     const char* stop = getenv("MWDG2_REF_STOP_AFTER");
     if (stop) g_stop_after = atoi(stop);
+    const char* wt = getenv("MWDG2_REF_WINDOW_TIME");
+    const char* ws = getenv("MWDG2_REF_WINDOW_STEPS");
+    if (wt && ws) { g_window_time = atof(wt); g_window_steps = atoi(ws); }
     const char* ddir = getenv("MWDG2_REF_DIGEST_DIR");
     if (ddir)
     {
@@ -146,7 +158,7 @@ void load_cfg()
     if (csv)
     {
         g_steps_csv = fopen(csv, "w");
-        if (g_steps_csv) fprintf(g_steps_csv, "step,dt,n_leaves,wall_s\n");
+        if (g_steps_csv) fprintf(g_steps_csv, "step,dt,n_leaves,wall_s,time\n");
     }
 }
 
@@ -352,17 +364,23 @@ real ref_hook_get_dt_CFL
     load_cfg();
     real dt = get_dt_CFL(d_dt_CFL, sol_len);
     g_step_done++;
+    // run_simulation.cu:228-235 advances the clock by the previous step's dt at the start
+    // of each step (the last step is clipped to sim_time, which a timing window never reaches)
+    g_sim_time += g_dt_next;
+    g_dt_next = (double)dt;
     const double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - g_t0).count();
     if (g_steps_csv)
     {
-        fprintf(g_steps_csv, "%d,%.17g,%d,%.9f\n", g_step_done, (double)dt, sol_len, wall);
+        fprintf(g_steps_csv, "%d,%.17g,%d,%.9f,%.9f\n", g_step_done, (double)dt, sol_len, wall, g_sim_time);
     }
+    if (g_window_steps > 0 && g_window_first < 0 && g_sim_time >= g_window_time) g_window_first = g_step_done;
+    const bool window_done = g_window_first > 0 && g_step_done >= g_window_first + g_window_steps;
     if (want(g_step_done))
     {
         dump_dev(g_step_done, "dt_cfl", d_dt_CFL, (size_t)sol_len);
         dump_host(g_step_done, "dt", &dt, 1);
     }
-    if (g_stop_after > 0 && g_step_done >= g_stop_after)
+    if ((g_stop_after > 0 && g_step_done >= g_stop_after) || window_done)
     {
         if (g_steps_csv) fclose(g_steps_csv);
         if (g_digest_csv) fclose(g_digest_csv);

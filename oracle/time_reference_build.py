@@ -24,36 +24,53 @@ ROOT = os.path.dirname(HERE)
 
 
 def time_reference(par: str, precision: int, steps: int, warmup: int, exe: str | None = None,
-                   timeout: float = 1800.0) -> dict:
-    """Runs the reference build on `par` (from its folder) for warmup + steps steps and times
-    steps warmup+1 .. warmup+steps from its per-step log: ms per step, active-cell updates/s
-    and wall seconds per simulated second (the simulated time of a step is the dt the step
-    before it logged)."""
+                   timeout: float = 1800.0, window_time: float | None = None) -> dict:
+    """Runs the reference build on `par` (from its folder) and times `steps` steps after
+    `warmup` untimed ones, from its per-step log: ms per step, active-cell updates/s and
+    wall seconds per simulated second (the simulated time of a step is the dt the step
+    before it logged). The window starts at the beginning of the run, or with
+    `window_time` after the first step that ends at or after that simulated time."""
     work = os.path.dirname(os.path.abspath(par))
     exe = os.path.abspath(exe) if exe else os.path.join(HERE, "_ref", f"gpu-mwdg2-ref-fp{precision}")
     if not os.path.exists(exe):
         raise FileNotFoundError(f"{exe} is missing: build it with `make -C oracle ref`")
     log = os.path.join(work, f"ref_steps_{os.getpid()}.csv")
-    env = dict(os.environ, MWDG2_REF_STOP_AFTER=str(warmup + steps), MWDG2_REF_STEPS_CSV=log)
+    env = dict(os.environ, MWDG2_REF_STEPS_CSV=log)
+    if window_time is None:
+        env["MWDG2_REF_STOP_AFTER"] = str(warmup + steps)
+    else:
+        env["MWDG2_REF_WINDOW_TIME"] = repr(float(window_time))
+        env["MWDG2_REF_WINDOW_STEPS"] = str(warmup + steps)
     r = subprocess.run([exe, os.path.basename(par)], cwd=work, env=env, capture_output=True, text=True,
                        timeout=timeout)
     if r.returncode != 0:
         raise RuntimeError(f"reference build exited {r.returncode}: {r.stderr[-2000:]}")
     rows = list(csv.DictReader(open(log)))
     os.remove(log)
-    if len(rows) < warmup + steps:
-        raise RuntimeError(f"reference build logged {len(rows)} steps, {warmup + steps} wanted")
-    t0 = float(rows[warmup - 1]["wall_s"]) if warmup > 0 else 0.0
-    t1 = float(rows[warmup + steps - 1]["wall_s"])
-    leaves = sum(int(rw["n_leaves"]) for rw in rows[warmup:warmup + steps])
+    first = 0   # rows before the window (row k - 1 is step k)
+    if window_time is not None:
+        hits = [k for k, rw in enumerate(rows) if float(rw.get("time", "-1")) >= window_time]
+        if not hits:
+            raise RuntimeError(f"reference build never reached t = {window_time} s")
+        first = hits[0] + 1
+    if len(rows) < first + warmup + steps:
+        raise RuntimeError(f"reference build logged {len(rows)} steps, {first + warmup + steps} wanted")
+    w0 = first + warmup
+    t0 = float(rows[w0 - 1]["wall_s"]) if w0 > 0 else 0.0
+    t1 = float(rows[w0 + steps - 1]["wall_s"])
+    leaves = sum(int(rw["n_leaves"]) for rw in rows[w0:w0 + steps])
     # step k advances the clock by the dt logged at the end of step k - 1
-    sim = sum(float(rw["dt"]) for rw in rows[max(0, warmup - 1):warmup + steps - 1])
-    return {"impl": "reference CUDA build", "dtype": f"f{precision}", "steps": steps, "warmup": warmup,
-            "ms_per_step": 1e3 * (t1 - t0) / steps, "value": leaves / (t1 - t0), "unit": "cell-updates/s",
-            "leaves_mean": leaves / steps, "sim_seconds": sim,
-            "wall_s_per_sim_s": (t1 - t0) / sim if sim > 0 else None,
-            "timing": "host wall clock between the ends of steps W and W+K (each step ends with a "
-                      "device-to-host copy of dt)"}
+    sim = sum(float(rw["dt"]) for rw in rows[max(0, w0 - 1):w0 + steps - 1])
+    out = {"impl": "reference CUDA build", "dtype": f"f{precision}", "steps": steps, "warmup": warmup,
+           "ms_per_step": 1e3 * (t1 - t0) / steps, "value": leaves / (t1 - t0), "unit": "cell-updates/s",
+           "leaves_mean": leaves / steps, "sim_seconds": sim,
+           "wall_s_per_sim_s": (t1 - t0) / sim if sim > 0 else None,
+           "timing": "host wall clock between the ends of steps W and W+K of the window (each step ends with "
+                     "a device-to-host copy of dt)"}
+    if window_time is not None:
+        out["window"] = {"from_time": window_time, "first_step": w0 + 1,
+                         "time": float(rows[w0]["time"]) if "time" in rows[w0] else None}
+    return out
 
 
 def main():

@@ -1,0 +1,119 @@
+"""The learned refinement proposal inside the time step (MWDG2, max_ref_lvl 11 fBm
+catchment, FP64), through the C ABI:
+
+* recording the features and activity labels leaves every result bit-identical;
+* a proposal that keeps every subtree gives the plain step's results bit for bit (the masked
+  encode, decode and re-encode kernels with an all-ones mask);
+* a proposal that keeps none skips the upper levels' encode and decode, misses the active
+  subtrees, and the fallback then runs full steps (judge every 4 steps, miss bound 5 %);
+* the device-built feature rows equal the NumPy restatement of the feature builder
+  (tests/mlp_ref.py) from the hierarchy, flags and activity bits the previous step left;
+* the trainer takes an Adam step on the features and labels a recorded step left on the
+  device.
+"""
+import numpy as np
+import pytest
+
+import cases
+import mlp_ref
+import mwdg2_b200
+from gpu_util import FIELDS, assert_same_topology
+
+pytestmark = pytest.mark.gpu
+L = 11
+STEPS = 6
+
+
+def _case(tmp_path):
+    n = 1 << L
+    z = cases.fbm_surface(n, 0.8, 20261203, 30.0)
+    h0 = np.maximum(0.0, 10.0 - z)   # valleys filled: many wet leaves from the start
+    return cases.fbm_catchment(str(tmp_path), L=L, start_depth=h0, sim_time=600.0)
+
+
+def _constant_mlp(logit: float) -> np.ndarray:
+    p = np.zeros(mwdg2_b200.MLP_PARAMS, np.float32)
+    p[-4:] = logit
+    return p
+
+
+def _run(par, setup, steps=STEPS):
+    sim = mwdg2_b200.Simulation(par, precision=64)
+    setup(sim)
+    out = []
+    for _ in range(steps):
+        sim.step()
+        out.append((sim.leaves(), sim.sig(), sim.state(), sim.proposal_stats() if setup is not _none else None))
+    sim.close()
+    return out
+
+
+def _none(sim):
+    pass
+
+
+def _same(a, b, what):
+    for s, (x, y) in enumerate(zip(a, b)):
+        assert_same_topology(x[0], y[0], f"{what} step {s + 1}")
+        np.testing.assert_array_equal(x[1], y[1], err_msg=f"{what} step {s + 1}: flags")
+        for f in FIELDS:
+            np.testing.assert_array_equal(x[2][f], y[2][f], err_msg=f"{what} step {s + 1}: {f}")
+
+
+def test_recording_and_all_ones_proposal_change_nothing(tmp_path):
+    c = _case(tmp_path)
+    plain = _run(c.par, _none)
+    rec = _run(c.par, lambda s: s.proposal_record(True))
+    _same(plain, rec, "recording")
+    ones = _run(c.par, lambda s: s.proposal_enable(_constant_mlp(20.0), judge_every=0, threshold=0.0, miss_bound=1.0))
+    _same(plain, ones, "all-ones proposal")
+    st = ones[-1][3]
+    assert st["applied"] == 1.0 and st["proposed"] == st["subtrees"] and st["missed"] == 0
+    assert st["active"] > 0
+
+
+def test_empty_proposal_misses_and_falls_back(tmp_path):
+    c = _case(tmp_path)
+    sim = mwdg2_b200.Simulation(c.par, precision=64)
+    sim.proposal_enable(_constant_mlp(-20.0), judge_every=4, threshold=0.0, miss_bound=0.05)
+    sim.step()                      # the first step always runs in full
+    sim.step()                      # the empty proposal: every active subtree is missed
+    st = sim.proposal_stats()
+    assert st["applied"] == 1.0 and st["proposed"] == 0 and st["missed"] == st["active"] > 0
+    assert st["fallbacks"] == 1 and st["fallback_left"] == 4
+    for _ in range(4):
+        ok, dt, n = sim.step()
+        assert ok and dt > 0
+        assert sim.proposal_stats()["applied"] == 0.0
+    sim.close()
+
+
+def test_trainer_observes_a_recorded_step(tmp_path):
+    c = _case(tmp_path)
+    sim = mwdg2_b200.Simulation(c.par, precision=64)
+    sim.proposal_record(True)
+    sim.step()
+    sim.step()
+    tr = mwdg2_b200.Trainer(mwdg2_b200.mlp_init(2), lr=1e-3)
+    l1 = tr.observe(sim, pos_weight=2.0)
+    l2 = tr.observe(sim, pos_weight=2.0)
+    assert np.isfinite(l1) and np.isfinite(l2) and l2 < l1
+    tr.close()
+    sim.close()
+
+
+def test_features_match_numpy_restatement(tmp_path):
+    c = _case(tmp_path)
+    sim = mwdg2_b200.Simulation(c.par, precision=64)
+    sim.proposal_record(True)
+    for _ in range(3):
+        sim.step()
+    hier = [[sim.hierarchy(f, m) for m in range(3)] for f in range(4)]
+    sig = sim.sig()
+    _, lab_prev = sim.proposal_samples()
+    sim.step()
+    feats, _ = sim.proposal_samples()
+    sim.close()
+    want = mlp_ref.proposal_features(hier, sig, L, lab_prev)
+    np.testing.assert_array_equal(feats[:, :113], want[:, :113].astype(np.float32))
+    assert not np.any(feats[:, 113:])

@@ -33,3 +33,40 @@ def test_reference_timing_uses_the_steps_after_the_warmup(tmp_path):
     assert abs(d["ms_per_step"] - 4.0) < 1e-6
     assert abs(d["leaves_mean"] - 1004.5) < 1e-9
     assert abs(d["value"] - 4018 / 0.016) < 1e-3
+
+
+FAKE_WINDOW = """#!{py}
+import os
+T = float(os.environ["MWDG2_REF_WINDOW_TIME"])
+n = int(os.environ["MWDG2_REF_WINDOW_STEPS"])
+first = None
+with open(os.environ["MWDG2_REF_STEPS_CSV"], "w") as f:
+    f.write("step,dt,n_leaves,wall_s,time\\n")
+    t, s = 0.0, 0
+    while True:
+        s += 1
+        t += 0.5
+        f.write(f"{{s}},0.5,{{100 * s}},{{0.01 * s:.9f}},{{t:.9f}}\\n")
+        if first is None and t >= T:
+            first = s
+        if first is not None and s >= first + n:
+            break
+"""
+
+
+def test_reference_timing_window_later_in_the_run(tmp_path):
+    """A window from simulated time T: the steps after the first one that ends at t >= T,
+    W of them untimed, then K timed."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import time_reference_build
+    exe = tmp_path / "fake_ref"
+    exe.write_text(FAKE_WINDOW.format(py=sys.executable))
+    exe.chmod(exe.stat().st_mode | stat.S_IXUSR)
+    par = tmp_path / "case.par"
+    par.write_text("mwdg2\n")
+    d = time_reference_build.time_reference(str(par), 32, steps=4, warmup=2, exe=str(exe), window_time=10.0)
+    # t = 0.5 s per step: step 20 ends at t = 10; warm-up steps 21, 22; timed steps 23..26
+    assert d["window"]["first_step"] == 23
+    assert abs(d["ms_per_step"] - 10.0) < 1e-6
+    assert abs(d["leaves_mean"] - 2450.0) < 1e-9
+    assert abs(d["wall_s_per_sim_s"] - 0.04 / 2.0) < 1e-9
