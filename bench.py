@@ -47,10 +47,16 @@ def parse():
     ap.add_argument("--cpu-steps", type=int, default=16, help="timed FP64 oracle steps for cpu_baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--case-dir", default=None)
-    ap.add_argument("--workload", default="catchment", choices=["catchment", "urban", "ensemble"],
+    ap.add_argument("--workload", default="catchment", choices=["catchment", "urban", "ensemble", "learned"],
                     help="urban: 8192^2 fBm base with building blocks, lake at rest at 1 m, rising point "
                          "inflow; ensemble: a batch of seeded uneven scenarios (mwdg2_batch_*) against the "
-                         "same members stepped one after another; prints its own line")
+                         "same members stepped one after another; learned: the catchment run to --eval-time "
+                         "plain in FP64 and FP32 and with the learned refinement proposal in FP32; each of "
+                         "the last two prints its own line")
+    ap.add_argument("--eval-time", type=float, default=1800.0, help="learned: simulated seconds of the runs")
+    ap.add_argument("--judge-every", type=int, default=20, help="learned: steps between judge steps")
+    ap.add_argument("--proposal", default=os.path.join(ROOT, "gpu-mwdg2_b200", "proposal_mlp.npz"),
+                    help="learned: trained MLP parameters")
     ap.add_argument("--members", type=int, default=64)
     ap.add_argument("--peak-time", type=float, default=1800.0,
                     help="catchment: a second timing window starting at this simulated time (the hydrograph "
@@ -367,12 +373,123 @@ def peak_window(sim, a, dist) -> dict:
     world = int(os.environ.get("WORLD_SIZE", "1"))
     tot_ms = max_over_ranks(float(sum(ms)), dist, "cuda")
     n_mean = float(np.mean(leaves))
+    # phase breakdown in the window (events between the phases; its first step captures)
+    sim.set_timing("phases")
+    sim.step()
+    ph = []
+    for _ in range(PHASE_STEPS):
+        sim.step()
+        ph.append(sim.last_step_timing().tolist())
+    mean_ph = np.array(ph).mean(axis=0)
     return {"from_time": a.peak_time, "steps_to_reach": advance, "seconds_to_reach": advance_s,
+            "phase_ms_mean": dict(zip(("step_open", "encode", "decode", "topology", "stage1", "reencode", "stage2",
+                                       "step"), [round(float(x), 4) for x in mean_ph])),
             "time_at_window": t_sim0, "value": replica_throughput(world, sum(leaves), tot_ms),
             "ms_per_step": tot_ms / a.steps, "leaves_mean": n_mean,
             "wet_fraction": [float(np.mean([w[k] for w in wet])) / n_mean for k in (0, 1)],
             "wall_s_per_sim_s": (tot_ms / 1e3) / sim_s if sim_s > 0 else None, "sim_seconds": sim_s,
             "timing": "device time of each step (CUDA events on the library's stream), max over ranks"}
+
+
+def finest_depth(sim):
+    """Depth at the centre of every finest cell (Z order) from the leaves' DG2 modes: h0 +
+    sqrt(3) (h1x (2 xu - 1) + h1y (2 yu - 1)) at the cell's local coordinates (xu, yu) in
+    its leaf (output/write_all_raster_maps_dg2.cu evaluates the same basis)."""
+    import numpy as np
+    L = sim.info()["L"]
+    lv, st = sim.leaves(), sim.state()
+    lvl = lv["lvl"].astype(np.int64)
+    first = ((1 << (2 * lvl)) - 1) // 3 + 3
+    code = lv["act"].astype(np.int64) - first
+    span = np.int64(1) << (2 * (L - lvl))
+    rep = np.repeat(np.arange(lvl.size), span)
+    fz = np.arange(1 << (2 * L), dtype=np.int64)
+
+    def compact(v):
+        v = v & 0x55555555
+        v = (v | (v >> 1)) & 0x33333333
+        v = (v | (v >> 2)) & 0x0F0F0F0F
+        v = (v | (v >> 4)) & 0x00FF00FF
+        return (v | (v >> 8)) & 0x0000FFFF
+    side = (np.int64(1) << (L - lvl))[rep].astype(np.float64)
+    x0 = compact(code << (2 * (L - lvl)))[rep]
+    y0 = compact((code << (2 * (L - lvl))) >> 1)[rep]
+    xu = (compact(fz) - x0 + 0.5) / side
+    yu = (compact(fz >> 1) - y0 + 0.5) / side
+    s3 = np.sqrt(3.0)
+    return st["h0"][rep] + st["h1x"][rep] * s3 * (2 * xu - 1) + st["h1y"][rep] * s3 * (2 * yu - 1)
+
+
+def run_learned(a):
+    """The learned refinement proposal on the 4096^2 catchment: the same
+    case run from t = 0 to --eval-time three times on this GPU -- plain in FP64 (the depth
+    reference), plain in FP32, and in FP32 with the trained MLP proposing the subtrees the
+    encode and decode visit, a full judge step every --judge-every steps. Each run's device
+    time is the sum of its steps' CUDA-event times (input resident, no host copies); the
+    depth error is the largest difference, over every finest cell, of the depth at the cell
+    centre from the FP64 run's at the same simulated time (each run ends exactly at
+    --eval-time). Prints one line for the plain FP32 run and one for the learned run."""
+    import numpy as np
+    import torch
+    import cases
+    import mwdg2_b200
+    torch.cuda.set_device(0)
+    base = a.case_dir or os.path.join(tempfile.gettempdir(), "mwdg2_bench_cases")
+    d = os.path.join(base, f"learned-{a.level}-{a.eval_time:g}-v1")
+    par = os.path.join(d, "case.par")
+    if not os.path.exists(os.path.join(d, "READY")):
+        os.makedirs(d, exist_ok=True)
+        cases.fbm_catchment(d, L=a.level, sim_time=a.eval_time)
+        open(os.path.join(d, "READY"), "w").close()
+    z = np.load(a.proposal)
+    params = z["params"]
+    train = json.loads(str(z["summary"]))
+
+    def run(precision, learned):
+        sim = mwdg2_b200.Simulation(par, precision=precision, timing="step")
+        if learned:
+            sim.proposal_enable(params, judge_every=a.judge_every, threshold=train["threshold"], miss_bound=0.02)
+        ms, leaves, steps, applied = 0.0, 0, 0, 0
+        while True:
+            ok, dt, n = sim.step()
+            if not ok:
+                break
+            ms += float(sim.last_step_timing()[7])
+            leaves += n
+            steps += 1
+            if learned:
+                applied += int(sim.proposal_stats()["applied"])
+        out = {"ms": ms, "leaves": leaves, "steps": steps, "time": sim.info()["time"], "depth": finest_depth(sim)}
+        if learned:
+            out["stats"] = sim.proposal_stats()
+            out["applied_steps"] = applied
+        sim.close()
+        return out
+
+    ref = run(64, False)
+    plain = run(32, False)
+    learned = run(32, True)
+    peak, peak_kind = peaks()
+    lines = []
+    for name, r in (("plain", plain), ("learned", learned)):
+        err = float(np.max(np.abs(r["depth"] - ref["depth"])))
+        line = {"metric": METRIC + f" ({name} FP32 vs plain FP64 depth)", "value": r["leaves"] / (r["ms"] / 1e3),
+                "unit": UNIT, "n_gpus": 1, "steps": r["steps"], "warmup": 0, "ms_per_step": r["ms"] / r["steps"],
+                "higher_is_better": True, "impl": f"ours-{name}", "dtype": "f32",
+                "data": "synthetic (seeded fBm DEM, no network)",
+                "config": {"workload": f"fBm catchment {1 << a.level}^2 (max_ref_lvl {a.level}) run from t = 0 to "
+                                       f"{a.eval_time:g} s (the hydrograph peak), MWDG2 FP32",
+                           "proposal": "none" if name == "plain" else
+                                       f"trained MLP ({a.proposal.split('/')[-1]}), judge every {a.judge_every} steps",
+                           "depth_reference": "the same case in FP64, plain"},
+                "max_depth_error_m": err, "time": r["time"], "reference_time": ref["time"],
+                "timing": "sum of CUDA-event device times of every step of the run"}
+        if name == "learned":
+            line["vs_plain"] = line["value"] / lines[0]["value"]
+            line["proposal"] = {**learned["stats"], "applied_steps": learned["applied_steps"], "training": train}
+        lines.append(line)
+    for line in lines:
+        print(json.dumps(line), flush=True)
 
 
 def main():
@@ -382,6 +499,9 @@ def main():
         return
     if a.workload == "ensemble":
         run_ensemble(a)
+        return
+    if a.workload == "learned":
+        run_learned(a)
         return
     import numpy as np
     import torch

@@ -77,6 +77,7 @@ struct SimBase
     virtual mwdg2_status timing(double* out, int n) = 0;
     virtual mwdg2_status set_timing(int mode) = 0;
     virtual mwdg2_status counters(int64_t* out, int n) = 0;
+    virtual mwdg2_status volume(double* out) = 0;
     // learned refinement proposal
     virtual mwdg2_status proposal_record(bool on) = 0;
     virtual mwdg2_status proposal_enable(const float* params, int judge_every, float threshold, float miss_bound) = 0;
@@ -112,6 +113,7 @@ public:
     mwdg2_status timing(double* out, int n) override;
     mwdg2_status set_timing(int mode) override;
     mwdg2_status counters(int64_t* out, int n) override;
+    mwdg2_status volume(double* out) override;
     mwdg2_status proposal_record(bool on) override;
     mwdg2_status proposal_enable(const float* params, int judge_every, float threshold, float miss_bound) override;
     mwdg2_status proposal_stats(double* out, int n) override;
@@ -916,6 +918,26 @@ template <typename T> mwdg2_status Sim<T>::finish_step(double* dt_out, int64_t* 
     return MWDG2_OK;
 }
 
+template <typename T> mwdg2_status Sim<T>::volume(double* out)
+{
+    CU(cudaSetDevice(device_));
+    double* d = nullptr;
+    CU(cudaMalloc(&d, sizeof(double)));
+    cudaError_t e = cudaMemsetAsync(d, 0, sizeof(double), st_);
+    if (e == cudaSuccess)
+    {
+        mw::k_volume<T><<<grid_leaf_, 256, 0, st_>>>(lf_, sc_, L_, d);
+        e = cudaGetLastError();
+    }
+    double v = 0.0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&v, d, sizeof(double), cudaMemcpyDeviceToHost, st_);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st_);
+    cudaFree(d);
+    CU(e);
+    *out = v * (double)cs_.dx * (double)cs_.dx;
+    return MWDG2_OK;
+}
+
 template <typename T> mwdg2_status Sim<T>::prop_alloc()
 {
     if (!mw_) return set_err(MWDG2_ERR_STATE, "the refinement proposal applies to MWDG2 only");
@@ -959,7 +981,6 @@ mwdg2_status Sim<T>::proposal_enable(const float* params, int judge_every, float
         prop_learned_ = false;
         return proposal_record(prop_rec_);
     }
-    if (L_ < 11) return set_err(MWDG2_ERR_STATE, "the refinement proposal acts on max_ref_lvl >= 11 (levels 10 and up)");
     if (mwdg2_status s = prop_alloc()) return s;
     CU(cudaMemcpy(d_mlp_, params, sizeof(float) * mlp::kParams, cudaMemcpyHostToDevice));
     prop_learned_ = true;
@@ -1632,6 +1653,12 @@ mwdg2_status mwdg2_last_step_counters(mwdg2_sim* s, int64_t* out, int n)
 }
 
 void mwdg2_destroy(mwdg2_sim* s) { delete s; }
+
+mwdg2_status mwdg2_volume(mwdg2_sim* s, double* out)
+{
+    if (!s || !out) return set_err(MWDG2_ERR_ARG, "null argument");
+    return s->impl->volume(out);
+}
 
 mwdg2_status mwdg2_proposal_record(mwdg2_sim* s, int on)
 {

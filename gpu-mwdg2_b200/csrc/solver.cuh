@@ -905,6 +905,28 @@ __global__ void k_sample_points(Leaves<T> lf, Hier<T> hr, Scalars<T>* sc, int L,
 }
 
 // Leaf state with the bed coefficients gathered from the hierarchy, 12 rows of n values.
+// Water volume of the leaf state in cell units: sum over leaves of h0 x 4^(L - level), each
+// term exact in FP64 (a power-of-two scaling of the leaf's depth) and summed in FP64 whatever
+// the state's precision; times dx^2 it is the volume in m^3. One atomic per block.
+template <typename T> __global__ void __launch_bounds__(256) k_volume(Leaves<T> lf, const Scalars<T>* sc, int L, double* out)
+{
+    const int n = sc->n_leaves;
+    double v = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        v += ldexp((double)lf.un[0][i], 2 * (L - (int)lf.lvl[i]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    __shared__ double red[8];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+        atomicAdd(out, t);
+    }
+}
+
 template <typename T> __global__ void k_gather_state(Leaves<T> lf, Hier<T> hr, Scalars<T>* sc, bool mw, double* out)
 {
     const int n = sc->n_leaves;

@@ -95,6 +95,8 @@ def lib():
         L.mwdg2_trainer_observe.argtypes = [vp, vp, ctypes.c_float, fp]
         L.mwdg2_trainer_params.argtypes = [vp, fp]
         L.mwdg2_trainer_destroy.argtypes = [vp]
+        L.mwdg2_volume.argtypes = [vp, dp]
+        L.mwdg2_volume.restype = ctypes.c_int
         L.mwdg2_proposal_record.argtypes = [vp, ctypes.c_int]
         L.mwdg2_proposal_enable.argtypes = [vp, fp, ctypes.c_int, ctypes.c_float, ctypes.c_float]
         L.mwdg2_proposal_stats.argtypes = [vp, dp, ctypes.c_int]
@@ -250,6 +252,12 @@ class Simulation:
         out = np.zeros(8)
         _check(lib().mwdg2_last_step_timing(self._h, _p(out, ctypes.c_double), 8))
         return out
+
+    def volume(self) -> float:
+        """Water volume of the current state (m^3), an FP64 reduction on the device."""
+        v = ctypes.c_double()
+        _check(lib().mwdg2_volume(self._h, ctypes.byref(v)))
+        return v.value
 
     def proposal_record(self, on: bool = True):
         """Record the proposal's features (step start) and activity labels (step end)."""

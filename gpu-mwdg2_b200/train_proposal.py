@@ -9,9 +9,9 @@ coarse cell (8 x 8 finest cells) are built on the device, and at its end each ch
 subtree's activity (a leaf the RK stages updated, or a significance flag the encode
 changed). Every `--every`-th step one Adam step of the tcgen05 training kernel is taken on
 all coarse cells of that step (mwdg2_trainer_observe), with the active class weighted by
-`--pos-weight`. The last `--holdout` scenarios are not trained on: the proposal's recall and
-precision on them are measured at the chosen logit threshold, and the parameters are
-written with those figures to proposal_mlp.npz.
+`--pos-weight`. The last `--holdout` scenarios are not trained on: every step of them scores
+the trained proposal (at the chosen logit threshold) against the step's activity on the
+device, and the parameters are written with its recall and precision to proposal_mlp.npz.
 
     python gpu-mwdg2_b200/train_proposal.py [--scenarios 200] [--sim-time 900] ...
 """
@@ -20,6 +20,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import shutil
 import sys
 import tempfile
 import time
@@ -78,7 +79,10 @@ def main():
             hold = i >= a.scenarios - a.holdout
             sim = mwdg2_b200.Simulation(par, precision=a.precision)
             sim.proposal_record(True)
-            params = tr.params() if hold else None
+            if hold:
+                # every step a judge step: the proposal is scored against the step's activity
+                # on the device and never applied
+                sim.proposal_enable(tr.params(), judge_every=1, threshold=a.threshold, miss_bound=1.0)
             k = 0
             while True:
                 ok, dt, n = sim.step()
@@ -86,19 +90,16 @@ def main():
                     break
                 k += 1
                 n_steps += 1
-                if k < 2 or k % a.every:
+                if k < 2:
                     continue
                 if hold:
-                    feats, labels = sim_samples(sim)
-                    _, prop = mwdg2_b200.mlp_forward(params, feats, a.threshold)
-                    y = ((labels[:, None] >> np.arange(4)) & 1).astype(bool)
-                    p = prop.astype(bool)
-                    counts += [np.sum(y & p), np.sum(y & ~p), np.sum(~y & p), np.sum(~y & ~p)]
-                else:
+                    st = sim.proposal_stats()
+                    tp = st["active"] - st["missed"]
+                    counts += [tp, st["missed"], st["proposed"] - tp, st["subtrees"] - st["proposed"] - st["missed"]]
+                elif k % a.every == 0:
                     losses.append(tr.observe(sim, a.pos_weight))
                     n_updates += 1
             sim.close()
-            import shutil
             shutil.rmtree(os.path.dirname(par), ignore_errors=True)
             if (i + 1) % 10 == 0:
                 print(json.dumps({"scenarios": i + 1, "steps": n_steps, "updates": n_updates,
@@ -118,11 +119,6 @@ def main():
                "seconds": round(time.time() - t0, 1)}
     np.savez(a.out, params=params, summary=json.dumps(summary))
     print(json.dumps(summary), flush=True)
-
-
-def sim_samples(sim) -> tuple[np.ndarray, np.ndarray]:
-    """The features and labels the simulation recorded for its last step, on the host."""
-    return sim.proposal_samples()
 
 
 if __name__ == "__main__":

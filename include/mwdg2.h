@@ -137,6 +137,11 @@ mwdg2_status mwdg2_set_timing(mwdg2_sim* sim, int mode);
  * device->host (its scalars and the stage-point values). n <= 10. */
 mwdg2_status mwdg2_last_step_counters(mwdg2_sim* sim, int64_t* out, int n);
 
+/* Water volume of the current state, sum over leaves of h0 x leaf area (m^3), reduced on
+ * the device in FP64 whatever the state's precision. No counterpart in the reference (its
+ * c-prop outputs print states, not volumes). */
+mwdg2_status mwdg2_volume(mwdg2_sim* sim, double* out);
+
 void mwdg2_destroy(mwdg2_sim* sim);
 
 /* ---------------------------------------------------------------- batched ensembles
@@ -254,7 +259,8 @@ mwdg2_status mwdg2_proposal_record(mwdg2_sim* sim, int on);
  * (logit > threshold); subtrees left out keep their flags and values. Every judge_every-th
  * step (0: never) runs in full as the judge; a step whose active subtrees the proposal left
  * out exceed the fraction miss_bound makes the next judge_every steps run in full. params =
- * NULL switches the proposal off. MWDG2 with max_ref_lvl >= 11 only (MWDG2_ERR_STATE). */
+ * NULL switches the proposal off. MWDG2 only (MWDG2_ERR_STATE). The proposal acts on the
+ * levels above 9 (one kernel launch per level), so below max_ref_lvl 11 it is only scored. */
 mwdg2_status mwdg2_proposal_enable(mwdg2_sim* sim, const float* params, int judge_every, float threshold,
                                    float miss_bound);
 

@@ -92,3 +92,19 @@ def test_urban_catchment_matches_oracle(tmp_path, solver):
     finally:
         sim.close()
         orc.close()
+
+
+@pytest.mark.parametrize("solver", ["mwdg2", "hwfv1"])
+@pytest.mark.parametrize("precision", [64, 32])
+def test_device_volume_reduction_matches_host_sum(tmp_path, solver, precision):
+    """mwdg2_volume (FP64 reduction on the device) equals the host's FP64 sum of h0 x leaf
+    area over the leaf state, on an adaptive fBm catchment after a few steps."""
+    c = cases.fbm_catchment(str(tmp_path), L=8, solver=solver, sim_time=600.0,
+                            start_depth=np.maximum(0.0, 12.0 - cases.fbm_surface(256, 0.8, 5, 30.0)))
+    with mwdg2_b200.Simulation(c.par, precision=precision) as sim:
+        for _ in range(5):
+            assert sim.step()[0]
+        host = _volume(sim, c.L, c.cellsize)
+        dev = sim.volume()
+    assert host > 0
+    assert abs(dev - host) <= 1e-12 * host, (dev, host)
