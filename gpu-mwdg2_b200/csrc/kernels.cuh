@@ -54,12 +54,10 @@ template <typename T> struct Scalars
 };
 
 // The subtrees below the nodes of level `level` (the proposal level) that a step's encode and
-// decode visit: prop[node] != 0 (null: all), and where the encode records a change of a
-// significance flag (act[node] = 1; null: nowhere).
+// decode visit: prop[node] != 0 (null: all).
 struct PropMask
 {
     const uint8_t* prop;
-    uint8_t* act;
     int level;
 };
 
@@ -374,7 +372,6 @@ __device__ __forceinline__ void encode_parent(const Hier<T>& hr, const Scalars<T
         ++n_done;
     }
     if (nf != f) hr.flags[p] = nf;   // most large-level parents keep their flags
-    if (PM && anc >= 0 && pm.act && ((nf ^ f) & F_SIG)) pm.act[anc] = 1;
 }
 
 // Small levels are processed in bands of up to kBandDepth levels, one CTA per node of the

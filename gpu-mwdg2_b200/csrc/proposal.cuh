@@ -15,9 +15,9 @@
 //   output  4 logits: the children whose subtrees need their encode and decode this step
 //
 // A child subtree is "active" in a step when one of its leaves was updated by the RK stages
-// (not dry) or its encode changed one of its significance flags; the step after, the
-// encode must revisit it. The label of a training sample is the activity of the step the
-// features precede.
+// (not dry) or its significance flags at the end of the step differ from the last step's;
+// the step after, the encode must revisit it. The label of a training sample is the
+// activity of the step the features precede.
 //
 // Kernels (one CTA of 128 threads = one warpgroup per 128-row tile; thread r owns row r,
 // which is TMEM lane r of every accumulator):
@@ -159,6 +159,40 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// 64 consecutive FP32 columns of this thread's TMEM lane in one load and one wait.
+__device__ __forceinline__ void tmem_ld64(uint32_t taddr, float (&v)[64])
+{
+    uint32_t r[64];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x64.b32 {"
+                 "%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+                 "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, "
+                 "%32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, "
+                 "%48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63}, [%64];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                   "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+                   "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+                   "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]),
+                   "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]),
+                   "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]),
+                   "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]),
+                   "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+                 : "r"(taddr)
+                 : "memory");
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+                   "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15]),
+                   "+r"(r[16]), "+r"(r[17]), "+r"(r[18]), "+r"(r[19]), "+r"(r[20]), "+r"(r[21]), "+r"(r[22]), "+r"(r[23]),
+                   "+r"(r[24]), "+r"(r[25]), "+r"(r[26]), "+r"(r[27]), "+r"(r[28]), "+r"(r[29]), "+r"(r[30]), "+r"(r[31]),
+                   "+r"(r[32]), "+r"(r[33]), "+r"(r[34]), "+r"(r[35]), "+r"(r[36]), "+r"(r[37]), "+r"(r[38]), "+r"(r[39]),
+                   "+r"(r[40]), "+r"(r[41]), "+r"(r[42]), "+r"(r[43]), "+r"(r[44]), "+r"(r[45]), "+r"(r[46]), "+r"(r[47]),
+                   "+r"(r[48]), "+r"(r[49]), "+r"(r[50]), "+r"(r[51]), "+r"(r[52]), "+r"(r[53]), "+r"(r[54]), "+r"(r[55]),
+                   "+r"(r[56]), "+r"(r[57]), "+r"(r[58]), "+r"(r[59]), "+r"(r[60]), "+r"(r[61]), "+r"(r[62]), "+r"(r[63])
+                 :
+                 : "memory");
+#pragma unroll
+    for (int i = 0; i < 64; ++i) v[i] = __uint_as_float(r[i]);
+}
+
 // ---------------------------------------------------------------- shared-memory operand layout
 // Canonical no-swizzle K-major tile of `K` columns: element (row r, column k) at
 //   (r / 8) * (16 K) + (k / 8) * 128 + (r % 8) * 16 + (k % 8) * 2 bytes,
@@ -227,6 +261,20 @@ __device__ __forceinline__ void load_weights(const float* prm, uint8_t* sW1, uin
     }
 }
 
+// The weights and biases as the forward kernels hold them in shared memory (the bytes from
+// FwdSmem::W1 to FwdSmem::Bar), built once per parameter set by k_mlp_pack, so that a CTA
+// starts with one vectorised copy instead of converting the FP32 block.
+constexpr int kPackBytes = 35648;   // FwdSmem::Bar - FwdSmem::W1
+
+// Shared-memory image of the parameters (one CTA).
+__device__ __forceinline__ void load_packed(const uint8_t* __restrict__ pack, uint8_t* dst)
+{
+    const uint4* src = reinterpret_cast<const uint4*>(pack);
+    uint4* d = reinterpret_cast<uint4*>(dst);
+#pragma unroll 6
+    for (int i = threadIdx.x; i < kPackBytes / 16; i += blockDim.x) d[i] = src[i];
+}
+
 // Row r of the features: 128 BF16 values from a row-major global array (zeros past n).
 __device__ __forceinline__ void load_feature_row(const __nv_bfloat16* feats, int64_t row, int64_t n, uint8_t* sX, int r)
 {
@@ -244,16 +292,12 @@ __device__ __forceinline__ void load_feature_row(const __nv_bfloat16* feats, int
 __device__ __forceinline__ void hidden_epilogue(uint32_t tcol, const float* bias, uint8_t* sH, int r)
 {
     const int warp = threadIdx.x >> 5;
+    float v[kH];
+    tmem_ld64(tcol + ((uint32_t)(warp * 32) << 16), v);
 #pragma unroll
-    for (int c = 0; c < kH; c += 16)
-    {
-        float v[16];
-        tmem_ld16(tcol + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
+    for (int i = 0; i < kH; ++i) v[i] = fmaxf(v[i] + bias[i], 0.0f);
 #pragma unroll
-        for (int i = 0; i < 16; ++i) v[i] = fmaxf(v[i] + bias[c + i], 0.0f);
-        st_row8(sH, r, c, kH, v);
-        st_row8(sH, r, c + 8, kH, v + 8);
-    }
+    for (int c = 0; c < kH; c += 8) st_row8(sH, r, c, kH, v + c);
 }
 
 // Dynamic shared memory of the forward kernel (bytes, 1024-aligned base).
@@ -344,7 +388,17 @@ __device__ __forceinline__ void load_biases(const float* prm, float* bias)
     }
 }
 
+static_assert(FwdSmem::Bar - FwdSmem::W1 == kPackBytes && FwdSmem::W1 % 16 == 0, "packed parameter image");
+
 // (static kernels here: the header is included by more than one translation unit)
+// The packed image of a parameter block (one CTA of 128 threads).
+static __global__ void __launch_bounds__(kRows) k_mlp_pack(const float* __restrict__ prm, uint8_t* __restrict__ pack)
+{
+    uint8_t* base = pack - FwdSmem::W1;   // the image's offsets are those of the shared memory
+    load_weights(prm, base + FwdSmem::W1, base + FwdSmem::W2, base + FwdSmem::W3, base + FwdSmem::W4);
+    load_biases(prm, reinterpret_cast<float*>(base + FwdSmem::Bias));
+}
+
 // Inference over n rows of features (row-major BF16 [n][128]). Outputs (either may be null):
 // logits[n][4]; prop[4 n] bytes, 1 where the logit exceeds `thr`. err: set to 1 if a wait
 // ran out. One CTA of 128 threads per tile, persistent over the tiles.

@@ -84,6 +84,7 @@ struct SimBase
     virtual mwdg2_status proposal_stats(double* out, int n) = 0;
     virtual mwdg2_status proposal_samples(const void** feats, const uint8_t** labels, int64_t* n, int* device) = 0;
     virtual mwdg2_status proposal_samples_host(float* feats, uint8_t* labels, int64_t cap, int64_t* n) = 0;
+    virtual mwdg2_status proposal_mask(uint8_t* out, int64_t cap, int64_t* n) = 0;
 };
 
 template <typename T> class Sim final : public SimBase
@@ -119,6 +120,17 @@ public:
     mwdg2_status proposal_stats(double* out, int n) override;
     mwdg2_status proposal_samples(const void** feats, const uint8_t** labels, int64_t* n, int* device) override;
     mwdg2_status proposal_samples_host(float* feats, uint8_t* labels, int64_t cap, int64_t* n) override;
+    mwdg2_status proposal_mask(uint8_t* out, int64_t cap, int64_t* n) override
+    {
+        if (!prop_learned_) return set_err(MWDG2_ERR_STATE, "no proposal is enabled");
+        if (n) *n = prop_nC_ * 4;
+        if (!out) return MWDG2_OK;
+        if (cap < prop_nC_ * 4) return set_err(MWDG2_ERR_ARG, "capacity below the number of subtrees");
+        CU(cudaSetDevice(device_));
+        CU(cudaStreamSynchronize(st_));
+        CU(cudaMemcpy(out, d_prop_, (size_t)prop_nC_ * 4, cudaMemcpyDeviceToHost));
+        return MWDG2_OK;
+    }
 
 private:
     mwio::Case<T> cs_;
@@ -220,7 +232,9 @@ private:
     uint8_t* d_lab_ = nullptr;          // [4^C] activity bits of the children in the last step
     uint8_t* d_act_ = nullptr;          // [4^(C+1)] activity marks of this step
     uint8_t* d_prop_ = nullptr;         // [4^(C+1)] proposal of this step
+    uint8_t* d_sig5_ = nullptr;         // [4^(C+1)] flags of each subtree's two parent levels, last step
     float* d_mlp_ = nullptr;            // MLP parameters
+    uint8_t* d_mlp_pack_ = nullptr;     // their shared-memory image (mlp::k_mlp_pack)
     int* d_mlp_err_ = nullptr;
     float prop_thr_ = 0.0f, prop_bound_ = 0.0f;
     int prop_judge_every_ = 0, prop_since_judge_ = 0, prop_fallback_left_ = 0;
@@ -289,13 +303,10 @@ private:
     // The proposal's mask of this step's encode / decode (prop_on_: the proposal records or
     // applies; the masked kernels are used on the levels at and below its level C + 1).
     bool prop_on() const { return prop_rec_ || prop_learned_; }
-    mw::PropMask prop_mask(bool record) const
-    {
-        return mw::PropMask{prop_apply_ ? d_prop_ : nullptr, record ? d_act_ : nullptr, prop_C_ + 1};
-    }
+    mw::PropMask prop_mask() const { return mw::PropMask{prop_apply_ ? d_prop_ : nullptr, prop_C_ + 1}; }
     template <bool FULL> void encode_tree(const mw::Hier<T>& h, T eps)
     {
-        const mw::PropMask pm = prop_mask(FULL);
+        const mw::PropMask pm = prop_mask();
         for (int level = L_ - 1; level > mw::kBandMaxLevel; --level)
         {
             if (folded_below(level)) continue;
@@ -682,17 +693,27 @@ template <typename T> mwdg2_status Sim<T>::enqueue_device()
     const bool remesh = (eps > T(0) || first_);
     if (prop_on() && remesh)
     {
-        // features of the step's start; the MLP's proposal (applied or, on judge and fallback
-        // steps, only scored against the step's activity)
-        const int grid = grid_for(prop_nC_, 128, 148 * 16);
-        mw::k_prop_features<T><<<grid, 128, 0, st_>>>(hr_, prop_C_, d_lab_, d_feat_);
-        ++launches_;
-        if (prop_learned_)
+        // the MLP's proposal (applied or, on judge and fallback steps, only scored against the
+        // step's activity): one fused kernel; with recording on, the features are written out
+        // for the trainer first and the MLP reads them
+        const int64_t tiles = (prop_nC_ + mlp::kRows - 1) / mlp::kRows;
+        const int g = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, 2 * (int64_t)(solver_blocks_ / 8)));
+        if (prop_rec_)
         {
-            const int64_t tiles = (prop_nC_ + mlp::kRows - 1) / mlp::kRows;
-            const int g = (int)std::min<int64_t>(tiles, 2 * (int64_t)(solver_blocks_ / 8));
-            mlp::k_mlp_forward<<<g, mlp::kRows, mlp::FwdSmem::Total + 1024, st_>>>(d_mlp_, d_feat_, prop_nC_, nullptr, d_prop_,
-                                                                                 prop_thr_, d_mlp_err_);
+            const int grid = grid_for(prop_nC_, 128, 148 * 16);
+            mw::k_prop_features<T><<<grid, 128, 0, st_>>>(hr_, prop_C_, d_lab_, d_feat_);
+            ++launches_;
+            if (prop_learned_)
+            {
+                mlp::k_mlp_forward<<<g, mlp::kRows, mlp::FwdSmem::Total + 1024, st_>>>(d_mlp_, d_feat_, prop_nC_, nullptr,
+                                                                                     d_prop_, prop_thr_, d_mlp_err_);
+                ++launches_;
+            }
+        }
+        else if (prop_learned_ && prop_nC_ >= mlp::kRows)
+        {
+            mw::k_mlp_propose<T><<<g, mlp::kRows, mw::ProposeSmem<T>::Total + 1024, st_>>>(d_mlp_pack_, hr_, prop_C_, d_lab_,
+                                                                                        d_prop_, prop_thr_, d_mlp_err_);
             ++launches_;
         }
     }
@@ -726,7 +747,7 @@ template <typename T> mwdg2_status Sim<T>::enqueue_device()
             CU(cudaStreamWaitEvent(st_dec_, ev_dec_fork_, 0));
             // (no folding here: a thread decoding a child after its parent lengthens the
             // kernel's tail, while the sparse level's own kernel overlaps the topology)
-            const mw::PropMask pm = prop_mask(false);
+            const mw::PropMask pm = prop_mask();
             for (int level = mw::kBandMaxLevel + 1; level < L_; ++level)
             {
                 const bool pmk = prop_on() && level >= pm.level;
@@ -783,8 +804,8 @@ template <typename T> mwdg2_status Sim<T>::enqueue_device()
     }
     if (prop_on() && remesh)
     {
-        mw::k_prop_labels<<<grid_for(prop_nC_, 256, 148 * 8), 256, 0, st_>>>(d_act_, prop_learned_ ? d_prop_ : nullptr,
-                                                                           d_lab_, prop_nC_, &sc_->prop_active);
+        mw::k_prop_labels<<<grid_for(prop_nC_, 256, 2 * (solver_blocks_ / 8)), 256, 0, st_>>>(
+            d_act_, prop_learned_ ? d_prop_ : nullptr, hr_.flags, prop_C_, d_sig5_, d_lab_, prop_nC_, &sc_->prop_active);
         ++launches_;
     }
     // the stage points of the new state come back with the step's scalars
@@ -949,7 +970,10 @@ template <typename T> mwdg2_status Sim<T>::prop_alloc()
     if (mwdg2_status s = dalloc(d_lab_, (size_t)prop_nC_)) return s;
     if (mwdg2_status s = dalloc(d_act_, (size_t)prop_nC_ * 4)) return s;
     if (mwdg2_status s = dalloc(d_prop_, (size_t)prop_nC_ * 4)) return s;
+    if (mwdg2_status s = dalloc(d_sig5_, (size_t)prop_nC_ * 4)) return s;
+    CU(cudaMemset(d_sig5_, 0, (size_t)prop_nC_ * 4));
     if (mwdg2_status s = dalloc(d_mlp_, mlp::kParams)) return s;
+    if (mwdg2_status s = dalloc(d_mlp_pack_, mlp::kPackBytes)) return s;
     if (mwdg2_status s = dalloc(d_mlp_err_, 1)) return s;
     CU(cudaMemset(d_lab_, 0, (size_t)prop_nC_));
     CU(cudaMemset(d_act_, 0, (size_t)prop_nC_ * 4));
@@ -957,6 +981,8 @@ template <typename T> mwdg2_status Sim<T>::prop_alloc()
     CU(cudaMemset(d_mlp_err_, 0, sizeof(int)));
     CU(cudaFuncSetAttribute(mlp::k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)(mlp::FwdSmem::Total + 1024)));
+    CU(cudaFuncSetAttribute(mw::k_mlp_propose<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)(mw::ProposeSmem<T>::Total + 1024)));
     return MWDG2_OK;
 }
 
@@ -983,6 +1009,9 @@ mwdg2_status Sim<T>::proposal_enable(const float* params, int judge_every, float
     }
     if (mwdg2_status s = prop_alloc()) return s;
     CU(cudaMemcpy(d_mlp_, params, sizeof(float) * mlp::kParams, cudaMemcpyHostToDevice));
+    mlp::k_mlp_pack<<<1, mlp::kRows, 0, st_>>>(d_mlp_, d_mlp_pack_);
+    CU(cudaGetLastError());
+    CU(cudaStreamSynchronize(st_));
     prop_learned_ = true;
     prop_judge_every_ = judge_every;
     prop_thr_ = threshold;
@@ -1677,6 +1706,12 @@ mwdg2_status mwdg2_proposal_samples(mwdg2_sim* s, float* feats, uint8_t* labels,
 {
     if (!s) return set_err(MWDG2_ERR_ARG, "null handle");
     return s->impl->proposal_samples_host(feats, labels, cap, n);
+}
+
+mwdg2_status mwdg2_proposal_mask(mwdg2_sim* s, uint8_t* out, int64_t cap, int64_t* n)
+{
+    if (!s) return set_err(MWDG2_ERR_ARG, "null handle");
+    return s->impl->proposal_mask(out, cap, n);
 }
 
 mwdg2_status mwdg2_proposal_stats(mwdg2_sim* s, double* out, int n)

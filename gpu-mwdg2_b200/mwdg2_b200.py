@@ -102,6 +102,8 @@ def lib():
         L.mwdg2_proposal_stats.argtypes = [vp, dp, ctypes.c_int]
         L.mwdg2_proposal_samples.argtypes = [vp, fp, u8p, ctypes.c_int64, i64p]
         L.mwdg2_proposal_samples.restype = ctypes.c_int
+        L.mwdg2_proposal_mask.argtypes = [vp, u8p, ctypes.c_int64, i64p]
+        L.mwdg2_proposal_mask.restype = ctypes.c_int
         for name in ("mwdg2_mlp_forward", "mwdg2_mlp_grad", "mwdg2_trainer_create", "mwdg2_trainer_step",
                      "mwdg2_trainer_observe", "mwdg2_trainer_params", "mwdg2_proposal_record", "mwdg2_proposal_enable",
                      "mwdg2_proposal_stats"):
@@ -281,6 +283,14 @@ class Simulation:
         _check(lib().mwdg2_proposal_samples(self._h, _p(feats, ctypes.c_float), _p(labels, ctypes.c_uint8), n.value,
                                             ctypes.byref(n)))
         return feats, labels
+
+    def proposal_mask(self) -> np.ndarray:
+        """The last step's proposal, one byte per child subtree of the coarse level."""
+        n = ctypes.c_int64()
+        _check(lib().mwdg2_proposal_mask(self._h, None, 0, ctypes.byref(n)))
+        out = np.zeros(n.value, np.uint8)
+        _check(lib().mwdg2_proposal_mask(self._h, _p(out, ctypes.c_uint8), n.value, ctypes.byref(n)))
+        return out
 
     def proposal_stats(self) -> dict:
         a = np.zeros(10)

@@ -6,8 +6,8 @@ chance, by a west-edge point inflow peaking at U(20, 50) m^3/s or by a dam break
 radius over part of the domain. The plain step runs on the GPU with the proposal's
 recording on (mwdg2_proposal_record): at the start of every step the features of every
 coarse cell (8 x 8 finest cells) are built on the device, and at its end each child
-subtree's activity (a leaf the RK stages updated, or a significance flag the encode
-changed). Every `--every`-th step one Adam step of the tcgen05 training kernel is taken on
+subtree's activity (a leaf the RK stages updated, or its significance flags changed since
+the last step). Every `--every`-th step one Adam step of the tcgen05 training kernel is taken on
 all coarse cells of that step (mwdg2_trainer_observe), with the active class weighted by
 `--pos-weight`. The last `--holdout` scenarios are not trained on: every step of them scores
 the trained proposal (at the chosen logit threshold) against the step's activity on the

@@ -249,9 +249,9 @@ mwdg2_status mwdg2_trainer_params(mwdg2_trainer* t, float* out);
 void mwdg2_trainer_destroy(mwdg2_trainer* t);
 
 /* Record, from the next step on, the proposal's features at each step's start and the
- * activity of each child subtree over the step (its leaves updated by the RK stages or its
- * significance flags changed by the encode), for mwdg2_trainer_observe. MWDG2 only; results
- * are unchanged. on = 0 stops recording. */
+ * activity of each child subtree over the step (one of its leaves updated by the RK stages,
+ * or its significance flags at the step's end different from the last step's), for
+ * mwdg2_trainer_observe. MWDG2 only; results are unchanged. on = 0 stops recording. */
 mwdg2_status mwdg2_proposal_record(mwdg2_sim* sim, int on);
 
 /* Let the MLP with `params` (MWDG2_MLP_PARAMS floats, copied) choose, from the next step on,
@@ -268,6 +268,10 @@ mwdg2_status mwdg2_proposal_enable(mwdg2_sim* sim, const float* params, int judg
  * bytes; may be NULL) the last recorded step left for its n coarse cells (cap: rows the
  * arrays hold; n is written in any case). */
 mwdg2_status mwdg2_proposal_samples(mwdg2_sim* sim, float* feats, uint8_t* labels, int64_t cap, int64_t* n);
+
+/* The last step's proposal: one byte per child subtree of the coarse level (4^(C+1), Z order
+ * of level C + 1), 1 = visited. *n receives the count; out may be NULL. */
+mwdg2_status mwdg2_proposal_mask(mwdg2_sim* sim, uint8_t* out, int64_t cap, int64_t* n);
 
 /* [0] active subtrees in the last step, [1] of them left out by the proposal, [2] subtrees
  * proposed, [3] 1 if the last step applied the proposal, [4] subtrees in all, [5] steps that

@@ -3,9 +3,13 @@ catchment, FP64), through the C ABI:
 
 * recording the features and activity labels leaves every result bit-identical;
 * a proposal that keeps every subtree gives the plain step's results bit for bit (the masked
-  encode, decode and re-encode kernels with an all-ones mask);
+  encode, decode and re-encode kernels with an all-ones mask; the MLP run on every coarse
+  cell, as with recording on);
 * a proposal that keeps none skips the upper levels' encode and decode, misses the active
   subtrees, and the fallback then runs full steps (judge every 4 steps, miss bound 5 %);
+* the fused proposal kernel (features from a shared-memory ring, then the MLP) gives the
+  proposal of the two-kernel path (features written out, then the MLP) on every tile whose
+  ring of coarse cells had activity last step, and proposes nothing elsewhere;
 * the device-built feature rows equal the NumPy restatement of the feature builder
   (tests/mlp_ref.py) from the hierarchy, flags and activity bits the previous step left;
 * the trainer takes an Adam step on the features and labels a recorded step left on the
@@ -65,7 +69,10 @@ def test_recording_and_all_ones_proposal_change_nothing(tmp_path):
     plain = _run(c.par, _none)
     rec = _run(c.par, lambda s: s.proposal_record(True))
     _same(plain, rec, "recording")
-    ones = _run(c.par, lambda s: s.proposal_enable(_constant_mlp(20.0), judge_every=0, threshold=0.0, miss_bound=1.0))
+    # with recording on the MLP runs on every coarse cell (the fused kernel would leave out
+    # tiles with no activity around them)
+    ones = _run(c.par, lambda s: (s.proposal_record(True),
+                                  s.proposal_enable(_constant_mlp(20.0), judge_every=0, threshold=0.0, miss_bound=1.0)))
     _same(plain, ones, "all-ones proposal")
     st = ones[-1][3]
     assert st["applied"] == 1.0 and st["proposed"] == st["subtrees"] and st["missed"] == 0
@@ -117,3 +124,43 @@ def test_features_match_numpy_restatement(tmp_path):
     want = mlp_ref.proposal_features(hier, sig, L, lab_prev)
     np.testing.assert_array_equal(feats[:, :113], want[:, :113].astype(np.float32))
     assert not np.any(feats[:, 113:])
+
+
+def _ring_active(labels: np.ndarray, C: int) -> np.ndarray:
+    """Per 128-row tile of the coarse level: any activity bit in its 16 x 8 block or ring."""
+    nside = 1 << C
+    code = np.arange(1 << (2 * C), dtype=np.int64)
+    x, y = mlp_ref._compact(code), mlp_ref._compact(code >> 1)
+    grid = np.zeros((nside + 2, nside + 2), bool)
+    grid[y + 1, x + 1] = labels != 0
+    out = np.zeros(len(code) // 128, bool)
+    for t in range(len(out)):
+        x0, y0 = x[128 * t], y[128 * t]
+        out[t] = grid[y0:y0 + 10, x0:x0 + 18].any()
+    return out
+
+
+def test_fused_proposal_matches_two_kernel_path(tmp_path):
+    c = _case(tmp_path)
+    params = np.load(mwdg2_b200.HERE + "/proposal_mlp.npz")["params"]
+    a = mwdg2_b200.Simulation(c.par, precision=64)
+    b = mwdg2_b200.Simulation(c.par, precision=64)
+    a.proposal_record(True)
+    for s in (a, b):
+        s.proposal_enable(params, judge_every=0, threshold=-2.0, miss_bound=1.0)
+    C = L - 3
+    checked = 0
+    for step in range(1, 5):
+        _, lab_prev = a.proposal_samples() if step > 1 else (None, np.zeros(1 << (2 * C), np.uint8))
+        a.step()
+        b.step()
+        if step == 1:
+            continue
+        ma, mb = a.proposal_mask(), b.proposal_mask()
+        active = np.repeat(_ring_active(lab_prev, C), 512)
+        np.testing.assert_array_equal(mb[active], ma[active], err_msg=f"step {step}: active tiles")
+        assert not mb[~active].any(), f"step {step}: a tile without activity around it proposed subtrees"
+        checked += int(active.sum())
+    assert checked > 0
+    a.close()
+    b.close()
