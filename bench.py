@@ -420,6 +420,38 @@ def finest_depth(sim):
     return st["h0"][rep] + st["h1x"][rep] * s3 * (2 * xu - 1) + st["h1y"][rep] * s3 * (2 * yu - 1)
 
 
+def learned_window(a, par, depth_plain, time_plain, value_plain) -> dict:
+    """The same window with the learned refinement proposal: a second simulation of the
+    same case with the trained MLP choosing the subtrees the encode and decode visit (judge
+    every --judge-every steps), W warm-up and K timed steps as the plain run's; its
+    active-cell updates/s, and the largest depth difference from the plain run at the end
+    of the window over every finest cell (cell-centre depths)."""
+    import numpy as np
+    import mwdg2_b200
+    z = np.load(a.proposal)
+    train = json.loads(str(z["summary"]))
+    sim = mwdg2_b200.Simulation(par, precision=a.precision, timing="step")
+    sim.proposal_enable(z["params"], judge_every=a.judge_every, threshold=train["threshold"], miss_bound=0.02)
+    for _ in range(a.warmup):
+        sim.step()
+    ms, leaves = [], []
+    for _ in range(a.steps):
+        ok, dt, n = sim.step()
+        ms.append(float(sim.last_step_timing()[7]))
+        leaves.append(n)
+    st = sim.proposal_stats()
+    diff = float(np.max(np.abs(finest_depth(sim) - depth_plain)))
+    t_end = sim.info()["time"]
+    sim.close()
+    v = sum(leaves) / (sum(ms) / 1e3)
+    return {"value": v, "ms_per_step": sum(ms) / a.steps, "vs_plain": v / value_plain,
+            "max_depth_diff_vs_plain_m": diff, "time": t_end, "plain_time": time_plain,
+            "proposal": {k: st[k] for k in ("active", "proposed", "subtrees", "learned_steps", "judge_steps",
+                                             "fallbacks")},
+            "mlp": os.path.basename(a.proposal), "judge_every": a.judge_every,
+            "timing": "device time of each step (CUDA events), steps W+1..W+K of a second run of the same case"}
+
+
 def run_learned(a):
     """The learned refinement proposal on the 4096^2 catchment: the same
     case run from t = 0 to --eval-time three times on this GPU -- plain in FP64 (the depth
@@ -545,6 +577,9 @@ def main():
     sim_s = sim.info()["time"] - t_sim0
     tot_ms = max_over_ranks(float(sum(ms_step)), dist, "cuda")
     value = replica_throughput(world, sum(leaves), tot_ms)
+    learned = None
+    if world == 1 and a.workload == "catchment" and a.solver == "mwdg2" and os.path.exists(a.proposal):
+        learned = learned_window(a, par, finest_depth(sim), sim.info()["time"], value)
 
     # end to end through the C ABI: each step's inputs (point-source values) go host->device
     # from pinned memory inside mwdg2_step, its scalars come back, and the stage-point
@@ -641,6 +676,8 @@ def main():
                                            "the timed steps over the simulated time they advanced)"},
             "init_s": t_init,
             "wet_fraction": [float(np.mean([cc[k] for cc in counters])) / n_mean for k in ("wet_stage1", "wet_stage2")]}
+    if learned is not None:
+        line["learned"] = learned
     if a.workload == "catchment" and a.peak_time > 0:
         line["window_peak"] = peak_window(sim, a, dist)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
