@@ -16,6 +16,11 @@ urban catchment (building blocks 5-20 m tall: wet/dry fronts against walls, fast
   threshold, where the wet/dry branch follows the last bit of the face value and hence
   the choice of fused multiply-adds (two IEEE CPU builds, with and without contraction,
   then differ by 1e-7 after one step); off the lattice the two agree to 2e-11 over 12 steps.
+* Partly wet fBm catchment with Manning friction and the slope limiter against the CPU
+  oracle (FP64, 12 steps, same bounds): valleys filled to a level off the DEM's 0.001 m
+  lattice leave about 30 % of the leaves wet, so from step 2 both RK stages run the wet
+  test, the dry-leaf writer and the wet-list kernel with friction on the listed leaves and
+  their neighbours' copies.
 Calls go through the C ABI (include/mwdg2.h)."""
 import numpy as np
 import pytest
@@ -108,3 +113,31 @@ def test_device_volume_reduction_matches_host_sum(tmp_path, solver, precision):
         dev = sim.volume()
     assert host > 0
     assert abs(dev - host) <= 1e-12 * host, (dev, host)
+
+
+def test_partly_wet_catchment_with_friction_matches_oracle(tmp_path):
+    L = 9
+    z = cases.fbm_surface(1 << L, 0.8, 20261203, 30.0)
+    h0 = np.maximum(0.0, 12.00037 - z)
+    c = cases.fbm_catchment(str(tmp_path), L=L, start_depth=h0, sim_time=600.0, manning=0.03, limitslopes=True)
+    sim = mwdg2_b200.Simulation(c.par, precision=64)
+    orc = oracle_py.Oracle(c.par, 64)
+    listed = 0
+    try:
+        for s in range(1, 13):
+            ok, dt, n = sim.step()
+            ok2, dt2, n2 = orc.step()
+            assert ok and ok2 and n == n2, f"step {s}: leaves {n} vs {n2}"
+            wet = sim.last_step_counters()["wet_stage1"]
+            listed += int(s > 1 and 0 < 2 * wet < n)
+            assert_same_topology(sim.leaves(), orc.leaves(), f"catchment step {s}")
+            np.testing.assert_array_equal(sim.sig(), orc.sig(), err_msg=f"step {s} sig")
+            st, so = sim.state(), orc.state()
+            for f in FIELDS:
+                e = rel_err(st[f], so[f])
+                assert e <= 1e-10, f"step {s} {f}: {e:.3e}"
+            assert abs(dt - dt2) <= 1e-9 * dt2
+    finally:
+        sim.close()
+        orc.close()
+    assert listed == 11, f"stage 1 ran over the wet list in {listed} of steps 2-12"
