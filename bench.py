@@ -171,9 +171,12 @@ class Clocks:
 # DRAM bytes per leaf (dram__bytes_read.sum + dram__bytes_write.sum of the phase's kernels,
 # summed, divided by the step's leaves) from a one-pass ncu launch list of this workload
 # (4096^2, FP32, 3.0 M leaves). Keyed by (solver, P, timing phase).
-TRAFFIC_SOURCE = "ncu launch list (dram bytes, 1 pass) of the same workload, per leaf x leaves"
+TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the phase's kernels (one kernel, three "
+                  "launches per capture) on the 2048^2 catchment (max_ref_lvl 11, 1.21 M leaves), per leaf, "
+                  "x this run's leaves")
 PHASE_STEPS = 5
-TRAFFIC_B_PER_LEAF: dict = {("mwdg2", 4, 3): 6.0, ("mwdg2", 4, 4): 208.6, ("mwdg2", 4, 6): 168.7}
+# DRAM bytes per leaf of the RK stages (phase 4: stage 1, phase 6: stage 2) in FP32
+TRAFFIC_B_PER_LEAF: dict = {("mwdg2", 4, 4): 181.0, ("mwdg2", 4, 6): 141.6}
 
 
 def max_over_ranks(x: float, dist, device: str) -> float:
@@ -344,6 +347,27 @@ def run_ensemble(a):
     print(json.dumps(line), flush=True)
 
 
+class nvtx_range:
+    """An NVTX range around a timed loop (a no-op without CUDA), so a profiler can capture
+    exactly those launches (ncu --nvtx --nvtx-include "<name>/")."""
+
+    def __init__(self, name: str):
+        self.name = name
+        self.on = False
+
+    def __enter__(self):
+        import torch
+        self.on = torch.cuda.is_available()
+        if self.on:
+            torch.cuda.nvtx.range_push(self.name)
+        return self
+
+    def __exit__(self, *exc):
+        if self.on:
+            import torch
+            torch.cuda.nvtx.range_pop()
+
+
 def peak_window(sim, a, dist) -> dict:
     """The same run later on: steps (untimed) until the simulated time reaches a.peak_time,
     then W warm-up steps and K steps timed as the first window (two CUDA events around each
@@ -363,13 +387,15 @@ def peak_window(sim, a, dist) -> dict:
         sim.step()
     t_sim0 = sim.info()["time"]
     ms, leaves, wet = [], [], []
-    for _ in range(a.steps):
-        ok, dt, n = sim.step()
-        ms.append(float(sim.last_step_timing()[7]))
-        leaves.append(n)
-        c = sim.last_step_counters()
-        wet.append((c["wet_stage1"], c["wet_stage2"]))
+    with nvtx_range("peak_window"):
+        for _ in range(a.steps):
+            ok, dt, n = sim.step()
+            ms.append(float(sim.last_step_timing()[7]))
+            leaves.append(n)
+            c = sim.last_step_counters()
+            wet.append((c["wet_stage1"], c["wet_stage2"]))
     sim_s = sim.info()["time"] - t_sim0
+    end_time, end_depth = sim.info()["time"], finest_depth(sim)   # for the learned run's comparison
     world = int(os.environ.get("WORLD_SIZE", "1"))
     tot_ms = max_over_ranks(float(sum(ms)), dist, "cuda")
     n_mean = float(np.mean(leaves))
@@ -388,7 +414,8 @@ def peak_window(sim, a, dist) -> dict:
             "ms_per_step": tot_ms / a.steps, "leaves_mean": n_mean,
             "wet_fraction": [float(np.mean([w[k] for w in wet])) / n_mean for k in (0, 1)],
             "wall_s_per_sim_s": (tot_ms / 1e3) / sim_s if sim_s > 0 else None, "sim_seconds": sim_s,
-            "timing": "device time of each step (CUDA events on the library's stream), max over ranks"}
+            "timing": "device time of each step (CUDA events on the library's stream), max over ranks",
+            "_end_time": end_time, "_end_depth": end_depth}
 
 
 def finest_depth(sim):
@@ -420,36 +447,60 @@ def finest_depth(sim):
     return st["h0"][rep] + st["h1x"][rep] * s3 * (2 * xu - 1) + st["h1y"][rep] * s3 * (2 * yu - 1)
 
 
-def learned_window(a, par, depth_plain, time_plain, value_plain) -> dict:
-    """The same window with the learned refinement proposal: a second simulation of the
-    same case with the trained MLP choosing the subtrees the encode and decode visit (judge
-    every --judge-every steps), W warm-up and K timed steps as the plain run's; its
-    active-cell updates/s, and the largest depth difference from the plain run at the end
-    of the window over every finest cell (cell-centre depths)."""
+def par_ending_at(par: str, t_end: float) -> str:
+    """A copy of the case's .par (same folder, so its relative paths hold) with sim_time =
+    t_end: a run of it takes the same steps as the original and shortens its last step to
+    land exactly on t_end (run_simulation.cu:228-235)."""
+    out = os.path.join(os.path.dirname(par), "to_%.9g.par" % t_end)
+    lines = []
+    for line in open(par).read().splitlines():
+        w = line.split()
+        lines.append(f"sim_time {t_end!r}" if w and w[0] == "sim_time" else line)
+    with open(out, "w") as fp:
+        fp.write("\n".join(lines) + "\n")
+    return out
+
+
+def learned_window(a, par, t_from, t_end, depth_plain, value_plain, name) -> dict:
+    """A window of the plain run again with the learned refinement proposal: a second
+    simulation of the same case (ending at t_end, where the plain run's window ended) with the
+    trained MLP choosing the subtrees the step visits (judge every --judge-every steps),
+    stepped untimed to t_from, then W warm-up and K timed steps as the plain window's; its
+    active-cell updates/s, and after stepping on to t_end the largest depth difference from the
+    plain run at t_end over every finest cell (cell-centre depths)."""
     import numpy as np
     import mwdg2_b200
     z = np.load(a.proposal)
     train = json.loads(str(z["summary"]))
-    sim = mwdg2_b200.Simulation(par, precision=a.precision, timing="step")
+    sim = mwdg2_b200.Simulation(par_ending_at(par, t_end), precision=a.precision, timing="step")
     sim.proposal_enable(z["params"], judge_every=a.judge_every, threshold=train["threshold"], miss_bound=0.02)
+    ok = True
+    while ok and sim.info()["time"] < t_from:
+        ok = sim.step()[0]
     for _ in range(a.warmup):
-        sim.step()
+        ok = ok and sim.step()[0]
     ms, leaves = [], []
-    for _ in range(a.steps):
-        ok, dt, n = sim.step()
-        ms.append(float(sim.last_step_timing()[7]))
-        leaves.append(n)
+    with nvtx_range(name):
+        for _ in range(a.steps):
+            ok, dt, n = sim.step()
+            if not ok:
+                break
+            ms.append(float(sim.last_step_timing()[7]))
+            leaves.append(n)
     st = sim.proposal_stats()
+    while ok:
+        ok = sim.step()[0]
     diff = float(np.max(np.abs(finest_depth(sim) - depth_plain)))
-    t_end = sim.info()["time"]
+    t_done = sim.info()["time"]
     sim.close()
     v = sum(leaves) / (sum(ms) / 1e3)
-    return {"value": v, "ms_per_step": sum(ms) / a.steps, "vs_plain": v / value_plain,
-            "max_depth_diff_vs_plain_m": diff, "time": t_end, "plain_time": time_plain,
+    return {"value": v, "ms_per_step": sum(ms) / len(ms), "steps": len(ms), "vs_plain": v / value_plain,
+            "max_depth_diff_vs_plain_m": diff, "compared_at_time": t_done, "plain_time": t_end,
             "proposal": {k: st[k] for k in ("active", "proposed", "subtrees", "learned_steps", "judge_steps",
-                                             "fallbacks")},
+                                             "fallbacks", "frozen_leaves")},
             "mlp": os.path.basename(a.proposal), "judge_every": a.judge_every,
-            "timing": "device time of each step (CUDA events), steps W+1..W+K of a second run of the same case"}
+            "timing": "device time of each step (CUDA events) of a second run of the same case, the plain "
+                      "window's W warm-up and K timed steps from its start time"}
 
 
 def run_learned(a):
@@ -568,18 +619,20 @@ def main():
     barrier()
     t_sim0 = sim.info()["time"]
     ms_step, leaves, counters = [], [], []
-    for _ in range(a.steps):
-        ok, dt, n = sim.step()
-        ms_step.append(float(sim.last_step_timing()[7]))
-        leaves.append(n)
-        counters.append(sim.last_step_counters())
+    with nvtx_range("timed_window"):
+        for _ in range(a.steps):
+            ok, dt, n = sim.step()
+            ms_step.append(float(sim.last_step_timing()[7]))
+            leaves.append(n)
+            counters.append(sim.last_step_counters())
     barrier()
     sim_s = sim.info()["time"] - t_sim0
     tot_ms = max_over_ranks(float(sum(ms_step)), dist, "cuda")
     value = replica_throughput(world, sum(leaves), tot_ms)
     learned = None
-    if world == 1 and a.workload == "catchment" and a.solver == "mwdg2" and os.path.exists(a.proposal):
-        learned = learned_window(a, par, finest_depth(sim), sim.info()["time"], value)
+    want_learned = world == 1 and a.workload == "catchment" and a.solver == "mwdg2" and os.path.exists(a.proposal)
+    if want_learned:
+        learned = learned_window(a, par, 0.0, sim.info()["time"], finest_depth(sim), value, "learned_window")
 
     # end to end through the C ABI: each step's inputs (point-source values) go host->device
     # from pinned memory inside mwdg2_step, its scalars come back, and the stage-point
@@ -679,7 +732,11 @@ def main():
     if learned is not None:
         line["learned"] = learned
     if a.workload == "catchment" and a.peak_time > 0:
-        line["window_peak"] = peak_window(sim, a, dist)
+        wp = peak_window(sim, a, dist)
+        t_end, depth_end = wp.pop("_end_time", None), wp.pop("_end_depth", None)
+        line["window_peak"] = wp
+        if want_learned and "value" in wp:
+            wp["learned"] = learned_window(a, par, a.peak_time, t_end, depth_end, wp["value"], "learned_peak_window")
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(par, a, a.cpu_steps)
     sim.close()

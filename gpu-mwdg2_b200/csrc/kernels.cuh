@@ -33,6 +33,9 @@ template <typename T> struct Leaves
     int32_t* nb[4];
     uint8_t* nbl[4];
     T* un[9];   // [field*3 + mode], field h, qx, qy
+    // learned refinement proposal (null otherwise): same[i] = 1 where position i holds the
+    // leaf it held in the last step (k_tile_emit), so un[i] already holds that leaf's state
+    uint8_t* same;
 };
 
 template <typename T> struct Scalars
@@ -41,16 +44,18 @@ template <typename T> struct Scalars
     T max_h2;                         // max |h0| for the stage-2 limiter (not floored)
     T dt_min;
     int32_t n_leaves;
-    int32_t status;                   // bit 0: NaN seen in the state
+    int32_t status;                   // bit 0: NaN seen in the state; bit 1: a proposal wait ran out
     unsigned long long enc, enc2, dec;
     uint32_t sig_level[16];           // significant parents decoded per level (levels above the bands)
     int32_t wet[2];                   // leaves not dry in RK stage 1 / stage 2 (wet-list lengths)
     T next_max[4];                    // maxima of the state at the end of the step (eta, h, qx, z)
     T xs_factor;                      // 2^(M_BAR+1) of the extra-significance threshold (extra_eps)
     int32_t min_leaf;                 // lowest leaf level of this step's tree (k_tile_emit)
+    int32_t n_prev;                   // the last step's leaf count (k_tile_scan, before it writes n_leaves)
     // learned refinement proposal (csrc/proposal.cuh): subtrees of the proposal level that
-    // were active in the step, active but not proposed, and proposed
-    uint32_t prop_active, prop_missed, prop_proposed;
+    // were active in the step, left out though they needed the step, proposed, and needed
+    uint32_t prop_active, prop_missed, prop_proposed, prop_needed;
+    uint32_t prop_frozen;             // dry leaves of left-out subtrees the RK stages left as they stood
 };
 
 // The subtrees below the nodes of level `level` (the proposal level) that a step's encode and
@@ -60,6 +65,28 @@ struct PropMask
     const uint8_t* prop;
     int level;
 };
+
+
+// A band CTA (node blockIdx.x of level lo and its subtree) holding no node of the mask's
+// level that the proposal kept: like the parents of a subtree the level kernels leave out,
+// its parents keep their flags and values (PM semantics extended to the levels above the
+// mask). Checked for masks at most 7 levels below lo (4^7 bytes per CTA); called by every
+// thread of the CTA.
+__device__ __forceinline__ bool band_left_out(const PropMask& pm, int lo)
+{
+    if (!pm.prop || pm.level < lo || pm.level - lo > 7) return false;
+    const int sh = 2 * (pm.level - lo), n = 1 << sh;
+    const int64_t first = (int64_t)blockIdx.x << sh;
+    bool any = false;
+    if (n >= 4)
+    {
+        const uint32_t* w = reinterpret_cast<const uint32_t*>(pm.prop + first);
+        for (int i = threadIdx.x; i < n / 4; i += blockDim.x) any |= (w[i] != 0u);
+    }
+    else
+        for (int i = threadIdx.x; i < n; i += blockDim.x) any |= (pm.prop[first + i] != 0);
+    return __syncthreads_or(any ? 1 : 0) == 0;
+}
 
 template <typename T> struct Params
 {
@@ -170,6 +197,8 @@ template <typename T> __device__ __forceinline__ void step_begin(Scalars<T>* sc,
     sc->prop_active = 0;
     sc->prop_missed = 0;
     sc->prop_proposed = 0;
+    sc->prop_needed = 0;
+    sc->prop_frozen = 0;
 }
 template <typename T> __global__ void k_step_begin(Scalars<T>* sc, bool carry) { step_begin(sc, carry); }
 
@@ -187,7 +216,7 @@ template <typename T> __device__ __forceinline__ void point_source(const Hier<T>
 // device memory for the later kernels, and applies the point sources, whose values it also
 // reads from pinned host memory. One launch in place of two copies and two kernels.
 template <typename T>
-__global__ void k_step_open(Scalars<T>* sc, bool carry, const StepArgs<T>* h_args, StepArgs<T>* d_args, const Src<T>* h_src,
+__device__ __forceinline__ void k_step_open_body(Scalars<T>* sc, bool carry, const StepArgs<T>* h_args, StepArgs<T>* d_args, const Src<T>* h_src,
                             int nsrc, Hier<T> hr, T dx, int L)
 {
     __shared__ T s_dt;
@@ -204,6 +233,12 @@ __global__ void k_step_open(Scalars<T>* sc, bool carry, const StepArgs<T>* h_arg
     __syncthreads();
     if ((int)threadIdx.x < nsrc) point_source(hr, first, s_dt, dx, L);
     for (int i = threadIdx.x + blockDim.x; i < nsrc; i += blockDim.x) point_source(hr, h_src[i], s_dt, dx, L);
+}
+template <typename T>
+__global__ void k_step_open(Scalars<T>* sc, bool carry, const StepArgs<T>* h_args, StepArgs<T>* d_args, const Src<T>* h_src,
+                            int nsrc, Hier<T> hr, T dx, int L)
+{
+    k_step_open_body<T>(sc, carry, h_args, d_args, h_src, nsrc, hr, dx, L);
 }
 
 // Maxima of the leaf state (mra/get_max_scale_coeffs.cu:3-27, with the reference's
@@ -390,7 +425,7 @@ constexpr int kBandMaxLevel = 9;
 // does) before the parent itself: a child's data is touched by its parent's thread only,
 // and the sparse level needs no launch (and no scan of its flags) of its own.
 template <typename T, bool MW, bool FULL, bool FOLD = false, bool PM = false>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 6 : 4) k_encode_level(Hier<T> hr, Scalars<T>* sc, int L, int level, T eps,
+__device__ __forceinline__ void k_encode_level_body(Hier<T> hr, Scalars<T>* sc, int L, int level, T eps,
                                                                          PropMask pm = PropMask{})
 {
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
@@ -426,6 +461,12 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 6 : 4) k_encode_level(Hi
     }
     const unsigned tot = __reduce_add_sync(0xffffffffu, done);
     if ((threadIdx.x & 31) == 0 && tot) atomicAdd(FULL ? &sc->enc : &sc->enc2, (unsigned long long)tot);
+}
+template <typename T, bool MW, bool FULL, bool FOLD = false, bool PM = false>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 6 : 4) k_encode_level(Hier<T> hr, Scalars<T>* sc, int L, int level, T eps,
+                                                                         PropMask pm = PropMask{})
+{
+    k_encode_level_body<T, MW, FULL, FOLD, PM>(hr, sc, L, level, eps, pm);
 }
 
 // One field of one significant parent's encode: its scale coefficients (stored) and, for
@@ -480,9 +521,11 @@ __device__ __forceinline__ T encode_field(const Hier<T>& hr, const Scalars<T>* s
 // loads); the fields' detail norms meet in shared memory and are combined in field order,
 // as encode_parent combines them, before the flags.
 template <typename T, bool MW, bool FULL>
-__global__ void __launch_bounds__(256) k_encode_band(Hier<T> hr, Scalars<T>* sc, int L, int lo, int depth, T eps)
+__device__ __forceinline__ void k_encode_band_body(Hier<T> hr, Scalars<T>* sc, int L, int lo, int depth, T eps,
+                                                     PropMask pm = PropMask{})
 {
     if (!FULL && sc->min_leaf > lo + depth - 1) return;   // see scale_only_needed
+    if (band_left_out(pm, lo)) return;
     static_assert(kBandDepth <= 5, "a band level has at most 4^(kBandDepth - 1) <= 256 parents");
     __shared__ T s_nd[3][256];
     unsigned done = 0;
@@ -524,6 +567,12 @@ __global__ void __launch_bounds__(256) k_encode_band(Hier<T> hr, Scalars<T>* sc,
     }
     const unsigned tot = __reduce_add_sync(0xffffffffu, done);
     if ((threadIdx.x & 31) == 0 && tot) atomicAdd(FULL ? &sc->enc : &sc->enc2, (unsigned long long)tot);
+}
+template <typename T, bool MW, bool FULL>
+__global__ void __launch_bounds__(256) k_encode_band(Hier<T> hr, Scalars<T>* sc, int L, int lo, int depth, T eps,
+                                                     PropMask pm = PropMask{})
+{
+    k_encode_band_body<T, MW, FULL>(hr, sc, L, lo, depth, eps, pm);
 }
 
 // Decode one significant parent into its four children (mra/decoding_kernel_{mw,hw}.cu)
@@ -673,8 +722,10 @@ __device__ __forceinline__ T decode_field(const Hier<T>& hr, const Scalars<T>* s
 // one thread per parent and field (see k_encode_band); the fields' detail norms are combined
 // in field order, as decode_parent combines them, for extra significance.
 template <typename T, bool MW>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4) k_decode_band(Hier<T> hr, Scalars<T>* sc, int L, int lo, int depth, T eps)
+__device__ __forceinline__ void k_decode_band_body(Hier<T> hr, Scalars<T>* sc, int L, int lo, int depth, T eps,
+                                                                                 PropMask pm = PropMask{})
 {
+    if (band_left_out(pm, lo)) return;
     static_assert(kBandDepth <= 5, "a band level has at most 4^(kBandDepth - 1) <= 256 parents");
     __shared__ T s_nd[3][256];
     unsigned done = 0;
@@ -708,6 +759,12 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4) k_decode_band(Hie
     const unsigned tot = __reduce_add_sync(0xffffffffu, done);
     if ((threadIdx.x & 31) == 0 && tot) atomicAdd(&sc->dec, (unsigned long long)tot);
 }
+template <typename T, bool MW>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4) k_decode_band(Hier<T> hr, Scalars<T>* sc, int L, int lo, int depth, T eps,
+                                                                                 PropMask pm = PropMask{})
+{
+    k_decode_band_body<T, MW>(hr, sc, L, lo, depth, eps, pm);
+}
 
 // Extra significance of one level of parents from their flags (levels above kBandMaxLevel,
 // level <= L - 2): a significant parent makes its children significant when its encode set
@@ -715,7 +772,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4) k_decode_band(Hie
 // Four parents per thread (one aligned flag word). The flags are final after this, so the
 // leaf topology can run beside the value decode of the level (k_decode_level).
 template <typename T>
-__global__ void __launch_bounds__(256) k_extra_sig_level(uint8_t* flags, const Scalars<T>* sc, int L, int level, T eps)
+__device__ __forceinline__ void k_extra_sig_level_body(uint8_t* flags, const Scalars<T>* sc, int L, int level, T eps)
 {
     const int w = blockIdx.x * blockDim.x + threadIdx.x;
     if (w >= (1 << (2 * level - 2))) return;
@@ -731,11 +788,16 @@ __global__ void __launch_bounds__(256) k_extra_sig_level(uint8_t* flags, const S
         if (xs) *reinterpret_cast<uint32_t*>(flags + lvl_idx(level + 1) + 4 * (4 * w + j)) |= 0x01010101u;
     }
 }
+template <typename T>
+__global__ void __launch_bounds__(256) k_extra_sig_level(uint8_t* flags, const Scalars<T>* sc, int L, int level, T eps)
+{
+    k_extra_sig_level_body<T>(flags, sc, L, level, eps);
+}
 
 // One level of parents (levels above kBandMaxLevel), values only (k_extra_sig_level set the
 // children's flags).
 template <typename T, bool MW, bool PM = false>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4) k_decode_level(Hier<T> hr, Scalars<T>* sc, int L, int level, T eps,
+__device__ __forceinline__ void k_decode_level_body(Hier<T> hr, Scalars<T>* sc, int L, int level, T eps,
                                                                          PropMask pm = PropMask{})
 {
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
@@ -747,6 +809,12 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4) k_decode_level(Hi
         atomicAdd(&sc->dec, (unsigned long long)tot);
         atomicAdd(&sc->sig_level[level], tot);
     }
+}
+template <typename T, bool MW, bool PM = false>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4) k_decode_level(Hier<T> hr, Scalars<T>* sc, int L, int level, T eps,
+                                                                         PropMask pm = PropMask{})
+{
+    k_decode_level_body<T, MW, PM>(hr, sc, L, level, eps, pm);
 }
 
 // Sparse form of one level (a level whose significant parents were few last step): a
@@ -918,17 +986,22 @@ __device__ __forceinline__ int tile_leaf_count(const uint8_t* flags, int Tl, int
 
 // Tile leaf counts from final flags.
 // static: the header is included by more than one translation unit of the library
-static __global__ void __launch_bounds__(kTileThreads) k_tile_count(const uint8_t* flags, int L, int32_t* counts)
+static __device__ __forceinline__ void k_tile_count_body(const uint8_t* flags, int L, int32_t* counts)
 {
     const int c = tile_leaf_count(flags, L - kTileDepth, (int)blockIdx.x);
     if (threadIdx.x == 0) counts[blockIdx.x] = c;
+}
+static __global__ void __launch_bounds__(kTileThreads) k_tile_count(const uint8_t* flags, int L, int32_t* counts)
+{
+    k_tile_count_body(flags, L, counts);
 }
 
 // Exclusive scan of n tile counts in one block of 1024 threads; total -> sc->n_leaves.
 // Thread t owns a contiguous chunk (read as int4 when chunks are multiples of four; tile
 // counts come in powers of four), warps scan their chunk sums with shuffles, and the 32 warp
 // totals are scanned by one warp.
-template <typename T> __global__ void __launch_bounds__(1024) k_tile_scan(int32_t* counts, int n, Scalars<T>* sc)
+template <typename T>
+__device__ __forceinline__ void k_tile_scan_body(int32_t* counts, int n, Scalars<T>* sc)
 {
     __shared__ int32_t warp_sum[32];
     const int per = (n + 1023) / 1024;
@@ -963,7 +1036,11 @@ template <typename T> __global__ void __launch_bounds__(1024) k_tile_scan(int32_
             if (lane >= o) ti += v;
         }
         warp_sum[lane] = ti - t;   // exclusive prefix of the warp totals
-        if (lane == 31) sc->n_leaves = ti;
+        if (lane == 31)
+        {
+            sc->n_prev = sc->n_leaves;
+            sc->n_leaves = ti;
+        }
     }
     __syncthreads();
     int32_t run = warp_sum[w] + incl - s;   // exclusive prefix of this thread's chunk
@@ -985,6 +1062,11 @@ template <typename T> __global__ void __launch_bounds__(1024) k_tile_scan(int32_
             counts[i] = run;
             run += c;
         }
+}
+template <typename T>
+__global__ void __launch_bounds__(1024) k_tile_scan(int32_t* counts, int n, Scalars<T>* sc)
+{
+    k_tile_scan_body<T>(counts, n, sc);
 }
 
 // Neighbour of a leaf (level l, finest reference cell code `ref`) across the finest cell
@@ -1017,13 +1099,22 @@ __device__ __forceinline__ void leaf_neighbour(const uint8_t* flags, int L, int 
 
 // A tile holding one leaf (the tile's root or the first tile of a coarser leaf): threads
 // 0..3 of the block find one neighbour each.
+// Position pos of the leaf list gets leaf `act`; with lf.same, whether it held that leaf in
+// the last step (n_prev leaves).
+template <typename T>
+__device__ __forceinline__ void put_act(const Leaves<T>& lf, int pos, int act, const int32_t* n_prev)
+{
+    if (lf.same) lf.same[pos] = (pos < *n_prev && lf.act[pos] == act) ? 1 : 0;
+    lf.act[pos] = act;
+}
+
 template <typename T, bool NBL>
 __device__ __forceinline__ void emit_single_leaf(const Leaves<T>& lf, const uint8_t* flags, int L, int M, int xsz,
-                                                 int ysz, int pos, int act, int l)
+                                                 int ysz, int pos, int act, int l, const int32_t* n_prev)
 {
     const int d = threadIdx.x;
     if (d >= 4) return;
-    if (d == 0) { lf.act[pos] = act; lf.lvl[pos] = (uint8_t)l; }
+    if (d == 0) { put_act(lf, pos, act, n_prev); lf.lvl[pos] = (uint8_t)l; }
     int32_t id;
     uint8_t lv;
     leaf_neighbour(flags, L, M, xsz, ysz, act, l, d, id, lv);
@@ -1042,8 +1133,9 @@ __device__ __forceinline__ void emit_single_leaf(const Leaves<T>& lf, const uint
 // NBL: also write the neighbours' levels (lf.nbl), which level_of(id) gives wherever the id
 // is not -1 (-1: the leaf's own level).
 template <typename T, bool NBL>
-__global__ void __launch_bounds__(kTileThreads, 8) k_tile_emit(Leaves<T> lf, const uint8_t* flags, const int32_t* offsets,
-                                                            int L, int M, int xsz, int ysz, int32_t* min_leaf)
+__device__ __forceinline__ void k_tile_emit_body(Leaves<T> lf, const uint8_t* flags, const int32_t* offsets,
+                                                            int L, int M, int xsz, int ysz, int32_t* min_leaf,
+                                                            const int32_t* n_prev)
 {
     constexpr int D = kTileDepth, kCells = 1 << (2 * D);
     const int Tl = L - D;
@@ -1066,14 +1158,14 @@ __global__ void __launch_bounds__(kTileThreads, 8) k_tile_emit(Leaves<T> lf, con
         if ((tcode & ((1 << (2 * (Tl - k))) - 1)) == 0)
         {
             if (min_leaf && threadIdx.x == 0) atomicMin(min_leaf, k);
-            emit_single_leaf<T, NBL>(lf, flags, L, M, xsz, ysz, off, lvl_idx(k) + (tcode >> (2 * (Tl - k))), k);
+            emit_single_leaf<T, NBL>(lf, flags, L, M, xsz, ysz, off, lvl_idx(k) + (tcode >> (2 * (Tl - k))), k, n_prev);
         }
         return;
     }
     if (k == Tl)
     {
         if (min_leaf && threadIdx.x == 0) atomicMin(min_leaf, Tl);
-        emit_single_leaf<T, NBL>(lf, flags, L, M, xsz, ysz, off, lvl_idx(Tl) + tcode, Tl);
+        emit_single_leaf<T, NBL>(lf, flags, L, M, xsz, ysz, off, lvl_idx(Tl) + tcode, Tl, n_prev);
         return;
     }
     if (threadIdx.x < 85)
@@ -1173,7 +1265,7 @@ __global__ void __launch_bounds__(kTileThreads, 8) k_tile_emit(Leaves<T> lf, con
         const int sh = 2 * (L - lev);
         const unsigned gc = tbase + (unsigned)c;       // finest code of the leaf's south-west cell
         const int pos = off + r;
-        lf.act[pos] = lvl_idx(lev) + (int)(gc >> sh);
+        put_act(lf, pos, lvl_idx(lev) + (int)(gc >> sh), n_prev);
         lf.lvl[pos] = (uint8_t)lev;
         const unsigned X0 = gc & kXBits, Y0 = gc & kYBits;            // dilated x0, y0
         const unsigned span = (1u << sh) - 1u;                         // dilated (size - 1) in both
@@ -1202,6 +1294,13 @@ __global__ void __launch_bounds__(kTileThreads, 8) k_tile_emit(Leaves<T> lf, con
             if (NBL) lf.nbl[d][pos] = (uint8_t)lv;
         }
     }
+}
+template <typename T, bool NBL>
+__global__ void __launch_bounds__(kTileThreads, 8) k_tile_emit(Leaves<T> lf, const uint8_t* flags, const int32_t* offsets,
+                                                            int L, int M, int xsz, int ysz, int32_t* min_leaf,
+                                                            const int32_t* n_prev)
+{
+    k_tile_emit_body<T, NBL>(lf, flags, offsets, L, M, xsz, ysz, min_leaf, n_prev);
 }
 
 // Initial leaf list: every finest cell, in Z order.

@@ -91,7 +91,7 @@ extern "C" mwdg2_status mwdg2_leaf_topology_static(const uint8_t* d_sig, int max
         lf.nbl[d] = d_nb_levels + (size_t)d * cap;
     }
     mw::k_tile_emit<float, true><<<ntiles, mw::kTileThreads, 0, st>>>(lf, d_sig, scratch->tile_counts, max_ref_lvl, M, xsz,
-                                                                ysz, nullptr);
+                                                                ysz, nullptr, nullptr);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(MWDG2_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
     int32_t n = 0;

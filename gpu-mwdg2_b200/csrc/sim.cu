@@ -16,6 +16,7 @@
 #include "outputs.cuh"
 #include "proposal_sim.cuh"
 #include "solver.cuh"
+#include "batch.cuh"
 
 #include <algorithm>
 #include <cerrno>
@@ -85,6 +86,9 @@ struct SimBase
     virtual mwdg2_status proposal_samples(const void** feats, const uint8_t** labels, int64_t* n, int* device) = 0;
     virtual mwdg2_status proposal_samples_host(float* feats, uint8_t* labels, int64_t cap, int64_t* n) = 0;
     virtual mwdg2_status proposal_mask(uint8_t* out, int64_t cap, int64_t* n) = 0;
+    // batched ensembles: members with the same key (>= 0) step together in one launch per
+    // kernel (Group); -1: this simulation steps on its own
+    virtual int group_key() const = 0;
 };
 
 template <typename T> class Sim final : public SimBase
@@ -98,6 +102,13 @@ public:
     mwdg2_status enqueue_step() override;
     mwdg2_status finish_step(double* dt_out, int64_t* n_out) override;
     bool first_step() const override { return first_; }
+    int group_key() const override
+    {
+        const bool ok = mw_ && !first_ && !finished_ && cs_.epsilon > T(0) && !prop_on() && timing_mode_ == 0 &&
+                        m_args_ && (cs_.srcs.empty() || m_src_) && cs_.stage_codes.size() <= 64;
+        return ok ? (L_ | (sizeof(T) == 8 ? 1 << 8 : 0)) : -1;
+    }
+    template <typename U> friend class Group;
     mwdg2_status prepare_outputs() override;
     mwdg2_status after_step(bool first, double dt, int64_t n, double step_seconds) override;
     void anchor_outputs(const std::string& dir) override
@@ -169,7 +180,12 @@ private:
     // Per-leaf kernels run persistent grids (grid-stride loops): SMs x resident blocks of each
     // kernel, so a step's launches do not depend on the leaf count and can be replayed.
     int grid_leaf_ = 0, grid_wet_ = 0, grid_dry_ = 0, grid_stage_ = 0;
-    uint8_t* dry_ = nullptr;            // dry marks of one RK stage (k_stage_wet -> k_stage_dry)
+    uint8_t* dry_ = nullptr;            // dry marks of RK stage 1 (k_stage_wet -> k_stage_dry)
+    uint8_t* dry2_ = nullptr;           // and of stage 2
+    // learned proposal: leaves dry in both stages of the last step (k_stage_wet<2>), valid
+    // (clean_ok_) when both stages of that step took the wet list
+    uint8_t* clean_ = nullptr;
+    bool step_lists_ = false, clean_ok_ = false;
     cudaStream_t st2_ = nullptr;        // the wet-list kernels, beside the dry-leaf writers
     cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
     // the value decode of the levels above the bands, beside the leaf topology (its own
@@ -193,7 +209,7 @@ private:
     {
         int key = (mw_ && use_list(1) ? 1 : 0) | (mw_ && use_list(2) ? 2 : 0) | (timed_ ? 1 << 24 : 0) |
                   (!mw_ && flip_ ? 1 << 23 : 0) | (prop_rec_ ? 1 << 22 : 0) | (prop_learned_ ? 1 << 21 : 0) |
-                  (prop_apply_ ? 1 << 20 : 0);
+                  (prop_apply_ ? 1 << 20 : 0) | (clean_ok_ ? 1 << 19 : 0);
         for (int level = mw::kBandMaxLevel + 1; level < L_; ++level)
             if (sparse_level(level)) key |= 4 << (level - mw::kBandMaxLevel - 1);
         return key;
@@ -230,6 +246,7 @@ private:
     int64_t prop_nC_ = 0;
     __nv_bfloat16* d_feat_ = nullptr;   // [4^C][128] features of the step's start
     uint8_t* d_lab_ = nullptr;          // [4^C] activity bits of the children in the last step
+    uint16_t* d_ring_ = nullptr;        // [4^C / 128] tile summaries of d_lab_ (mw::ring_bits)
     uint8_t* d_act_ = nullptr;          // [4^(C+1)] activity marks of this step
     uint8_t* d_prop_ = nullptr;         // [4^(C+1)] proposal of this step
     uint8_t* d_sig5_ = nullptr;         // [4^(C+1)] flags of each subtree's two parent levels, last step
@@ -239,7 +256,7 @@ private:
     float prop_thr_ = 0.0f, prop_bound_ = 0.0f;
     int prop_judge_every_ = 0, prop_since_judge_ = 0, prop_fallback_left_ = 0;
     int64_t prop_learned_steps_ = 0, prop_judge_steps_ = 0, prop_fallbacks_ = 0;
-    double prop_last_[4] = {0, 0, 0, 0};      // active, missed, proposed, applied (last step)
+    double prop_last_[6] = {0, 0, 0, 0, 0, 0};   // active, missed, proposed, applied, frozen leaves, needed
     double prop_judge_rate_ = 0.0;            // missed / active at the last judge step
     mwdg2_status prop_alloc();
     // outputs
@@ -258,6 +275,7 @@ private:
     void release();
     mwdg2_status launch_step();    // enqueue only (graph replay or direct launches)
     mwdg2_status launch_step_device();
+    void prepare_args();           // this step's dt, boundary and point-source values (host)
     mwdg2_status enqueue_device(); // the step's device work, on st_
     mwdg2_status collect_step();   // wait, timing, counters
     // One MWDG2 RK stage. When fewer than half of the leaves were wet in this stage last
@@ -275,12 +293,18 @@ private:
     {
         if (use_list(STAGE))
         {
-            mw::k_stage_wet<T, STAGE><<<grid_wet_, 256, 0, st_>>>(lf_, hin, sc_, P_, d_args_, dry_, wet_list_);
+            uint8_t* marks = STAGE == 1 ? dry_ : dry2_;
+            // learned proposal: stage 2 records which leaves stayed dry in both stages (clean_),
+            // and leaves left out by the proposal are frozen only when both stages take the list
+            const mw::PropMask pm = (use_list(1) && use_list(2)) ? prop_mask() : mw::PropMask{};
+            mw::k_stage_wet<T, STAGE><<<grid_wet_, 256, 0, st_>>>(lf_, hin, sc_, P_, d_args_, marks, wet_list_, dry_,
+                                                                  STAGE == 2 ? clean_ : nullptr);
             cudaEventRecord(ev_fork_, st_);
             cudaStreamWaitEvent(st2_, ev_fork_, 0);
             mw::k_mwdg2_stage<T, STAGE, true><<<grid_stage_, mw::kSolverThreads, 0, st2_>>>(lf_, hin, hout, sc_, P_,
                                                                                            d_args_, fric, wet_list_);
-            mw::k_stage_dry<T, STAGE><<<grid_dry_, 256, 0, st_>>>(lf_, hin, hout, sc_, P_, fric, dry_);
+            mw::k_stage_dry<T, STAGE><<<grid_dry_, 256, 0, st_>>>(lf_, hin, hout, sc_, P_, fric, marks, dry_, pm,
+                                                                  STAGE == 1 && clean_ok_ ? clean_ : nullptr);
             cudaEventRecord(ev_join_, st2_);
             cudaStreamWaitEvent(st_, ev_join_, 0);
             launches_ += 3;
@@ -333,7 +357,7 @@ private:
         }
         for (const Band& b : bands_)
         {
-            if (mw_) mw::k_encode_band<T, true, FULL><<<b.grid, 256, 0, st_>>>(h, sc_, L_, b.lo, b.depth, eps);
+            if (mw_) mw::k_encode_band<T, true, FULL><<<b.grid, 256, 0, st_>>>(h, sc_, L_, b.lo, b.depth, eps, pm);
             else mw::k_encode_band<T, false, FULL><<<b.grid, 256, 0, st_>>>(h, sc_, L_, b.lo, b.depth, eps);
             ++launches_;
         }
@@ -458,6 +482,7 @@ template <typename T> mwdg2_status Sim<T>::init(const char* par, const mwdg2_opt
     {
         char* block = nullptr;
         if (mwdg2_status s = dalloc(block, scal_bytes_)) return s;
+        CU(cudaMemset(block, 0, scal_bytes_));
         sc_ = reinterpret_cast<mw::Scalars<T>*>(block);
         if (nst > 0) d_stage_out_ = reinterpret_cast<T*>(block + stage_off);
         char* hblock = nullptr;
@@ -470,6 +495,7 @@ template <typename T> mwdg2_status Sim<T>::init(const char* par, const mwdg2_opt
     {
         if (mwdg2_status s = dalloc(wet_list_, F_)) return s;
         if (mwdg2_status s = dalloc(dry_, F_)) return s;
+        if (mwdg2_status s = dalloc(dry2_, F_)) return s;
         CU(cudaStreamCreateWithFlags(&st2_, cudaStreamNonBlocking));
         CU(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming));
         CU(cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming));
@@ -595,10 +621,10 @@ template <typename T> mwdg2_status Sim<T>::launch_step()
     return st;
 }
 
-template <typename T> mwdg2_status Sim<T>::launch_step_device()
+// host-side values of this step: point-source values (classes/PointSources.h:453-472)
+// and boundary inlets (classes/Boundaries.h:28-39) at the current time, and dt
+template <typename T> void Sim<T>::prepare_args()
 {
-    // host-side values of this step: point-source values (classes/PointSources.h:453-472)
-    // and boundary inlets (classes/Boundaries.h:28-39) at the current time, and dt
     for (auto& src : cs_.srcs)
         if (src.varying) src.value = src.series.at(time_);
     for (int i = 0; i < (int)cs_.srcs.size(); ++i)
@@ -607,6 +633,12 @@ template <typename T> mwdg2_status Sim<T>::launch_step_device()
         if (cs_.bnd[d].varying) cs_.bnd[d].inlet = cs_.bnd[d].series.at(time_);
     h_args_->dt = dt_;
     h_args_->B = bnd_now();
+}
+
+template <typename T> mwdg2_status Sim<T>::launch_step_device()
+{
+    prepare_args();
+    step_lists_ = mw_ && !first_ && use_list(1) && use_list(2);
     // step timing: stream events right around the step's device work (after any capture)
     auto rec_step = [&](int k) { if (timing_mode_ == 1) cudaEventRecord(ev_step_[k], st_); };
     auto direct = [&]() {
@@ -713,7 +745,8 @@ template <typename T> mwdg2_status Sim<T>::enqueue_device()
         else if (prop_learned_ && prop_nC_ >= mlp::kRows)
         {
             mw::k_mlp_propose<T><<<g, mlp::kRows, mw::ProposeSmem<T>::Total + 1024, st_>>>(d_mlp_pack_, hr_, prop_C_, d_lab_,
-                                                                                        d_prop_, prop_thr_, d_mlp_err_);
+                                                                                        d_ring_, d_prop_, prop_thr_,
+                                                                                        &sc_->status);
             ++launches_;
         }
     }
@@ -724,7 +757,7 @@ template <typename T> mwdg2_status Sim<T>::enqueue_device()
         for (size_t k = bands_.size(); k-- > 0;)  // top band first
         {
             const Band& b = bands_[k];
-            if (mw) mw::k_decode_band<T, true><<<b.grid, 256, 0, st_>>>(hr_, sc_, L_, b.lo, b.depth, eps);
+            if (mw) mw::k_decode_band<T, true><<<b.grid, 256, 0, st_>>>(hr_, sc_, L_, b.lo, b.depth, eps, prop_mask());
             else mw::k_decode_band<T, false><<<b.grid, 256, 0, st_>>>(hr_, sc_, L_, b.lo, b.depth, eps);
             ++launches_;
         }
@@ -774,7 +807,7 @@ template <typename T> mwdg2_status Sim<T>::enqueue_device()
         mw::k_tile_scan<T><<<1, 1024, 0, st_>>>(tile_counts_, ntiles_, sc_);
         ++launches_;
         mw::k_tile_emit<T, false><<<ntiles_, mw::kTileThreads, 0, st_>>>(lf_, hr_.flags, tile_counts_, L_, M_, cs_.xsz, cs_.ysz,
-                                                                        &sc_->min_leaf);
+                                                                        &sc_->min_leaf, &sc_->n_prev);
         ++launches_;
         if (fork)
         {
@@ -805,7 +838,8 @@ template <typename T> mwdg2_status Sim<T>::enqueue_device()
     if (prop_on() && remesh)
     {
         mw::k_prop_labels<<<grid_for(prop_nC_, 256, 2 * (solver_blocks_ / 8)), 256, 0, st_>>>(
-            d_act_, prop_learned_ ? d_prop_ : nullptr, hr_.flags, prop_C_, d_sig5_, d_lab_, prop_nC_, &sc_->prop_active);
+            d_act_, prop_learned_ ? d_prop_ : nullptr, hr_.flags, prop_C_, d_sig5_, d_lab_, d_ring_, prop_nC_,
+            &sc_->prop_active);
         ++launches_;
     }
     // the stage points of the new state come back with the step's scalars
@@ -903,17 +937,27 @@ template <typename T> mwdg2_status Sim<T>::finish_step(double* dt_out, int64_t* 
     if (sc_host_->status & 1) return set_err(MWDG2_ERR_NUMERIC, "NaN in the leaf state");
     if (prop_on())
     {
-        int mlp_err = 0;
-        if (prop_learned_) CU(cudaMemcpy(&mlp_err, d_mlp_err_, sizeof(int), cudaMemcpyDeviceToHost));
-        if (mlp_err) return set_err(MWDG2_ERR_TIMEOUT, "proposal MLP: a tensor-core wait ran out");
+        // the fused kernel reports through the step's status; the recording path's MLP
+        // through its own flag
+        int mlp_err = (sc_host_->status & 2) ? 1 : 0;
+        if (prop_learned_ && prop_rec_) CU(cudaMemcpy(&mlp_err, d_mlp_err_, sizeof(int), cudaMemcpyDeviceToHost));
+        if (mlp_err || (sc_host_->status & 2))
+            return set_err(MWDG2_ERR_TIMEOUT, "proposal MLP: a tensor-core wait ran out");
         const double active = sc_host_->prop_active, missed = sc_host_->prop_missed;
+        const double needed = sc_host_->prop_needed;
         prop_last_[0] = active;
         prop_last_[1] = missed;
         prop_last_[2] = sc_host_->prop_proposed;
+        prop_last_[4] = sc_host_->prop_frozen;
+        prop_last_[5] = needed;
         prop_last_[3] = prop_apply_ ? 1.0 : 0.0;
         if (prop_learned_ && !first_)
         {
-            const double rate = active > 0 ? missed / active : 0.0;
+            const double rate = needed > 0 ? missed / needed : 0.0;
+            // the fallback test counts the misses over at least 0.1 % of all subtrees, so
+            // that one or two misses among the few dozen active subtrees of a starting flood
+            // do not throw the next judge_every steps back to the full step
+            const double floor_rate = missed / std::max(needed, 1e-3 * (double)(prop_nC_ * 4));
             ++prop_since_judge_;
             if (prop_judge_)
             {
@@ -923,7 +967,7 @@ template <typename T> mwdg2_status Sim<T>::finish_step(double* dt_out, int64_t* 
             }
             else if (prop_apply_) ++prop_learned_steps_;
             else if (prop_fallback_left_ > 0) --prop_fallback_left_;
-            if ((prop_judge_ || prop_apply_) && rate > prop_bound_)
+            if ((prop_judge_ || prop_apply_) && floor_rate > prop_bound_)
             {
                 prop_fallback_left_ = prop_judge_every_ > 0 ? prop_judge_every_ : 1;
                 ++prop_fallbacks_;
@@ -932,6 +976,7 @@ template <typename T> mwdg2_status Sim<T>::finish_step(double* dt_out, int64_t* 
     }
     n_leaves_ = sc_host_->n_leaves;
     dt_ = sc_host_->dt_min;
+    clean_ok_ = step_lists_ && clean_ != nullptr;
     first_ = false;
     timestep_++;
     if (dt_out) *dt_out = (double)dt_;
@@ -968,6 +1013,14 @@ template <typename T> mwdg2_status Sim<T>::prop_alloc()
     prop_nC_ = (int64_t)1 << (2 * prop_C_);
     if (mwdg2_status s = dalloc(d_feat_, (size_t)prop_nC_ * mlp::kIn)) return s;
     if (mwdg2_status s = dalloc(d_lab_, (size_t)prop_nC_)) return s;
+    const size_t nring = (size_t)std::max<int64_t>(1, prop_nC_ / mw::kPropTile);
+    if (mwdg2_status s = dalloc(d_ring_, nring)) return s;
+    CU(cudaMemset(d_ring_, 0xff, nring * sizeof(uint16_t)));   // every tile runs until labels exist
+    if (mwdg2_status s = dalloc(lf_.same, F_)) return s;
+    CU(cudaMemset(lf_.same, 0, F_));
+    if (mwdg2_status s = dalloc(clean_, F_)) return s;
+    CU(cudaMemset(clean_, 0, F_));
+    clean_ok_ = false;
     if (mwdg2_status s = dalloc(d_act_, (size_t)prop_nC_ * 4)) return s;
     if (mwdg2_status s = dalloc(d_prop_, (size_t)prop_nC_ * 4)) return s;
     if (mwdg2_status s = dalloc(d_sig5_, (size_t)prop_nC_ * 4)) return s;
@@ -1024,9 +1077,10 @@ mwdg2_status Sim<T>::proposal_enable(const float* params, int judge_every, float
 template <typename T> mwdg2_status Sim<T>::proposal_stats(double* out, int n)
 {
     const double nodes = (double)(prop_nC_ * 4);
-    const double v[10] = {prop_last_[0], prop_last_[1], prop_last_[2], prop_last_[3], nodes, (double)prop_learned_steps_,
-                          (double)prop_judge_steps_, prop_judge_rate_, (double)prop_fallbacks_, (double)prop_fallback_left_};
-    for (int i = 0; i < n && i < 10; ++i) out[i] = v[i];
+    const double v[12] = {prop_last_[0], prop_last_[1], prop_last_[2], prop_last_[3], nodes, (double)prop_learned_steps_,
+                          (double)prop_judge_steps_, prop_judge_rate_, (double)prop_fallbacks_, (double)prop_fallback_left_,
+                          prop_last_[4], prop_last_[5]};
+    for (int i = 0; i < n && i < 12; ++i) out[i] = v[i];
     return MWDG2_OK;
 }
 
@@ -1532,6 +1586,276 @@ void mwdg2_detail_set_last_error(const char* msg) { g_last_error = msg ? msg : "
 mwdg2_status mwdg2_detail_proposal_samples(mwdg2_sim* sim, const void** feats, const uint8_t** labels, int64_t* n,
                                            int* device);
 
+// ============================================================================ batched ensembles
+
+namespace {
+
+// A size class of batch members (same max_ref_lvl, MWDG2, same precision, past their first
+// step): one launch per kernel steps every member of the class (csrc/batch.cuh), the
+// launches captured once into one CUDA graph. The members keep their own state, clocks and
+// outputs (Sim); the group only replaces their launches.
+struct GroupBase
+{
+    virtual ~GroupBase() = default;
+    // Launch one step of the members with stepping[k] (member k of the group; their
+    // begin_step has run); the others are skipped by every kernel.
+    virtual mwdg2_status launch(const std::vector<uint8_t>& stepping) = 0;
+    virtual mwdg2_status wait() = 0;
+    std::vector<int> idx;   // the members' indices in the batch
+    int key = -1;
+};
+
+template <typename T> class Group final : public GroupBase
+{
+public:
+    ~Group() override
+    {
+        if (exec_) cudaGraphExecDestroy(exec_);
+        if (d_tab_) cudaFree(d_tab_);
+        if (d_on_) cudaFree(d_on_);
+        if (d_map_) cudaFree(d_map_);
+        if (h_map_) cudaFreeHost(h_map_);
+        if (h_active_) cudaFreeHost(h_active_);
+        for (auto& e : ev_)
+            if (e) cudaEventDestroy(e);
+        if (st2_) cudaStreamDestroy(st2_);
+        if (st_) cudaStreamDestroy(st_);
+    }
+
+    mwdg2_status build(const std::vector<Sim<T>*>& ms)
+    {
+        ms_ = ms;
+        n_ = (int)ms.size();
+        const Sim<T>& m0 = *ms[0];
+        L_ = m0.L_;
+        ntiles_ = m0.ntiles_;
+        bands_ = m0.bands_;
+        CU(cudaSetDevice(m0.device_));
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m0.device_);
+        // per-leaf launches: the device's resident blocks of the kernel, shared among the
+        // members by the block maps (plus one block per member, the rounding's room)
+        auto capacity = [&](auto kernel, int threads) {
+            int b = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, threads, 0) != cudaSuccess || b < 1) b = 1;
+            return sms * b;
+        };
+        cap_wet_ = capacity(mw::k_members_stage_wet<T, 1>, 256);
+        cap_dry_ = capacity(mw::k_members_stage_dry<T, 1>, 256);
+        cap_list_ = capacity(mw::k_members_stage_list<T, 1>, mw::kSolverThreads);
+        cap_leaf_ = capacity(mw::k_members_stage2_maxh<T>, 256);
+        std::vector<mw::MemberArgs<T>> tab(n_);
+        for (int k = 0; k < n_; ++k)
+        {
+            const Sim<T>& m = *ms[k];
+            mw::MemberArgs<T>& a = tab[k];
+            a.sc = m.sc_;
+            a.sc_host = m.sc_host_;
+            a.scal_bytes = (int)m.scal_bytes_;
+            a.m_args = m.m_args_;
+            a.d_args = m.d_args_;
+            a.m_src = m.m_src_;
+            a.nsrc = (int)m.cs_.srcs.size();
+            a.hr = m.hr_;
+            a.hs = m.hs_;
+            a.lf = m.lf_;
+            a.P = m.P_;
+            a.dx = m.cs_.dx;
+            a.eps = m.cs_.epsilon;
+            a.M = m.M_;
+            a.xsz = m.cs_.xsz;
+            a.ysz = m.cs_.ysz;
+            a.tile_counts = m.tile_counts_;
+            a.dry1 = m.dry_;
+            a.dry2 = m.dry2_;
+            a.wet = m.wet_list_;
+            a.fric = m.cs_.manning > T(0) ? 1 : 0;
+            a.limit = m.cs_.limitslopes ? 1 : 0;
+            a.stage_codes = m.d_stage_codes_;
+            a.np = (int)m.cs_.stage_codes.size();
+            a.stage_out = m.d_stage_out_;
+            np_max_ = std::max(np_max_, a.np);
+        }
+        CU(cudaMalloc(&d_tab_, sizeof(mw::MemberArgs<T>) * n_));
+        CU(cudaMemcpy(d_tab_, tab.data(), sizeof(mw::MemberArgs<T>) * n_, cudaMemcpyHostToDevice));
+        CU(cudaMalloc(&d_on_, n_));
+        const size_t nmap = (size_t)mw::kBlockMaps * (n_ + 1);
+        CU(cudaMalloc(&d_map_, sizeof(int32_t) * nmap));
+        CU(cudaHostAlloc(&h_map_, sizeof(int32_t) * nmap, cudaHostAllocMapped));
+        CU(cudaHostGetDevicePointer(reinterpret_cast<void**>(&m_map_), h_map_, 0));
+        CU(cudaHostAlloc(&h_active_, n_, cudaHostAllocMapped));
+        CU(cudaHostGetDevicePointer(reinterpret_cast<void**>(&m_active_), h_active_, 0));
+        CU(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+        CU(cudaStreamCreateWithFlags(&st2_, cudaStreamNonBlocking));
+        for (auto& e : ev_) CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        return MWDG2_OK;
+    }
+
+    mwdg2_status launch(const std::vector<uint8_t>& stepping) override
+    {
+        CU(cudaSetDevice(ms_[0]->device_));
+        for (int k = 0; k < n_; ++k)
+        {
+            h_active_[k] = stepping[k];
+            if (stepping[k]) ms_[k]->prepare_args();
+        }
+        // the block maps from the members' last step: leaves; wet leaves of stage 1 and 2
+        for (int map = 0; map < mw::kBlockMaps; ++map)
+        {
+            const int cap = map == 0 ? std::min(cap_wet_, std::min(cap_dry_, cap_leaf_)) : cap_list_;
+            std::vector<double> w(n_, 0.0);
+            double tot = 0;
+            for (int k = 0; k < n_; ++k)
+                if (stepping[k])
+                {
+                    const Sim<T>& m = *ms_[k];
+                    w[k] = map == 0 ? (double)std::max<int64_t>(1, m.n_leaves_)
+                                    : (double)std::max<int64_t>(1, m.wet_prev_[map - 1] + 1);
+                    tot += w[k];
+                }
+            int32_t* first = h_map_ + map * (n_ + 1);
+            int32_t b = 0;
+            for (int k = 0; k < n_; ++k)
+            {
+                first[k] = b;
+                if (stepping[k]) b += std::max(1, (int)(cap * (w[k] / tot)));
+            }
+            first[n_] = b;   // at most cap + n_
+        }
+        if (!exec_)
+        {
+            cudaGraph_t g = nullptr;
+            CU(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+            launches_ = 0;
+            enqueue();
+            const cudaError_t e = cudaStreamEndCapture(st_, &g);
+            if (e != cudaSuccess) return set_err(MWDG2_ERR_CUDA, std::string("batch group capture: ") + cudaGetErrorString(e));
+            const cudaError_t e2 = cudaGraphInstantiate(&exec_, g, 0);
+            cudaGraphDestroy(g);
+            if (e2 != cudaSuccess) return set_err(MWDG2_ERR_CUDA, std::string("batch group graph: ") + cudaGetErrorString(e2));
+        }
+        for (int k = 0; k < n_; ++k)
+            if (stepping[k]) ms_[k]->launches_ = launches_;
+        CU(cudaGraphLaunch(exec_, st_));
+        return MWDG2_OK;
+    }
+
+    mwdg2_status wait() override
+    {
+        CU(cudaStreamSynchronize(st_));
+        return MWDG2_OK;
+    }
+
+private:
+    static int blocks(int64_t n, int threads)
+    {
+        const int64_t b = (n + threads - 1) / threads;
+        return (int)std::max<int64_t>(1, std::min<int64_t>(b, 1 << 30));
+    }
+    void fork(cudaEvent_t e)
+    {
+        cudaEventRecord(e, st_);
+        cudaStreamWaitEvent(st2_, e, 0);
+    }
+    void join(cudaEvent_t e)
+    {
+        cudaEventRecord(e, st2_);
+        cudaStreamWaitEvent(st_, e, 0);
+    }
+    template <bool FULL> void encode()
+    {
+        for (int level = L_ - 1; level > mw::kBandMaxLevel; --level)
+        {
+            mw::k_members_encode_level<T, FULL><<<dim3(blocks((int64_t)1 << (2 * level), 256), n_), 256, 0, st_>>>(
+                d_tab_, d_on_, L_, level);
+            ++launches_;
+        }
+        for (const auto& b : bands_)
+        {
+            mw::k_members_encode_band<T, FULL><<<dim3(b.grid, n_), 256, 0, st_>>>(d_tab_, d_on_, L_, b.lo, b.depth);
+            ++launches_;
+        }
+    }
+    template <int STAGE> void stage()
+    {
+        const int32_t* leaves = d_map_;
+        const int32_t* wet = d_map_ + STAGE * (n_ + 1);
+        const int g = std::min(cap_wet_, std::min(cap_dry_, cap_leaf_)) + n_;
+        mw::k_members_stage_wet<T, STAGE><<<g, 256, 0, st_>>>(d_tab_, d_on_, leaves, n_);
+        fork(ev_[2]);
+        mw::k_members_stage_list<T, STAGE><<<cap_list_ + n_, mw::kSolverThreads, 0, st2_>>>(d_tab_, d_on_, wet, n_);
+        mw::k_members_stage_dry<T, STAGE><<<g, 256, 0, st_>>>(d_tab_, d_on_, leaves, n_);
+        join(ev_[3]);
+        launches_ += 3;
+    }
+    // the launches of one step, in the order of Sim::enqueue_device for a step after the
+    // first with every RK stage over the wet list and no sparse level
+    void enqueue()
+    {
+        mw::k_members_open<T><<<dim3(1, n_), 128, 0, st_>>>(d_tab_, m_active_, d_on_, L_, m_map_, d_map_, n_);
+        ++launches_;
+        encode<true>();
+        for (size_t k = bands_.size(); k-- > 0;)
+        {
+            const auto& b = bands_[k];
+            mw::k_members_decode_band<T><<<dim3(b.grid, n_), 256, 0, st_>>>(d_tab_, d_on_, L_, b.lo, b.depth);
+            ++launches_;
+        }
+        for (int level = mw::kBandMaxLevel + 1; level <= L_ - 2; ++level)
+        {
+            mw::k_members_extra_sig<T><<<dim3(blocks((int64_t)1 << (2 * level - 2), 256), n_), 256, 0, st_>>>(
+                d_tab_, d_on_, L_, level);
+            ++launches_;
+        }
+        const bool split = L_ - 1 > mw::kBandMaxLevel;
+        if (split)
+        {
+            fork(ev_[0]);
+            for (int level = mw::kBandMaxLevel + 1; level < L_; ++level)
+            {
+                mw::k_members_decode_level<T><<<dim3(blocks((int64_t)1 << (2 * level), 256), n_), 256, 0, st2_>>>(
+                    d_tab_, d_on_, L_, level);
+                ++launches_;
+            }
+        }
+        mw::k_members_tile_count<T><<<dim3(ntiles_, n_), 96, 0, st_>>>(d_tab_, d_on_, L_);
+        mw::k_members_tile_scan<T><<<dim3(1, n_), 1024, 0, st_>>>(d_tab_, d_on_, ntiles_);
+        mw::k_members_tile_emit<T><<<dim3(ntiles_, n_), mw::kTileThreads, 0, st_>>>(d_tab_, d_on_, L_);
+        launches_ += 3;
+        if (split) join(ev_[1]);
+        stage<1>();
+        encode<false>();
+        mw::k_members_stage2_maxh<T><<<std::min(cap_wet_, std::min(cap_dry_, cap_leaf_)) + n_, 256, 0, st_>>>(
+            d_tab_, d_on_, d_map_, n_);
+        ++launches_;
+        stage<2>();
+        if (np_max_ > 0)
+        {
+            mw::k_members_sample<T><<<dim3((32 * np_max_ + 127) / 128, n_), 128, 0, st_>>>(d_tab_, d_on_, L_, ntiles_);
+            ++launches_;
+        }
+        mw::k_members_scalars_out<T><<<dim3(1, n_), 128, 0, st_>>>(d_tab_, d_on_);
+        ++launches_;
+    }
+
+    std::vector<Sim<T>*> ms_;
+    int n_ = 0, L_ = 0, ntiles_ = 0, np_max_ = 0, launches_ = 0;
+    int cap_wet_ = 1, cap_dry_ = 1, cap_list_ = 1, cap_leaf_ = 1;
+    std::vector<typename Sim<T>::Band> bands_;
+    mw::MemberArgs<T>* d_tab_ = nullptr;
+    uint8_t* d_on_ = nullptr;
+    uint8_t* h_active_ = nullptr;   // pinned, mapped
+    uint8_t* m_active_ = nullptr;   // its device address
+    int32_t* h_map_ = nullptr;      // block maps, pinned and mapped (host writes before each launch)
+    int32_t* m_map_ = nullptr;      // its device address
+    int32_t* d_map_ = nullptr;      // the maps in device memory (k_members_open copies them)
+    cudaStream_t st_ = nullptr, st2_ = nullptr;
+    cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaGraphExec_t exec_ = nullptr;
+};
+
+} // namespace
+
 // ============================================================================ C ABI
 
 struct mwdg2_sim
@@ -1543,6 +1867,11 @@ struct mwdg2_batch
 {
     std::vector<std::unique_ptr<mwdg2_sim>> members;
     std::vector<uint8_t> done;
+    // size classes stepped by one launch per kernel (formed once every member is past its
+    // first step); group_of[i] = -1: member i steps on its own
+    std::vector<std::unique_ptr<GroupBase>> groups;
+    std::vector<int> group_of;
+    bool grouped = false;
 };
 
 namespace {
@@ -1572,6 +1901,60 @@ template <typename Fn> mwdg2_status for_members(int n, Fn fn)
     for (int i = 0; i < n; ++i)
         if (st[i] != MWDG2_OK && st[i] != MWDG2_DONE)
             return set_err(st[i], "batch member " + std::to_string(i) + ": " + msg[i]);
+    return MWDG2_OK;
+}
+
+// Forms the batch's size classes of two or more members with the same group key (none is
+// formed while a member has its first step to take); checks that grouped members still
+// qualify and dissolves the groups otherwise (they are formed again at the next step).
+mwdg2_status regroup(mwdg2_batch* b)
+{
+    const int n = (int)b->members.size();
+    if (b->grouped)
+    {
+        bool ok = true;
+        for (const auto& g : b->groups)
+            for (int i : g->idx)
+                if (!b->done[i] && b->members[i]->impl->group_key() != g->key) ok = false;
+        if (ok) return MWDG2_OK;
+        b->groups.clear();
+        b->grouped = false;
+    }
+    b->group_of.assign(n, -1);
+    std::map<int, std::vector<int>> by_key;
+    for (int i = 0; i < n; ++i)
+    {
+        if (b->done[i]) continue;
+        if (b->members[i]->impl->first_step()) return MWDG2_OK;   // not yet
+        const int k = b->members[i]->impl->group_key();
+        if (k >= 0) by_key[k].push_back(i);
+    }
+    for (auto& kv : by_key)
+    {
+        if (kv.second.size() < 2) continue;
+        std::unique_ptr<GroupBase> g;
+        if (kv.first & (1 << 8))
+        {
+            std::vector<Sim<double>*> ms;
+            for (int i : kv.second) ms.push_back(static_cast<Sim<double>*>(b->members[i]->impl.get()));
+            auto* gg = new Group<double>();
+            g.reset(gg);
+            if (mwdg2_status st = gg->build(ms)) return st;
+        }
+        else
+        {
+            std::vector<Sim<float>*> ms;
+            for (int i : kv.second) ms.push_back(static_cast<Sim<float>*>(b->members[i]->impl.get()));
+            auto* gg = new Group<float>();
+            g.reset(gg);
+            if (mwdg2_status st = gg->build(ms)) return st;
+        }
+        g->idx = kv.second;
+        g->key = kv.first;
+        for (int i : kv.second) b->group_of[i] = (int)b->groups.size();
+        b->groups.push_back(std::move(g));
+    }
+    b->grouped = true;
     return MWDG2_OK;
 }
 
@@ -1759,11 +2142,11 @@ mwdg2_status mwdg2_batch_step(mwdg2_batch* b, double* dts, int64_t* leaves, int3
 {
     if (!b) return set_err(MWDG2_ERR_ARG, "null batch");
     const int n = (int)b->members.size();
+    if (mwdg2_status s = regroup(b)) return s;
+    if (b->group_of.size() != (size_t)n) b->group_of.assign(n, -1);
     std::vector<uint8_t> stepped(n, 0), first(n, 0);
     std::vector<std::chrono::steady_clock::time_point> t0(n);
-    // clock updates and kernels of every member, without waiting
-    mwdg2_status st = for_members(n, [&](int i) -> mwdg2_status {
-        if (b->done[i]) return MWDG2_OK;
+    auto begin = [&](int i) -> mwdg2_status {
         SimBase& m = *b->members[i]->impl;
         first[i] = m.first_step();
         t0[i] = std::chrono::steady_clock::now();
@@ -1771,10 +2154,32 @@ mwdg2_status mwdg2_batch_step(mwdg2_batch* b, double* dts, int64_t* leaves, int3
         if (s == MWDG2_DONE) { b->done[i] = 1; return MWDG2_OK; }
         if (s != MWDG2_OK) return s;
         stepped[i] = 1;
-        return m.enqueue_step();
+        return MWDG2_OK;
+    };
+    // clock updates and kernels of every member on its own, without waiting
+    mwdg2_status st = for_members(n, [&](int i) -> mwdg2_status {
+        if (b->done[i] || b->group_of[i] >= 0) return MWDG2_OK;
+        if (mwdg2_status s = begin(i)) return s;
+        return stepped[i] ? b->members[i]->impl->enqueue_step() : MWDG2_OK;
     });
+    // the size classes: one launch per kernel for all their members
+    for (auto& g : b->groups)
+    {
+        if (st != MWDG2_OK) break;
+        std::vector<uint8_t> stepping(g->idx.size(), 0);
+        for (size_t k = 0; k < g->idx.size() && st == MWDG2_OK; ++k)
+        {
+            const int i = g->idx[k];
+            if (b->done[i]) continue;
+            st = begin(i);
+            stepping[k] = stepped[i];
+        }
+        if (st == MWDG2_OK) st = g->launch(stepping);
+    }
+    for (auto& g : b->groups)
+        if (st == MWDG2_OK) st = g->wait();
     // then wait for each member, take its dt and write its outputs
-    mwdg2_status st2 = for_members(n, [&](int i) -> mwdg2_status {
+    mwdg2_status st2 = st != MWDG2_OK ? st : for_members(n, [&](int i) -> mwdg2_status {
         double dt = 0;
         int64_t nl = 0;
         if (stepped[i])

@@ -391,14 +391,15 @@ __device__ __forceinline__ void put_leaf_fv1(const Hier<T>& hout, int a, T h, T 
 // leaves). Stage 1 also keeps a dry leaf's depth after ghost cells in U^n (un[0]); stage 2
 // reports initial_tstep as the CFL step of dry leaves (dg2_update.cu:61).
 template <typename T, int STAGE>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4) k_stage_wet(Leaves<T> lf, Hier<T> hin, Scalars<T>* sc, Params<T> P,
-                                                   const StepArgs<T>* args, uint8_t* dry, int32_t* wet)
+__device__ __forceinline__ void k_stage_wet_body(int bid, int nb, Leaves<T> lf, Hier<T> hin, Scalars<T>* sc, Params<T> P,
+                                                   const StepArgs<T>* args, uint8_t* dry, int32_t* wet,
+                                                   const uint8_t* dry1 = nullptr, uint8_t* clean = nullptr)
 {
     const T dt = args->dt;
     const Bnd<T>& B = args->B;
     const int n = sc->n_leaves;
     bool any_dry = false;
-    for (int i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x)
+    for (int i0 = bid * blockDim.x; i0 < n; i0 += nb * blockDim.x)
     {
         const int i = i0 + threadIdx.x;
         bool is_wet = false;
@@ -429,6 +430,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4) k_stage_wet(Leave
             any_dry |= is_dry;
             dry[i] = is_dry ? 1 : 0;
             if (STAGE == 1 && is_dry) lf.un[0][i] = h0;
+            if (STAGE == 2 && clean) clean[i] = (is_dry && dry1[i]) ? 1 : 0;
         }
         // warp-aggregated append
         const unsigned mask = __ballot_sync(0xffffffffu, is_wet);
@@ -440,22 +442,41 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4) k_stage_wet(Leave
     }
     if (STAGE == 2 && __syncthreads_or(any_dry) && threadIdx.x == 0) atomic_min_nn(&sc->dt_min, P.initial_tstep);
 }
+template <typename T, int STAGE>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4) k_stage_wet(Leaves<T> lf, Hier<T> hin, Scalars<T>* sc, Params<T> P,
+                                                   const StepArgs<T>* args, uint8_t* dry, int32_t* wet,
+                                                   const uint8_t* dry1 = nullptr, uint8_t* clean = nullptr)
+{
+    k_stage_wet_body<T, STAGE>(blockIdx.x, gridDim.x, lf, hin, sc, P, args, dry, wet, dry1, clean);
+}
 
 // The dry leaves of one RK stage, marked by k_stage_wet (bandwidth-bound; it runs beside
 // the latency-bound wet-list kernel). Stage 1 (hin: hierarchy, hout: stage hierarchy): U^n
 // is the leaf's state with the discharge cleared by friction (depth after ghost cells as
 // k_stage_wet left it in un[0]) and U* equals it. Stage 2 (hout: hierarchy): the leaf keeps
 // U^n, which is re-inserted into the hierarchy and enters the next step's maxima.
+// pm (learned refinement proposal, applied steps with both stages over the wet list): a
+// leaf inside a subtree the proposal left out (its subtree's encode and decode are skipped
+// too) keeps its state as it stands in the hierarchy where nothing has changed it.
+// Stage 1 skips such a leaf when it is dry, its position holds the same leaf as in the last
+// step (lf.same) and it was dry in both stages of the last step (clean, from the last
+// step's stage-2 wet test; null when that step did not record it): its U^n copy (un) and
+// its U* in the stage hierarchy are then still the ones written when it last changed.
+// Stage 1 marks the leaves it skips (dry[i] = 2); stage 2 writes nothing for such a leaf that
+// is dry in stage 2 as well (dry1: stage 1's marks) and only adds it to the maxima, so a
+// leaf's state is re-inserted at least once after it last changed.
 template <typename T, int STAGE>
-__global__ void __launch_bounds__(256) k_stage_dry(Leaves<T> lf, Hier<T> hin, Hier<T> hout, Scalars<T>* sc, Params<T> P,
-                                                   bool friction, const uint8_t* dry)
+__device__ __forceinline__ void k_stage_dry_body(int bid, int nb, Leaves<T> lf, Hier<T> hin, Hier<T> hout, Scalars<T>* sc, Params<T> P,
+                                                   bool friction, uint8_t* dry, const uint8_t* dry1, PropMask pm,
+                                                   const uint8_t* clean = nullptr)
 {
     const int n = sc->n_leaves;
-    const int stride = gridDim.x * blockDim.x;
+    const int stride = nb * blockDim.x;
     StateMax<T> mx;
+    unsigned frozen = 0;
     // software pipeline: the next leaf's mark and hierarchy index are loaded while this
     // leaf's gathers at its index are in flight (one dependent round trip per leaf, not two)
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int i = bid * blockDim.x + threadIdx.x;
     bool dry_next = i < n && dry[i];
     int a_next = i < n ? lf.act[i] : 0;
     for (; i < n; i += stride)
@@ -468,6 +489,26 @@ __global__ void __launch_bounds__(256) k_stage_dry(Leaves<T> lf, Hier<T> hin, Hi
             a_next = lf.act[i + stride];
         }
         if (!is_dry) continue;
+        if (pm.prop && (STAGE == 2 || clean))
+        {
+            const int lv = lf.lvl[i];
+            const bool left_out = lv >= pm.level && !pm.prop[(a - lvl_idx(lv)) >> (2 * (lv - pm.level))];
+            if (STAGE == 1 && left_out && lf.same[i] && clean[i])
+            {
+                dry[i] = 2;
+                ++frozen;
+                continue;
+            }
+            if (STAGE == 2 && left_out && dry1[i] == 2)
+            {
+                T u[9];
+                u[0] = lf.un[0][i];
+                u[3] = lf.un[3][i];
+                mx.add(u, hin.s[3][0][a]);
+                if (P.dt_leaf) P.dt_leaf[i] = P.initial_tstep;
+                continue;
+            }
+        }
         const T z[3] = {hin.s[3][0][a], hin.s[3][1][a], hin.s[3][2][a]};
         T u[9];
         if (STAGE == 1)
@@ -495,6 +536,18 @@ __global__ void __launch_bounds__(256) k_stage_dry(Leaves<T> lf, Hier<T> hin, Hi
         put_leaf(hout, a, u, z);
     }
     if (STAGE == 2) mx.flush(sc);
+    if (STAGE == 1 && pm.prop)
+    {
+        frozen = __reduce_add_sync(0xffffffffu, frozen);
+        if ((threadIdx.x & 31) == 0 && frozen) atomicAdd(&sc->prop_frozen, frozen);
+    }
+}
+template <typename T, int STAGE>
+__global__ void __launch_bounds__(256) k_stage_dry(Leaves<T> lf, Hier<T> hin, Hier<T> hout, Scalars<T>* sc, Params<T> P,
+                                                   bool friction, uint8_t* dry, const uint8_t* dry1, PropMask pm,
+                                                   const uint8_t* clean = nullptr)
+{
+    k_stage_dry_body<T, STAGE>(blockIdx.x, gridDim.x, lf, hin, hout, sc, P, friction, dry, dry1, pm, clean);
 }
 
 // One RK2 stage of MWDG2, reading the hierarchy `hin` and writing each leaf's result into
@@ -506,7 +559,7 @@ __global__ void __launch_bounds__(256) k_stage_dry(Leaves<T> lf, Hier<T> hin, Hi
 // mra/reinsert_assem_sol.cu), the next step's maxima, CFL dt. LIST: only the leaves in
 // the wet list built by k_stage_wet; otherwise every leaf.
 template <typename T, int STAGE, bool LIST>
-__global__ void __launch_bounds__(kSolverThreads, sizeof(T) == 4 ? 5 : 2) k_mwdg2_stage(Leaves<T> lf, Hier<T> hin, Hier<T> hout, Scalars<T>* sc,
+__device__ __forceinline__ void k_mwdg2_stage_body(int bid, int nb, Leaves<T> lf, Hier<T> hin, Hier<T> hout, Scalars<T>* sc,
                                                                 Params<T> P, const StepArgs<T>* args, bool friction,
                                                                 const int32_t* wet)
 {
@@ -519,7 +572,7 @@ __global__ void __launch_bounds__(kSolverThreads, sizeof(T) == 4 ? 5 : 2) k_mwdg
     bool nan_seen = false;
     unsigned n_wet = 0;
     const T max_h = (STAGE == 1) ? fmax(T(1.0), sc->max_h) : sc->max_h2;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+    for (int k = bid * blockDim.x + threadIdx.x; k < n; k += nb * blockDim.x)
     {
         const int i = LIST ? wet[k] : k;
         const int a = lf.act[i];
@@ -696,17 +749,24 @@ __global__ void __launch_bounds__(kSolverThreads, sizeof(T) == 4 ? 5 : 2) k_mwdg
         if (__syncthreads_or(nan_seen) && threadIdx.x == 0) atomicOr(&sc->status, 1);
     }
 }
+template <typename T, int STAGE, bool LIST>
+__global__ void __launch_bounds__(kSolverThreads, sizeof(T) == 4 ? 5 : 2) k_mwdg2_stage(Leaves<T> lf, Hier<T> hin, Hier<T> hout, Scalars<T>* sc,
+                                                                Params<T> P, const StepArgs<T>* args, bool friction,
+                                                                const int32_t* wet)
+{
+    k_mwdg2_stage_body<T, STAGE, LIST>(blockIdx.x, gridDim.x, lf, hin, hout, sc, P, args, friction, wet);
+}
 
 // max |h0| of the stage-2 leaf state after ghost cells (run_simulation.cu:613-620).
 template <typename T>
-__global__ void __launch_bounds__(256) k_stage2_maxh(Leaves<T> lf, Hier<T> hr, Scalars<T>* sc, Params<T> P,
+__device__ __forceinline__ void k_stage2_maxh_body(int bid, int nb, Leaves<T> lf, Hier<T> hr, Scalars<T>* sc, Params<T> P,
                                                      const StepArgs<T>* args)
 {
     const T dt = args->dt;
     const Bnd<T>& B = args->B;
     const int n = sc->n_leaves;
     T mh = T(0);
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    for (int i = bid * blockDim.x + threadIdx.x; i < n; i += nb * blockDim.x)
     {
         const int a = lf.act[i];
         const T z0 = hr.s[3][0][a];
@@ -725,6 +785,12 @@ __global__ void __launch_bounds__(256) k_stage2_maxh(Leaves<T> lf, Hier<T> hr, S
     T v[1] = {mh};
     T* const dst[1] = {&sc->max_h2};
     block_max_atomic<T, 1>(v, dst);
+}
+template <typename T>
+__global__ void __launch_bounds__(256) k_stage2_maxh(Leaves<T> lf, Hier<T> hr, Scalars<T>* sc, Params<T> P,
+                                                     const StepArgs<T>* args)
+{
+    k_stage2_maxh_body<T>(blockIdx.x, gridDim.x, lf, hr, sc, P, args);
 }
 
 // operators/fv1_update.cu:3-243 with friction and ghost cells fused. Reads the leaf and its
@@ -867,7 +933,7 @@ __global__ void __launch_bounds__(kSolverThreads, sizeof(T) == 4 ? 6 : 3) k_hwfv
 // c is among the leaves of tile c >> 10, or is the last leaf before them when a coarser leaf
 // covers the whole tile.
 template <typename T>
-__global__ void k_sample_points(Leaves<T> lf, Hier<T> hr, Scalars<T>* sc, int L, const int32_t* codes, int np,
+__device__ __forceinline__ void k_sample_points_body(Leaves<T> lf, Hier<T> hr, Scalars<T>* sc, int L, const int32_t* codes, int np,
                                 const int32_t* tile_offsets, int ntiles, T* out)
 {
     const int k = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
@@ -902,6 +968,12 @@ __global__ void k_sample_points(Leaves<T> lf, Hier<T> hr, Scalars<T>* sc, int L,
     out[4 * k + 1] = lf.un[3][lo];
     out[4 * k + 2] = lf.un[6][lo];
     out[4 * k + 3] = z0;
+}
+template <typename T>
+__global__ void k_sample_points(Leaves<T> lf, Hier<T> hr, Scalars<T>* sc, int L, const int32_t* codes, int np,
+                                const int32_t* tile_offsets, int ntiles, T* out)
+{
+    k_sample_points_body<T>(lf, hr, sc, L, codes, np, tile_offsets, ntiles, out);
 }
 
 // Leaf state with the bed coefficients gathered from the hierarchy, 12 rows of n values.

@@ -293,10 +293,10 @@ class Simulation:
         return out
 
     def proposal_stats(self) -> dict:
-        a = np.zeros(10)
-        _check(lib().mwdg2_proposal_stats(self._h, _p(a, ctypes.c_double), 10))
+        a = np.zeros(12)
+        _check(lib().mwdg2_proposal_stats(self._h, _p(a, ctypes.c_double), 12))
         keys = ("active", "missed", "proposed", "applied", "subtrees", "learned_steps", "judge_steps", "judge_miss_rate",
-                "fallbacks", "fallback_left")
+                "fallbacks", "fallback_left", "frozen_leaves", "needed")
         return dict(zip(keys, a.tolist()))
 
     def last_step_counters(self) -> dict:

@@ -256,11 +256,13 @@ mwdg2_status mwdg2_proposal_record(mwdg2_sim* sim, int on);
 
 /* Let the MLP with `params` (MWDG2_MLP_PARAMS floats, copied) choose, from the next step on,
  * the child subtrees of the coarse level that the encode, decode and scale re-encode visit
- * (logit > threshold); subtrees left out keep their flags and values. Every judge_every-th
- * step (0: never) runs in full as the judge; a step whose active subtrees the proposal left
- * out exceed the fraction miss_bound makes the next judge_every steps run in full. params =
- * NULL switches the proposal off. MWDG2 only (MWDG2_ERR_STATE). The proposal acts on the
- * levels above 9 (one kernel launch per level), so below max_ref_lvl 11 it is only scored. */
+ * (logit > threshold); subtrees left out keep their flags and values, and so do their
+ * leaves that stay dry through the step (wet leaves are updated everywhere). Every
+ * judge_every-th step (0: never) runs in full as the judge. The subtrees that needed a step
+ * are those whose leaves it updated or whose flags gained significance; when the proposal
+ * left out more than the fraction miss_bound of them (counted as at least 0.1 % of all
+ * subtrees), the next judge_every steps run in full. params = NULL switches the proposal
+ * off. MWDG2 only (MWDG2_ERR_STATE). */
 mwdg2_status mwdg2_proposal_enable(mwdg2_sim* sim, const float* params, int judge_every, float threshold,
                                    float miss_bound);
 
@@ -273,10 +275,13 @@ mwdg2_status mwdg2_proposal_samples(mwdg2_sim* sim, float* feats, uint8_t* label
  * of level C + 1), 1 = visited. *n receives the count; out may be NULL. */
 mwdg2_status mwdg2_proposal_mask(mwdg2_sim* sim, uint8_t* out, int64_t cap, int64_t* n);
 
-/* [0] active subtrees in the last step, [1] of them left out by the proposal, [2] subtrees
- * proposed, [3] 1 if the last step applied the proposal, [4] subtrees in all, [5] steps that
- * applied it, [6] judge steps, [7] missed fraction at the last judge step, [8] fallbacks,
- * [9] full steps left in the current fallback. n <= 10. */
+/* [0] active subtrees in the last step (leaves updated or significance flags changed), [1]
+ * subtrees the proposal left out that needed the step (leaves updated or flags gaining
+ * significance), [2] subtrees proposed, [3] 1 if the last step applied the proposal, [4]
+ * subtrees in all, [5] steps that applied it, [6] judge steps, [7] missed fraction ([1] /
+ * [11]) at the last judge step, [8] fallbacks, [9] full steps left in the current fallback,
+ * [10] dry leaves of left-out subtrees that the last step left as they stood, [11] subtrees
+ * that needed the step. n <= 12. */
 mwdg2_status mwdg2_proposal_stats(mwdg2_sim* sim, double* out, int n);
 
 #ifdef __cplusplus

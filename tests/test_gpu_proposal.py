@@ -5,11 +5,15 @@ catchment, FP64), through the C ABI:
 * a proposal that keeps every subtree gives the plain step's results bit for bit (the masked
   encode, decode and re-encode kernels with an all-ones mask; the MLP run on every coarse
   cell, as with recording on);
-* a proposal that keeps none skips the upper levels' encode and decode, misses the active
-  subtrees, and the fallback then runs full steps (judge every 4 steps, miss bound 5 %);
+* a proposal that keeps none skips the upper levels' encode and decode, misses every
+  subtree that needed the step (leaves updated or flags gaining significance), and the
+  fallback then runs full steps (judge every 4 steps, miss bound 5 %);
+* where the proposal leaves a subtree out, its leaves that stay dry keep their state in the
+  hierarchy bit for bit, while the wet leaves are still updated;
 * the fused proposal kernel (features from a shared-memory ring, then the MLP) gives the
   proposal of the two-kernel path (features written out, then the MLP) on every tile whose
-  ring of coarse cells had activity last step, and proposes nothing elsewhere;
+  ring of coarse cells had activity last step, and proposes nothing elsewhere (both runs
+  judge every step, so their states stay identical);
 * the device-built feature rows equal the NumPy restatement of the feature builder
   (tests/mlp_ref.py) from the hierarchy, flags and activity bits the previous step left;
 * the trainer takes an Adam step on the features and labels a recorded step left on the
@@ -76,7 +80,7 @@ def test_recording_and_all_ones_proposal_change_nothing(tmp_path):
     _same(plain, ones, "all-ones proposal")
     st = ones[-1][3]
     assert st["applied"] == 1.0 and st["proposed"] == st["subtrees"] and st["missed"] == 0
-    assert st["active"] > 0
+    assert st["active"] > 0 and st["needed"] > 0
 
 
 def test_empty_proposal_misses_and_falls_back(tmp_path):
@@ -86,12 +90,70 @@ def test_empty_proposal_misses_and_falls_back(tmp_path):
     sim.step()                      # the first step always runs in full
     sim.step()                      # the empty proposal: every active subtree is missed
     st = sim.proposal_stats()
-    assert st["applied"] == 1.0 and st["proposed"] == 0 and st["missed"] == st["active"] > 0
+    assert st["applied"] == 1.0 and st["proposed"] == 0 and st["missed"] == st["needed"] > 0
+    assert st["active"] >= st["needed"]
     assert st["fallbacks"] == 1 and st["fallback_left"] == 4
     for _ in range(4):
         ok, dt, n = sim.step()
         assert ok and dt > 0
         assert sim.proposal_stats()["applied"] == 0.0
+    sim.close()
+
+
+def _dry_two_rings(sim, tol_h=1e-3) -> np.ndarray:
+    """Leaves that are dry, with dry neighbours and dry neighbours' neighbours (the wet test
+    of both RK stages of the next step then finds them dry)."""
+    lv, st = sim.leaves(), sim.state()
+    ids = lv["nb_ids"]
+    pos = {int(a): i for i, a in enumerate(lv["act"])}
+    dry = st["h0"] < tol_h
+    # a neighbour id is a leaf or a significant parent (finer leaves): treat parents as wet
+    nb_dry = np.ones(len(dry), bool)
+    for d in range(4):
+        for i, a in enumerate(ids[d]):
+            if a >= 0:
+                j = pos.get(int(a))
+                nb_dry[i] &= (j is not None) and bool(dry[j])
+    one = dry & nb_dry
+    two = one.copy()
+    for d in range(4):
+        for i, a in enumerate(ids[d]):
+            if a >= 0:
+                j = pos.get(int(a))
+                two[i] &= (j is not None) and bool(one[j])
+    return two
+
+
+def test_left_out_dry_subtrees_keep_their_state(tmp_path):
+    c = _case(tmp_path)
+    sim = mwdg2_b200.Simulation(c.par, precision=64)
+    sim.proposal_enable(_constant_mlp(-20.0), judge_every=0, threshold=0.0, miss_bound=1.0)
+    # the first step runs in full; the second, with nothing proposed (every subtree of level
+    # L - 2 left out), records which leaves stayed dry in both stages
+    sim.step()
+    sim.step()
+    lv = sim.leaves()
+    keep = _dry_two_rings(sim) & (lv["lvl"] >= L - 2)
+    hier = [[sim.hierarchy(f, m) for m in range(3)] for f in range(3)]
+    st = sim.state()
+    sim.step()                      # those of them still dry are left as they stand
+    stats = sim.proposal_stats()
+    assert stats["applied"] == 1.0 and stats["frozen_leaves"] >= keep.sum()
+    lv2 = sim.leaves()
+    np.testing.assert_array_equal(lv2["act"], lv["act"], err_msg="the tree of a step with nothing proposed")
+    a = lv["act"][keep]
+    assert keep.sum() > 1000
+    for f in range(3):
+        for m in range(3):
+            np.testing.assert_array_equal(sim.hierarchy(f, m)[a], hier[f][m][a], err_msg=f"field {f} mode {m}")
+    st2 = sim.state()
+    for f in FIELDS:
+        if f == "h0":   # re-derived each step as eta - z from the unchanged hierarchy
+            assert np.max(np.abs(st2[f][keep] - st[f][keep])) <= 1e-12
+        else:
+            np.testing.assert_array_equal(st2[f][keep], st[f][keep], err_msg=f"state {f}")
+    wet = st["h0"] >= 1e-3
+    assert np.any(st2["h0"][wet] != st["h0"][wet]), "the wet leaves were not updated"
     sim.close()
 
 
@@ -147,7 +209,7 @@ def test_fused_proposal_matches_two_kernel_path(tmp_path):
     b = mwdg2_b200.Simulation(c.par, precision=64)
     a.proposal_record(True)
     for s in (a, b):
-        s.proposal_enable(params, judge_every=0, threshold=-2.0, miss_bound=1.0)
+        s.proposal_enable(params, judge_every=1, threshold=-2.0, miss_bound=1.0)
     C = L - 3
     checked = 0
     for step in range(1, 5):
