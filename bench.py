@@ -38,7 +38,8 @@ UNIT = "cell-updates/s"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (catchment: 1000, a window of about 0.6 s on the device; others: 20)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", type=int, default=32, choices=[32, 64])
@@ -64,6 +65,8 @@ def parse():
     a = ap.parse_args()
     if a.level is None:
         a.level = 13 if a.workload == "urban" else 12
+    if a.steps is None:
+        a.steps = 1000 if a.workload == "catchment" else 20
     return a
 
 
@@ -175,6 +178,7 @@ TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the phase
                   "launches per capture) on the 2048^2 catchment (max_ref_lvl 11, 1.21 M leaves), per leaf, "
                   "x this run's leaves")
 PHASE_STEPS = 5
+REF_CPU_STEPS = 20   # the reference arm's timed steps on the host cores (at most)
 # DRAM bytes per leaf of the RK stages (phase 4: stage 1, phase 6: stage 2) in FP32
 TRAFFIC_B_PER_LEAF: dict = {("mwdg2", 4, 4): 181.0, ("mwdg2", 4, 6): 141.6}
 
@@ -258,10 +262,12 @@ def run_reference(a):
     if rank != 0:
         return
     par = make_case(a, 0)
-    cpu = oracle_timing(par, a.steps, a.warmup)
+    # a bounded sample of the workload on the host cores (about half a second per step)
+    cpu_steps = min(a.steps, REF_CPU_STEPS)
+    cpu = oracle_timing(par, cpu_steps, a.warmup)
     v = cpu["value"]
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
-            "ms_per_step": 1e3 * cpu["wall_s"] / a.steps, "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": 1e3 * cpu["wall_s"] / cpu_steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded fBm DEM)", "config": workload(a),
             "impl": "reference",
             "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample", "cpu_model", "dtype")},
@@ -396,6 +402,7 @@ def peak_window(sim, a, dist) -> dict:
             wet.append((c["wet_stage1"], c["wet_stage2"]))
     sim_s = sim.info()["time"] - t_sim0
     end_time, end_depth = sim.info()["time"], finest_depth(sim)   # for the learned run's comparison
+    end_volume = wet_volume(sim)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     tot_ms = max_over_ranks(float(sum(ms)), dist, "cuda")
     n_mean = float(np.mean(leaves))
@@ -415,7 +422,20 @@ def peak_window(sim, a, dist) -> dict:
             "wet_fraction": [float(np.mean([w[k] for w in wet])) / n_mean for k in (0, 1)],
             "wall_s_per_sim_s": (tot_ms / 1e3) / sim_s if sim_s > 0 else None, "sim_seconds": sim_s,
             "timing": "device time of each step (CUDA events on the library's stream), max over ranks",
-            "_end_time": end_time, "_end_depth": end_depth}
+            "wet_volume_m3": end_volume, "_end_time": end_time, "_end_depth": end_depth}
+
+
+def wet_volume(sim, tol_h: float = 1e-3) -> float:
+    """Water volume (m^3) in the leaves at least tol_h deep: the depths below tol_h in the
+    dry area are the multiresolution representation's rounding of eta = h + z over rough
+    terrain (a few 1e-6 m per cell in FP32, of either sign, accumulating over a run), which
+    would otherwise dominate the total."""
+    import numpy as np
+    info = sim.info()
+    st, lv = sim.state(), sim.leaves()
+    area = info["dx"] ** 2 * np.ldexp(1.0, 2 * (info["L"] - lv["lvl"].astype(np.int64)))
+    h = st["h0"]
+    return float(np.sum(np.where(h >= tol_h, h, 0.0) * area))
 
 
 def finest_depth(sim):
@@ -461,7 +481,7 @@ def par_ending_at(par: str, t_end: float) -> str:
     return out
 
 
-def learned_window(a, par, t_from, t_end, depth_plain, value_plain, name) -> dict:
+def learned_window(a, par, t_from, t_end, depth_plain, value_plain, name, volume_plain=None) -> dict:
     """A window of the plain run again with the learned refinement proposal: a second
     simulation of the same case (ending at t_end, where the plain run's window ended) with the
     trained MLP choosing the subtrees the step visits (judge every --judge-every steps),
@@ -479,7 +499,7 @@ def learned_window(a, par, t_from, t_end, depth_plain, value_plain, name) -> dic
         ok = sim.step()[0]
     for _ in range(a.warmup):
         ok = ok and sim.step()[0]
-    ms, leaves = [], []
+    ms, leaves, wet = [], [], []
     with nvtx_range(name):
         for _ in range(a.steps):
             ok, dt, n = sim.step()
@@ -487,15 +507,21 @@ def learned_window(a, par, t_from, t_end, depth_plain, value_plain, name) -> dic
                 break
             ms.append(float(sim.last_step_timing()[7]))
             leaves.append(n)
+            c = sim.last_step_counters()
+            wet.append((c["wet_stage1"], c["wet_stage2"]))
     st = sim.proposal_stats()
     while ok:
         ok = sim.step()[0]
     diff = float(np.max(np.abs(finest_depth(sim) - depth_plain)))
     t_done = sim.info()["time"]
+    volume = wet_volume(sim)
     sim.close()
     v = sum(leaves) / (sum(ms) / 1e3)
+    n_mean = float(np.mean(leaves))
     return {"value": v, "ms_per_step": sum(ms) / len(ms), "steps": len(ms), "vs_plain": v / value_plain,
+            "leaves_mean": n_mean, "wet_fraction": [float(np.mean([w[k] for w in wet])) / n_mean for k in (0, 1)],
             "max_depth_diff_vs_plain_m": diff, "compared_at_time": t_done, "plain_time": t_end,
+            "wet_volume_m3": volume, "plain_wet_volume_m3": volume_plain,
             "proposal": {k: st[k] for k in ("active", "proposed", "subtrees", "learned_steps", "judge_steps",
                                              "fallbacks", "frozen_leaves")},
             "mlp": os.path.basename(a.proposal), "judge_every": a.judge_every,
@@ -542,7 +568,8 @@ def run_learned(a):
             steps += 1
             if learned:
                 applied += int(sim.proposal_stats()["applied"])
-        out = {"ms": ms, "leaves": leaves, "steps": steps, "time": sim.info()["time"], "depth": finest_depth(sim)}
+        out = {"ms": ms, "leaves": leaves, "steps": steps, "time": sim.info()["time"], "depth": finest_depth(sim),
+               "wet_volume": wet_volume(sim)}
         if learned:
             out["stats"] = sim.proposal_stats()
             out["applied_steps"] = applied
@@ -566,6 +593,7 @@ def run_learned(a):
                                        f"trained MLP ({a.proposal.split('/')[-1]}), judge every {a.judge_every} steps",
                            "depth_reference": "the same case in FP64, plain"},
                 "max_depth_error_m": err, "time": r["time"], "reference_time": ref["time"],
+                "wet_volume_m3": r["wet_volume"], "reference_wet_volume_m3": ref["wet_volume"],
                 "timing": "sum of CUDA-event device times of every step of the run"}
         if name == "learned":
             line["vs_plain"] = line["value"] / lines[0]["value"]
@@ -629,10 +657,25 @@ def main():
     sim_s = sim.info()["time"] - t_sim0
     tot_ms = max_over_ranks(float(sum(ms_step)), dist, "cuda")
     value = replica_throughput(world, sum(leaves), tot_ms)
+    # phase breakdown (and the dominant phase's time for the roofline), right after the timed
+    # steps: a separate pass with events between the phases inside the step's graph, which
+    # the timed steps do not carry (each such event node costs ~10 us of launch pipelining);
+    # its first step captures the graph variant with the events and is not used
+    sim.set_timing("phases")
+    sim.step()
+    ms_phase, leaves_ph = [], []
+    for _ in range(PHASE_STEPS):
+        ok, dt, n = sim.step()
+        ms_phase.append(sim.last_step_timing().tolist())
+        leaves_ph.append(n)
+    sim.set_timing("step")
+    barrier()
+
     learned = None
     want_learned = world == 1 and a.workload == "catchment" and a.solver == "mwdg2" and os.path.exists(a.proposal)
     if want_learned:
-        learned = learned_window(a, par, 0.0, sim.info()["time"], finest_depth(sim), value, "learned_window")
+        learned = learned_window(a, par, 0.0, sim.info()["time"], finest_depth(sim), value, "learned_window",
+                                 wet_volume(sim))
 
     # end to end through the C ABI: each step's inputs (point-source values) go host->device
     # from pinned memory inside mwdg2_step, its scalars come back, and the stage-point
@@ -648,18 +691,6 @@ def main():
     barrier()
     e2e_wall = time.perf_counter() - t0
     clk.__exit__(None, None, None)
-    # phase breakdown (and the dominant phase's time for the roofline): a separate pass with
-    # events between the phases inside the step's graph, which the steps above do not carry
-    # (each such event node costs ~10 us of launch pipelining); its first step captures the
-    # graph variant with the events and is not used
-    sim.set_timing("phases")
-    sim.step()
-    ms_phase, leaves_ph = [], []
-    for _ in range(PHASE_STEPS):
-        ok, dt, n = sim.step()
-        ms_phase.append(sim.last_step_timing().tolist())
-        leaves_ph.append(n)
-    barrier()
     e2e_wall = max_over_ranks(e2e_wall, dist, "cuda")
     P = a.precision // 8
     # bytes the library copied per step (its counters): host->device the step's dt, boundary
@@ -736,7 +767,8 @@ def main():
         t_end, depth_end = wp.pop("_end_time", None), wp.pop("_end_depth", None)
         line["window_peak"] = wp
         if want_learned and "value" in wp:
-            wp["learned"] = learned_window(a, par, a.peak_time, t_end, depth_end, wp["value"], "learned_peak_window")
+            wp["learned"] = learned_window(a, par, a.peak_time, t_end, depth_end, wp["value"], "learned_peak_window",
+                                           wp["wet_volume_m3"])
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(par, a, a.cpu_steps)
     sim.close()

@@ -43,6 +43,15 @@ template <typename T> struct MemberArgs
     T* stage_out;
 };
 
+// The members' table, passed by value as the kernels' parameter (a __grid_constant__
+// parameter lives in the constant bank, so a block reads its member's pointers where it uses
+// them instead of holding the whole entry in registers); a class has at most kMax members.
+template <typename T> struct MemberTable
+{
+    static constexpr int kMax = 30000 / (int)sizeof(MemberArgs<T>);
+    MemberArgs<T> m[kMax];
+};
+
 // Per-leaf launches split their blocks among the members in proportion to each member's
 // work in the last step (leaves, or wet leaves for the wet-list kernels), so that a large or
 // wet member does not finish long after the others with a fixed share: first[m] is the
@@ -68,7 +77,7 @@ __device__ __forceinline__ int member_of(const int32_t* first, int n, int b)
 // host before the launch); the flag goes to on[m] in device memory for the later kernels,
 // and so do the block maps (map_host -> map, kBlockMaps x (n + 1)).
 template <typename T>
-__global__ void k_members_open(const MemberArgs<T>* tab, const uint8_t* active, uint8_t* on, int L,
+__global__ void k_members_open(const __grid_constant__ MemberTable<T> tab, const uint8_t* active, uint8_t* on, int L,
                                const int32_t* map_host, int32_t* map, int n)
 {
     const int m = blockIdx.y;
@@ -86,77 +95,77 @@ __global__ void k_members_open(const MemberArgs<T>* tab, const uint8_t* active, 
     }
     __syncthreads();
     if (!go) return;
-    const MemberArgs<T>& a = tab[m];
+    const MemberArgs<T>& a = tab.m[m];
     k_step_open_body<T>(a.sc, true, a.m_args, a.d_args, a.m_src, a.nsrc, a.hr, a.dx, L);
 }
 
 // FULL: the encode of the hierarchy, else the scale-only re-encode of the stage hierarchy.
 template <typename T, bool FULL>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 6 : 4) k_members_encode_level(const MemberArgs<T>* tab,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 6 : 4) k_members_encode_level(const __grid_constant__ MemberTable<T> tab,
                                                                                      const uint8_t* on, int L, int level)
 {
     if (!on[blockIdx.y]) return;
-    const MemberArgs<T>& a = tab[blockIdx.y];
+    const MemberArgs<T>& a = tab.m[blockIdx.y];
     k_encode_level_body<T, true, FULL>(FULL ? a.hr : a.hs, a.sc, L, level, a.eps);
 }
 
 template <typename T, bool FULL>
-__global__ void __launch_bounds__(256) k_members_encode_band(const MemberArgs<T>* tab, const uint8_t* on, int L, int lo,
+__global__ void __launch_bounds__(256) k_members_encode_band(const __grid_constant__ MemberTable<T> tab, const uint8_t* on, int L, int lo,
                                                             int depth)
 {
     if (!on[blockIdx.y]) return;
-    const MemberArgs<T>& a = tab[blockIdx.y];
+    const MemberArgs<T>& a = tab.m[blockIdx.y];
     k_encode_band_body<T, true, FULL>(FULL ? a.hr : a.hs, a.sc, L, lo, depth, a.eps, PropMask{});
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4) k_members_decode_band(const MemberArgs<T>* tab,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4) k_members_decode_band(const __grid_constant__ MemberTable<T> tab,
                                                                                     const uint8_t* on, int L, int lo,
                                                                                     int depth)
 {
     if (!on[blockIdx.y]) return;
-    const MemberArgs<T>& a = tab[blockIdx.y];
+    const MemberArgs<T>& a = tab.m[blockIdx.y];
     k_decode_band_body<T, true>(a.hr, a.sc, L, lo, depth, a.eps, PropMask{});
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_members_extra_sig(const MemberArgs<T>* tab, const uint8_t* on, int L, int level)
+__global__ void __launch_bounds__(256) k_members_extra_sig(const __grid_constant__ MemberTable<T> tab, const uint8_t* on, int L, int level)
 {
     if (!on[blockIdx.y]) return;
-    const MemberArgs<T>& a = tab[blockIdx.y];
+    const MemberArgs<T>& a = tab.m[blockIdx.y];
     k_extra_sig_level_body<T>(a.hr.flags, a.sc, L, level, a.eps);
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4) k_members_decode_level(const MemberArgs<T>* tab,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4) k_members_decode_level(const __grid_constant__ MemberTable<T> tab,
                                                                                      const uint8_t* on, int L, int level)
 {
     if (!on[blockIdx.y]) return;
-    const MemberArgs<T>& a = tab[blockIdx.y];
+    const MemberArgs<T>& a = tab.m[blockIdx.y];
     k_decode_level_body<T, true>(a.hr, a.sc, L, level, a.eps, PropMask{});
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kTileThreads) k_members_tile_count(const MemberArgs<T>* tab, const uint8_t* on, int L)
+__global__ void __launch_bounds__(kTileThreads) k_members_tile_count(const __grid_constant__ MemberTable<T> tab, const uint8_t* on, int L)
 {
     if (!on[blockIdx.y]) return;
-    const MemberArgs<T>& a = tab[blockIdx.y];
+    const MemberArgs<T>& a = tab.m[blockIdx.y];
     k_tile_count_body(a.hr.flags, L, a.tile_counts);
 }
 
 template <typename T>
-__global__ void __launch_bounds__(1024) k_members_tile_scan(const MemberArgs<T>* tab, const uint8_t* on, int ntiles)
+__global__ void __launch_bounds__(1024) k_members_tile_scan(const __grid_constant__ MemberTable<T> tab, const uint8_t* on, int ntiles)
 {
     if (!on[blockIdx.y]) return;
-    const MemberArgs<T>& a = tab[blockIdx.y];
+    const MemberArgs<T>& a = tab.m[blockIdx.y];
     k_tile_scan_body<T>(a.tile_counts, ntiles, a.sc);
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kTileThreads, 8) k_members_tile_emit(const MemberArgs<T>* tab, const uint8_t* on, int L)
+__global__ void __launch_bounds__(kTileThreads, 8) k_members_tile_emit(const __grid_constant__ MemberTable<T> tab, const uint8_t* on, int L)
 {
     if (!on[blockIdx.y]) return;
-    const MemberArgs<T>& a = tab[blockIdx.y];
+    const MemberArgs<T>& a = tab.m[blockIdx.y];
     k_tile_emit_body<T, false>(a.lf, a.hr.flags, a.tile_counts, L, a.M, a.xsz, a.ysz, &a.sc->min_leaf, &a.sc->n_prev);
 }
 
@@ -175,48 +184,48 @@ __device__ __forceinline__ bool member_block(const int32_t* first, int n, const 
 }
 
 template <typename T, int STAGE>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4) k_members_stage_wet(const MemberArgs<T>* tab,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4) k_members_stage_wet(const __grid_constant__ MemberTable<T> tab,
                                                                                   const uint8_t* on,
                                                                                   const int32_t* first, int n)
 {
     int m, bid, nb;
     if (!member_block(first, n, on, m, bid, nb)) return;
-    const MemberArgs<T>& a = tab[m];
+    const MemberArgs<T>& a = tab.m[m];
     k_stage_wet_body<T, STAGE>(bid, nb, a.lf, STAGE == 1 ? a.hr : a.hs, a.sc, a.P, a.d_args,
                                STAGE == 1 ? a.dry1 : a.dry2, a.wet);
 }
 
 template <typename T, int STAGE>
-__global__ void __launch_bounds__(kSolverThreads, sizeof(T) == 4 ? 5 : 2) k_members_stage_list(const MemberArgs<T>* tab,
+__global__ void __launch_bounds__(kSolverThreads, sizeof(T) == 4 ? 5 : 2) k_members_stage_list(const __grid_constant__ MemberTable<T> tab,
                                                                                               const uint8_t* on,
                                                                                               const int32_t* first,
                                                                                               int n)
 {
     int m, bid, nb;
     if (!member_block(first, n, on, m, bid, nb)) return;
-    const MemberArgs<T>& a = tab[m];
+    const MemberArgs<T>& a = tab.m[m];
     k_mwdg2_stage_body<T, STAGE, true>(bid, nb, a.lf, STAGE == 1 ? a.hr : a.hs, STAGE == 1 ? a.hs : a.hr, a.sc, a.P,
                                        a.d_args, STAGE == 1 && a.fric, a.wet);
 }
 
 template <typename T, int STAGE>
-__global__ void __launch_bounds__(256) k_members_stage_dry(const MemberArgs<T>* tab, const uint8_t* on,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 5) k_members_stage_dry(const __grid_constant__ MemberTable<T> tab, const uint8_t* on,
                                                           const int32_t* first, int n)
 {
     int m, bid, nb;
     if (!member_block(first, n, on, m, bid, nb)) return;
-    const MemberArgs<T>& a = tab[m];
+    const MemberArgs<T>& a = tab.m[m];
     k_stage_dry_body<T, STAGE>(bid, nb, a.lf, STAGE == 1 ? a.hr : a.hs, STAGE == 1 ? a.hs : a.hr, a.sc, a.P,
                                STAGE == 1 && a.fric, STAGE == 1 ? a.dry1 : a.dry2, a.dry1, PropMask{});
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_members_stage2_maxh(const MemberArgs<T>* tab, const uint8_t* on,
+__global__ void __launch_bounds__(256) k_members_stage2_maxh(const __grid_constant__ MemberTable<T> tab, const uint8_t* on,
                                                             const int32_t* first, int n)
 {
     int m, bid, nb;
     if (!member_block(first, n, on, m, bid, nb)) return;
-    const MemberArgs<T>& a = tab[m];
+    const MemberArgs<T>& a = tab.m[m];
     if (!a.limit) return;
     k_stage2_maxh_body<T>(bid, nb, a.lf, a.hs, a.sc, a.P, a.d_args);
 }
@@ -224,18 +233,18 @@ __global__ void __launch_bounds__(256) k_members_stage2_maxh(const MemberArgs<T>
 // The step's end: the stage points of members that have them, then every stepping member's
 // scalars (and stage-point values) straight into its pinned host block.
 template <typename T>
-__global__ void k_members_sample(const MemberArgs<T>* tab, const uint8_t* on, int L, int ntiles)
+__global__ void k_members_sample(const __grid_constant__ MemberTable<T> tab, const uint8_t* on, int L, int ntiles)
 {
     if (!on[blockIdx.y]) return;
-    const MemberArgs<T>& a = tab[blockIdx.y];
+    const MemberArgs<T>& a = tab.m[blockIdx.y];
     if ((int)(blockIdx.x * blockDim.x) >= 32 * a.np) return;
     k_sample_points_body<T>(a.lf, a.hr, a.sc, L, a.stage_codes, a.np, a.tile_counts, ntiles, a.stage_out);
 }
 
-template <typename T> __global__ void k_members_scalars_out(const MemberArgs<T>* tab, const uint8_t* on)
+template <typename T> __global__ void k_members_scalars_out(const __grid_constant__ MemberTable<T> tab, const uint8_t* on)
 {
     if (!on[blockIdx.y]) return;
-    const MemberArgs<T>& a = tab[blockIdx.y];
+    const MemberArgs<T>& a = tab.m[blockIdx.y];
     const uint32_t* src = reinterpret_cast<const uint32_t*>(a.sc);
     uint32_t* dst = reinterpret_cast<uint32_t*>(a.sc_host);
     for (int i = threadIdx.x; i < a.scal_bytes / 4; i += blockDim.x) dst[i] = src[i];

@@ -59,12 +59,20 @@ template <typename T> struct Scalars
 };
 
 // The subtrees below the nodes of level `level` (the proposal level) that a step's encode and
-// decode visit: prop[node] != 0 (null: all).
+// decode visit: prop[node] != 0 (null: all), or act[node] != 0 where act is given (the
+// subtrees whose leaves this step's RK stages have updated so far).
 struct PropMask
 {
     const uint8_t* prop;
     int level;
+    const uint8_t* act = nullptr;
 };
+
+// Whether the subtree below node `node` of the mask's level is left out.
+__device__ __forceinline__ bool pm_out(const PropMask& pm, int64_t node)
+{
+    return pm.prop && !pm.prop[node] && !(pm.act && pm.act[node]);
+}
 
 
 // A band CTA (node blockIdx.x of level lo and its subtree) holding no node of the mask's
@@ -81,10 +89,11 @@ __device__ __forceinline__ bool band_left_out(const PropMask& pm, int lo)
     if (n >= 4)
     {
         const uint32_t* w = reinterpret_cast<const uint32_t*>(pm.prop + first);
-        for (int i = threadIdx.x; i < n / 4; i += blockDim.x) any |= (w[i] != 0u);
+        const uint32_t* wa = pm.act ? reinterpret_cast<const uint32_t*>(pm.act + first) : nullptr;
+        for (int i = threadIdx.x; i < n / 4; i += blockDim.x) any |= (w[i] != 0u) || (wa && wa[i] != 0u);
     }
     else
-        for (int i = threadIdx.x; i < n; i += blockDim.x) any |= (pm.prop[first + i] != 0);
+        for (int i = threadIdx.x; i < n; i += blockDim.x) any |= !pm_out(pm, first + i);
     return __syncthreads_or(any ? 1 : 0) == 0;
 }
 
@@ -338,7 +347,7 @@ __device__ __forceinline__ void encode_parent(const Hier<T>& hr, const Scalars<T
     const int p = lvl_idx(level) + idx;
     // PM: a parent in a subtree the proposal leaves out keeps its flags and values
     const int anc = (PM && level >= pm.level) ? (idx >> (2 * (level - pm.level))) : -1;
-    if (PM && anc >= 0 && pm.prop && !pm.prop[anc]) return;
+    if (PM && anc >= 0 && pm_out(pm, anc)) return;
     const uint8_t f = hr.flags[p];
     const bool was_sig = (f & F_SIG) != 0;
     const int c = lvl_idx(level + 1) + 4 * idx;
@@ -445,8 +454,7 @@ __device__ __forceinline__ void k_encode_level_body(Hier<T> hr, Scalars<T>* sc, 
         {
             const uint32_t f = (cw >> (8 * j)) & 0xffu;
             go = (f & F_SIG) != 0;
-            const bool kept = PM && level + 1 >= pm.level && pm.prop &&
-                              !pm.prop[(cb + j) >> (2 * (level + 1 - pm.level))];
+            const bool kept = PM && level + 1 >= pm.level && pm_out(pm, (cb + j) >> (2 * (level + 1 - pm.level)));
             if (FULL && !go && !kept && (f & ~(uint32_t)F_PRE)) hr.flags[cfirst + cb + j] = (uint8_t)(f & F_PRE);
             lv = level + 1;
             id = cb + j;
@@ -592,7 +600,7 @@ __device__ __forceinline__ void decode_parent(const Hier<T>& hr, const Scalars<T
 {
     const int p = lvl_idx(level) + idx;
     // PM: the children of a parent in a subtree the proposal leaves out keep their values
-    if (PM && level >= pm.level && pm.prop && !pm.prop[idx >> (2 * (level - pm.level))]) return;
+    if (PM && level >= pm.level && pm_out(pm, idx >> (2 * (level - pm.level)))) return;
     const uint8_t f = hr.flags[p];
     if (!(f & F_SIG)) return;
     const bool enc = (f & F_ENC) != 0;
@@ -843,8 +851,7 @@ __global__ void __launch_bounds__(256) k_level_sparse(Hier<T> hr, Scalars<T>* sc
         for (int j = 0; j < 8; ++j)
         {
             const uint32_t f = ((j < 4 ? w.x : w.y) >> (8 * (j & 3))) & 0xffu;
-            const bool kept = PM && level >= pm.level && pm.prop &&
-                              !pm.prop[(int)((first + j) >> (2 * (level - pm.level)))];
+            const bool kept = PM && level >= pm.level && pm_out(pm, (int)((first + j) >> (2 * (level - pm.level))));
             if (f & F_SIG) sig |= kept ? 0u : 1u << j;
             // FULL encode of a parent that was not significant: only its flag changes (its
             // encode / extra-significance bits from the last step clear, the preflag stays)

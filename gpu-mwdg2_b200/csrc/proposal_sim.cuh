@@ -245,6 +245,25 @@ static __global__ void __launch_bounds__(256) k_prop_labels(uint8_t* __restrict_
     }
 }
 
+// What the proposal keeps whatever the MLP says: the subtrees that were active in the last
+// step (lab_prev: their leaves or flags changed, so their parents must be encoded again
+// before their values are read as neighbours) and the subtrees holding a point source (its
+// inflow enters the finest level and reaches the leaves only through the encode).
+static __global__ void __launch_bounds__(256) k_prop_force(uint8_t* __restrict__ prop, const uint8_t* __restrict__ lab_prev,
+                                                           int64_t nC, const int32_t* __restrict__ src_nodes, int nsrc)
+{
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < nC; c += (int64_t)gridDim.x * blockDim.x)
+    {
+        const uint32_t b = lab_prev[c];
+        if (b)
+            atomicOr(reinterpret_cast<unsigned int*>(prop + 4 * c),
+                     (b & 1u) | ((b & 2u) << 7) | ((b & 4u) << 14) | ((b & 8u) << 21));
+    }
+    if (blockIdx.x == 0)
+        for (int i = threadIdx.x; i < nsrc; i += blockDim.x)
+            atomicOr(reinterpret_cast<unsigned int*>(prop + (src_nodes[i] & ~3)), 1u << (8 * (src_nodes[i] & 3)));
+}
+
 // ---------------------------------------------------------------- fused proposal
 // Shared memory of k_mlp_propose after the MLP's own regions: the coarse-level values of a
 // tile's 16 x 8 cells and their one-cell ring (18 x 10), the CTA's list of tiles to run, and

@@ -247,6 +247,7 @@ private:
     __nv_bfloat16* d_feat_ = nullptr;   // [4^C][128] features of the step's start
     uint8_t* d_lab_ = nullptr;          // [4^C] activity bits of the children in the last step
     uint16_t* d_ring_ = nullptr;        // [4^C / 128] tile summaries of d_lab_ (mw::ring_bits)
+    int32_t* d_prop_src_ = nullptr;     // the subtree (node of level C + 1) of each point source
     uint8_t* d_act_ = nullptr;          // [4^(C+1)] activity marks of this step
     uint8_t* d_prop_ = nullptr;         // [4^(C+1)] proposal of this step
     uint8_t* d_sig5_ = nullptr;         // [4^(C+1)] flags of each subtree's two parent levels, last step
@@ -330,7 +331,10 @@ private:
     mw::PropMask prop_mask() const { return mw::PropMask{prop_apply_ ? d_prop_ : nullptr, prop_C_ + 1}; }
     template <bool FULL> void encode_tree(const mw::Hier<T>& h, T eps)
     {
-        const mw::PropMask pm = prop_mask();
+        // the scale re-encode between the RK stages also visits the subtrees whose leaves
+        // stage 1 updated (stage 2 reads their parents as neighbours)
+        mw::PropMask pm = prop_mask();
+        if (!FULL && pm.prop) pm.act = d_act_;
         for (int level = L_ - 1; level > mw::kBandMaxLevel; --level)
         {
             if (folded_below(level)) continue;
@@ -749,6 +753,12 @@ template <typename T> mwdg2_status Sim<T>::enqueue_device()
                                                                                         &sc_->status);
             ++launches_;
         }
+        if (prop_learned_)
+        {
+            mw::k_prop_force<<<grid_for(prop_nC_, 256, 2 * (solver_blocks_ / 8)), 256, 0, st_>>>(
+                d_prop_, d_lab_, prop_nC_, d_prop_src_, (int)cs_.srcs.size());
+            ++launches_;
+        }
     }
     if (remesh) encode_tree<true>(hr_, eps);
     rec(2);
@@ -1016,6 +1026,13 @@ template <typename T> mwdg2_status Sim<T>::prop_alloc()
     const size_t nring = (size_t)std::max<int64_t>(1, prop_nC_ / mw::kPropTile);
     if (mwdg2_status s = dalloc(d_ring_, nring)) return s;
     CU(cudaMemset(d_ring_, 0xff, nring * sizeof(uint16_t)));   // every tile runs until labels exist
+    {
+        std::vector<int32_t> nodes;
+        for (const auto& src : cs_.srcs) nodes.push_back(src.code >> (2 * (L_ - (prop_C_ + 1))));
+        if (mwdg2_status s = dalloc(d_prop_src_, std::max<size_t>(1, nodes.size()))) return s;
+        if (!nodes.empty())
+            CU(cudaMemcpy(d_prop_src_, nodes.data(), sizeof(int32_t) * nodes.size(), cudaMemcpyHostToDevice));
+    }
     if (mwdg2_status s = dalloc(lf_.same, F_)) return s;
     CU(cudaMemset(lf_.same, 0, F_));
     if (mwdg2_status s = dalloc(clean_, F_)) return s;
@@ -1611,7 +1628,6 @@ public:
     ~Group() override
     {
         if (exec_) cudaGraphExecDestroy(exec_);
-        if (d_tab_) cudaFree(d_tab_);
         if (d_on_) cudaFree(d_on_);
         if (d_map_) cudaFree(d_map_);
         if (h_map_) cudaFreeHost(h_map_);
@@ -1644,11 +1660,12 @@ public:
         cap_dry_ = capacity(mw::k_members_stage_dry<T, 1>, 256);
         cap_list_ = capacity(mw::k_members_stage_list<T, 1>, mw::kSolverThreads);
         cap_leaf_ = capacity(mw::k_members_stage2_maxh<T>, 256);
-        std::vector<mw::MemberArgs<T>> tab(n_);
+        if (n_ > mw::MemberTable<T>::kMax) return set_err(MWDG2_ERR_STATE, "batch group larger than its table");
+        tab_ = std::make_unique<mw::MemberTable<T>>();
         for (int k = 0; k < n_; ++k)
         {
             const Sim<T>& m = *ms[k];
-            mw::MemberArgs<T>& a = tab[k];
+            mw::MemberArgs<T>& a = tab_->m[k];
             a.sc = m.sc_;
             a.sc_host = m.sc_host_;
             a.scal_bytes = (int)m.scal_bytes_;
@@ -1676,8 +1693,6 @@ public:
             a.stage_out = m.d_stage_out_;
             np_max_ = std::max(np_max_, a.np);
         }
-        CU(cudaMalloc(&d_tab_, sizeof(mw::MemberArgs<T>) * n_));
-        CU(cudaMemcpy(d_tab_, tab.data(), sizeof(mw::MemberArgs<T>) * n_, cudaMemcpyHostToDevice));
         CU(cudaMalloc(&d_on_, n_));
         const size_t nmap = (size_t)mw::kBlockMaps * (n_ + 1);
         CU(cudaMalloc(&d_map_, sizeof(int32_t) * nmap));
@@ -1767,12 +1782,12 @@ private:
         for (int level = L_ - 1; level > mw::kBandMaxLevel; --level)
         {
             mw::k_members_encode_level<T, FULL><<<dim3(blocks((int64_t)1 << (2 * level), 256), n_), 256, 0, st_>>>(
-                d_tab_, d_on_, L_, level);
+                *tab_, d_on_, L_, level);
             ++launches_;
         }
         for (const auto& b : bands_)
         {
-            mw::k_members_encode_band<T, FULL><<<dim3(b.grid, n_), 256, 0, st_>>>(d_tab_, d_on_, L_, b.lo, b.depth);
+            mw::k_members_encode_band<T, FULL><<<dim3(b.grid, n_), 256, 0, st_>>>(*tab_, d_on_, L_, b.lo, b.depth);
             ++launches_;
         }
     }
@@ -1781,10 +1796,10 @@ private:
         const int32_t* leaves = d_map_;
         const int32_t* wet = d_map_ + STAGE * (n_ + 1);
         const int g = std::min(cap_wet_, std::min(cap_dry_, cap_leaf_)) + n_;
-        mw::k_members_stage_wet<T, STAGE><<<g, 256, 0, st_>>>(d_tab_, d_on_, leaves, n_);
+        mw::k_members_stage_wet<T, STAGE><<<g, 256, 0, st_>>>(*tab_, d_on_, leaves, n_);
         fork(ev_[2]);
-        mw::k_members_stage_list<T, STAGE><<<cap_list_ + n_, mw::kSolverThreads, 0, st2_>>>(d_tab_, d_on_, wet, n_);
-        mw::k_members_stage_dry<T, STAGE><<<g, 256, 0, st_>>>(d_tab_, d_on_, leaves, n_);
+        mw::k_members_stage_list<T, STAGE><<<cap_list_ + n_, mw::kSolverThreads, 0, st2_>>>(*tab_, d_on_, wet, n_);
+        mw::k_members_stage_dry<T, STAGE><<<g, 256, 0, st_>>>(*tab_, d_on_, leaves, n_);
         join(ev_[3]);
         launches_ += 3;
     }
@@ -1792,19 +1807,19 @@ private:
     // first with every RK stage over the wet list and no sparse level
     void enqueue()
     {
-        mw::k_members_open<T><<<dim3(1, n_), 128, 0, st_>>>(d_tab_, m_active_, d_on_, L_, m_map_, d_map_, n_);
+        mw::k_members_open<T><<<dim3(1, n_), 128, 0, st_>>>(*tab_, m_active_, d_on_, L_, m_map_, d_map_, n_);
         ++launches_;
         encode<true>();
         for (size_t k = bands_.size(); k-- > 0;)
         {
             const auto& b = bands_[k];
-            mw::k_members_decode_band<T><<<dim3(b.grid, n_), 256, 0, st_>>>(d_tab_, d_on_, L_, b.lo, b.depth);
+            mw::k_members_decode_band<T><<<dim3(b.grid, n_), 256, 0, st_>>>(*tab_, d_on_, L_, b.lo, b.depth);
             ++launches_;
         }
         for (int level = mw::kBandMaxLevel + 1; level <= L_ - 2; ++level)
         {
             mw::k_members_extra_sig<T><<<dim3(blocks((int64_t)1 << (2 * level - 2), 256), n_), 256, 0, st_>>>(
-                d_tab_, d_on_, L_, level);
+                *tab_, d_on_, L_, level);
             ++launches_;
         }
         const bool split = L_ - 1 > mw::kBandMaxLevel;
@@ -1814,27 +1829,27 @@ private:
             for (int level = mw::kBandMaxLevel + 1; level < L_; ++level)
             {
                 mw::k_members_decode_level<T><<<dim3(blocks((int64_t)1 << (2 * level), 256), n_), 256, 0, st2_>>>(
-                    d_tab_, d_on_, L_, level);
+                    *tab_, d_on_, L_, level);
                 ++launches_;
             }
         }
-        mw::k_members_tile_count<T><<<dim3(ntiles_, n_), 96, 0, st_>>>(d_tab_, d_on_, L_);
-        mw::k_members_tile_scan<T><<<dim3(1, n_), 1024, 0, st_>>>(d_tab_, d_on_, ntiles_);
-        mw::k_members_tile_emit<T><<<dim3(ntiles_, n_), mw::kTileThreads, 0, st_>>>(d_tab_, d_on_, L_);
+        mw::k_members_tile_count<T><<<dim3(ntiles_, n_), 96, 0, st_>>>(*tab_, d_on_, L_);
+        mw::k_members_tile_scan<T><<<dim3(1, n_), 1024, 0, st_>>>(*tab_, d_on_, ntiles_);
+        mw::k_members_tile_emit<T><<<dim3(ntiles_, n_), mw::kTileThreads, 0, st_>>>(*tab_, d_on_, L_);
         launches_ += 3;
         if (split) join(ev_[1]);
         stage<1>();
         encode<false>();
         mw::k_members_stage2_maxh<T><<<std::min(cap_wet_, std::min(cap_dry_, cap_leaf_)) + n_, 256, 0, st_>>>(
-            d_tab_, d_on_, d_map_, n_);
+            *tab_, d_on_, d_map_, n_);
         ++launches_;
         stage<2>();
         if (np_max_ > 0)
         {
-            mw::k_members_sample<T><<<dim3((32 * np_max_ + 127) / 128, n_), 128, 0, st_>>>(d_tab_, d_on_, L_, ntiles_);
+            mw::k_members_sample<T><<<dim3((32 * np_max_ + 127) / 128, n_), 128, 0, st_>>>(*tab_, d_on_, L_, ntiles_);
             ++launches_;
         }
-        mw::k_members_scalars_out<T><<<dim3(1, n_), 128, 0, st_>>>(d_tab_, d_on_);
+        mw::k_members_scalars_out<T><<<dim3(1, n_), 128, 0, st_>>>(*tab_, d_on_);
         ++launches_;
     }
 
@@ -1842,7 +1857,7 @@ private:
     int n_ = 0, L_ = 0, ntiles_ = 0, np_max_ = 0, launches_ = 0;
     int cap_wet_ = 1, cap_dry_ = 1, cap_list_ = 1, cap_leaf_ = 1;
     std::vector<typename Sim<T>::Band> bands_;
-    mw::MemberArgs<T>* d_tab_ = nullptr;
+    std::unique_ptr<mw::MemberTable<T>> tab_;   // passed by value to every launch
     uint8_t* d_on_ = nullptr;
     uint8_t* h_active_ = nullptr;   // pinned, mapped
     uint8_t* m_active_ = nullptr;   // its device address
@@ -1872,6 +1887,14 @@ struct mwdg2_batch
     std::vector<std::unique_ptr<GroupBase>> groups;
     std::vector<int> group_of;
     bool grouped = false;
+    // Size classes hold members of at most this max_ref_lvl (mwdg2_batch_group_max_level;
+    // 0: none). Off by default: on the 64-member ensemble (FP32, 512^2 to 2048^2) the members
+    // stepped as their own CUDA graphs on their own streams, launched from host threads, beat
+    // one launch per kernel for a whole class at every size (against stepping the members one
+    // after another: 512^2 1.68x against 1.46x, 1024^2 1.26x against 1.08x, 2048^2 1.12x
+    // against 0.97x): a class launch lasts as long as its slowest member's part, while
+    // independent member graphs fill each other's gaps.
+    int group_max_level = 0;
 };
 
 namespace {
@@ -1927,32 +1950,39 @@ mwdg2_status regroup(mwdg2_batch* b)
         if (b->done[i]) continue;
         if (b->members[i]->impl->first_step()) return MWDG2_OK;   // not yet
         const int k = b->members[i]->impl->group_key();
-        if (k >= 0) by_key[k].push_back(i);
+        if (k >= 0 && (k & 0xff) <= b->group_max_level) by_key[k].push_back(i);
     }
     for (auto& kv : by_key)
     {
-        if (kv.second.size() < 2) continue;
-        std::unique_ptr<GroupBase> g;
-        if (kv.first & (1 << 8))
+        const bool dbl = (kv.first & (1 << 8)) != 0;
+        const size_t cap = dbl ? mw::MemberTable<double>::kMax : mw::MemberTable<float>::kMax;
+        // a class larger than one table is stepped as several groups
+        for (size_t c0 = 0; c0 < kv.second.size(); c0 += cap)
         {
-            std::vector<Sim<double>*> ms;
-            for (int i : kv.second) ms.push_back(static_cast<Sim<double>*>(b->members[i]->impl.get()));
-            auto* gg = new Group<double>();
-            g.reset(gg);
-            if (mwdg2_status st = gg->build(ms)) return st;
+            const std::vector<int> idx(kv.second.begin() + c0, kv.second.begin() + std::min(kv.second.size(), c0 + cap));
+            if (idx.size() < 2) continue;
+            std::unique_ptr<GroupBase> g;
+            if (dbl)
+            {
+                std::vector<Sim<double>*> ms;
+                for (int i : idx) ms.push_back(static_cast<Sim<double>*>(b->members[i]->impl.get()));
+                auto* gg = new Group<double>();
+                g.reset(gg);
+                if (mwdg2_status st = gg->build(ms)) return st;
+            }
+            else
+            {
+                std::vector<Sim<float>*> ms;
+                for (int i : idx) ms.push_back(static_cast<Sim<float>*>(b->members[i]->impl.get()));
+                auto* gg = new Group<float>();
+                g.reset(gg);
+                if (mwdg2_status st = gg->build(ms)) return st;
+            }
+            g->idx = idx;
+            g->key = kv.first;
+            for (int i : idx) b->group_of[i] = (int)b->groups.size();
+            b->groups.push_back(std::move(g));
         }
-        else
-        {
-            std::vector<Sim<float>*> ms;
-            for (int i : kv.second) ms.push_back(static_cast<Sim<float>*>(b->members[i]->impl.get()));
-            auto* gg = new Group<float>();
-            g.reset(gg);
-            if (mwdg2_status st = gg->build(ms)) return st;
-        }
-        g->idx = kv.second;
-        g->key = kv.first;
-        for (int i : kv.second) b->group_of[i] = (int)b->groups.size();
-        b->groups.push_back(std::move(g));
     }
     b->grouped = true;
     return MWDG2_OK;
@@ -2222,6 +2252,15 @@ mwdg2_status mwdg2_batch_run(mwdg2_batch* b, int64_t max_batch_steps, int64_t* b
     if (batch_steps) *batch_steps = bs;
     if (member_steps) *member_steps = ms;
     if (updates) *updates = upd;
+    return MWDG2_OK;
+}
+
+mwdg2_status mwdg2_batch_group_max_level(mwdg2_batch* b, int level)
+{
+    if (!b) return set_err(MWDG2_ERR_ARG, "null batch");
+    b->group_max_level = level;
+    b->groups.clear();   // formed again at the next step
+    b->grouped = false;
     return MWDG2_OK;
 }
 

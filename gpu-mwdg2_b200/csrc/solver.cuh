@@ -492,7 +492,7 @@ __device__ __forceinline__ void k_stage_dry_body(int bid, int nb, Leaves<T> lf, 
         if (pm.prop && (STAGE == 2 || clean))
         {
             const int lv = lf.lvl[i];
-            const bool left_out = lv >= pm.level && !pm.prop[(a - lvl_idx(lv)) >> (2 * (lv - pm.level))];
+            const bool left_out = lv >= pm.level && pm_out(pm, (a - lvl_idx(lv)) >> (2 * (lv - pm.level)));
             if (STAGE == 1 && left_out && lf.same[i] && clean[i])
             {
                 dry[i] = 2;
@@ -543,7 +543,7 @@ __device__ __forceinline__ void k_stage_dry_body(int bid, int nb, Leaves<T> lf, 
     }
 }
 template <typename T, int STAGE>
-__global__ void __launch_bounds__(256) k_stage_dry(Leaves<T> lf, Hier<T> hin, Hier<T> hout, Scalars<T>* sc, Params<T> P,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 5) k_stage_dry(Leaves<T> lf, Hier<T> hin, Hier<T> hout, Scalars<T>* sc, Params<T> P,
                                                    bool friction, uint8_t* dry, const uint8_t* dry1, PropMask pm,
                                                    const uint8_t* clean = nullptr)
 {

@@ -86,6 +86,7 @@ def lib():
         L.mwdg2_batch_step.argtypes = [vp, dp, i64p, i32p]
         L.mwdg2_batch_run.argtypes = [vp, ctypes.c_int64, i64p, i64p, i64p]
         L.mwdg2_batch_member.argtypes = [vp, ctypes.c_int, ctypes.POINTER(vp)]
+        L.mwdg2_batch_group_max_level.argtypes = [vp, ctypes.c_int]
         L.mwdg2_batch_destroy.argtypes = [vp]
         fp = ctypes.POINTER(ctypes.c_float)
         L.mwdg2_mlp_forward.argtypes = [fp, fp, ctypes.c_int, ctypes.c_int64, ctypes.c_float, fp, u8p]
@@ -112,7 +113,7 @@ def lib():
                      "mwdg2_get_leaves", "mwdg2_get_state", "mwdg2_get_sig", "mwdg2_get_hierarchy",
                      "mwdg2_read_stage", "mwdg2_last_step_timing", "mwdg2_set_timing", "mwdg2_last_step_counters",
                      "mwdg2_batch_create",
-                     "mwdg2_batch_step", "mwdg2_batch_run", "mwdg2_batch_member"):
+                     "mwdg2_batch_step", "mwdg2_batch_run", "mwdg2_batch_member", "mwdg2_batch_group_max_level"):
             getattr(L, name).restype = ctypes.c_int
         _lib = L
     return _lib
@@ -351,6 +352,11 @@ class Batch:
         bs, ms, upd = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
         _check(lib().mwdg2_batch_run(self._h, max_batch_steps, ctypes.byref(bs), ctypes.byref(ms), ctypes.byref(upd)))
         return bs.value, ms.value, upd.value
+
+    def group_max_level(self, level: int):
+        """Size classes (one launch per kernel for all their members) hold members of at
+        most this max_ref_lvl (default 0: none)."""
+        _check(lib().mwdg2_batch_group_max_level(self._h, level))
 
     def member(self, i: int) -> Simulation:
         h = ctypes.c_void_p()

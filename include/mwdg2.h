@@ -174,6 +174,13 @@ mwdg2_status mwdg2_batch_step(mwdg2_batch* b, double* dts, int64_t* leaves, int3
 mwdg2_status mwdg2_batch_run(mwdg2_batch* b, int64_t max_batch_steps, int64_t* batch_steps, int64_t* member_steps,
                              int64_t* updates);
 
+/* Members of the batch that are MWDG2, past their first step and of the same max_ref_lvl
+ * (at most `level`) and precision step together with one launch per kernel for the whole
+ * size class; the others step as their own CUDA graphs on their own streams. Default 0 (no
+ * classes): own graphs on own streams measured faster at every member size tried. Takes
+ * effect at the next step. */
+mwdg2_status mwdg2_batch_group_max_level(mwdg2_batch* b, int level);
+
 /* Member i as a simulation handle for the getters above (mwdg2_info, mwdg2_get_state, ...).
  * The batch owns it: do not pass it to mwdg2_destroy or step it on its own. */
 mwdg2_status mwdg2_batch_member(mwdg2_batch* b, int i, mwdg2_sim** out);

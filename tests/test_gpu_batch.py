@@ -5,10 +5,12 @@ leaf's update is independent of it and the dt and maxima reductions are exact), 
 member of a batch must reproduce a standalone run of its case bit for bit: the same dt
 sequence, leaf grids and states. The members differ in size, solver, friction and limiter,
 and one ends earlier than the others. From their second step on, members of one size class
-(MWDG2, the same max_ref_lvl and precision) take one launch per kernel for the whole class
-(a member table, one member per blockIdx.y); the others step on their own. The second test
-holds a class of three max_ref_lvl 11 members (per-level kernels above the bands, the value
-decode beside the leaf topology) to their standalone runs."""
+(MWDG2, the same max_ref_lvl and precision, up to the batch's class level; none by default)
+take one launch per kernel for the whole class (a member table, one member per blockIdx.y);
+the others step on their own. The first test runs without and with classes (the two L = 7
+MWDG2 members form one); the second holds a class of three max_ref_lvl 11 members (per-level
+kernels above the bands, the value decode beside the leaf topology) to their standalone
+runs."""
 import os
 
 import numpy as np
@@ -33,8 +35,8 @@ def _members(root: str):
     return out
 
 
-@pytest.mark.parametrize("precision", [64, 32])
-def test_batch_members_equal_standalone_runs(tmp_path, precision):
+@pytest.mark.parametrize("precision,group_level", [(64, 0), (32, 0), (64, 9), (32, 9)])
+def test_batch_members_equal_standalone_runs(tmp_path, precision, group_level):
     pars = _members(str(tmp_path))
     steps = 25
     alone = []
@@ -49,6 +51,7 @@ def test_batch_members_equal_standalone_runs(tmp_path, precision):
         alone.append((dts, s.leaves(), s.state()))
         s.close()
     with mwdg2_b200.Batch(pars, precision=precision) as b:
+        b.group_max_level(group_level)
         dts = [[] for _ in pars]
         for _ in range(steps):
             k, dt, n = b.step()
@@ -99,6 +102,7 @@ def test_size_class_members_equal_standalone_runs(tmp_path, precision):
     steps = 8
     alone = _run_alone(pars, precision, steps)
     with mwdg2_b200.Batch(pars, precision=precision) as b:
+        b.group_max_level(L)   # classes hold members up to 512^2 by default
         dts = [[] for _ in pars]
         for _ in range(steps):
             k, dt, n = b.step()
