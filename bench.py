@@ -576,19 +576,20 @@ def run_learned(a):
         sim.close()
         return out
 
+    # the plain FP64 run is the depth reference; plain and learned run in --precision
     ref = run(64, False)
-    plain = run(32, False)
-    learned = run(32, True)
-    peak, peak_kind = peaks()
+    plain = ref if a.precision == 64 else run(a.precision, False)
+    learned = run(a.precision, True)
+    fp = f"FP{a.precision}"
     lines = []
     for name, r in (("plain", plain), ("learned", learned)):
         err = float(np.max(np.abs(r["depth"] - ref["depth"])))
-        line = {"metric": METRIC + f" ({name} FP32 vs plain FP64 depth)", "value": r["leaves"] / (r["ms"] / 1e3),
+        line = {"metric": METRIC + f" ({name} {fp} vs plain FP64 depth)", "value": r["leaves"] / (r["ms"] / 1e3),
                 "unit": UNIT, "n_gpus": 1, "steps": r["steps"], "warmup": 0, "ms_per_step": r["ms"] / r["steps"],
-                "higher_is_better": True, "impl": f"ours-{name}", "dtype": "f32",
+                "higher_is_better": True, "impl": f"ours-{name}", "dtype": f"f{a.precision}",
                 "data": "synthetic (seeded fBm DEM, no network)",
                 "config": {"workload": f"fBm catchment {1 << a.level}^2 (max_ref_lvl {a.level}) run from t = 0 to "
-                                       f"{a.eval_time:g} s (the hydrograph peak), MWDG2 FP32",
+                                       f"{a.eval_time:g} s (the hydrograph peak), MWDG2 {fp}",
                            "proposal": "none" if name == "plain" else
                                        f"trained MLP ({a.proposal.split('/')[-1]}), judge every {a.judge_every} steps",
                            "depth_reference": "the same case in FP64, plain"},
