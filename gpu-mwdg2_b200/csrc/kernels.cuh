@@ -56,6 +56,7 @@ template <typename T> struct Scalars
     // were active in the step, left out though they needed the step, proposed, and needed
     uint32_t prop_active, prop_missed, prop_proposed, prop_needed;
     uint32_t prop_frozen;             // dry leaves of left-out subtrees the RK stages left as they stood
+    uint32_t step_tag;                // 1, 2, ...: the step's number for the frozen-leaf tags
 };
 
 // The subtrees below the nodes of level `level` (the proposal level) that a step's encode and
@@ -208,6 +209,7 @@ template <typename T> __device__ __forceinline__ void step_begin(Scalars<T>* sc,
     sc->prop_proposed = 0;
     sc->prop_needed = 0;
     sc->prop_frozen = 0;
+    sc->step_tag += 1u;
 }
 template <typename T> __global__ void k_step_begin(Scalars<T>* sc, bool carry) { step_begin(sc, carry); }
 

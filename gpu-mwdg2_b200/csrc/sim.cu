@@ -182,10 +182,9 @@ private:
     int grid_leaf_ = 0, grid_wet_ = 0, grid_dry_ = 0, grid_stage_ = 0;
     uint8_t* dry_ = nullptr;            // dry marks of RK stage 1 (k_stage_wet -> k_stage_dry)
     uint8_t* dry2_ = nullptr;           // and of stage 2
-    // learned proposal: leaves dry in both stages of the last step (k_stage_wet<2>), valid
-    // (clean_ok_) when both stages of that step took the wet list
-    uint8_t* clean_ = nullptr;
-    bool step_lists_ = false, clean_ok_ = false;
+    // learned proposal: per hierarchy index, the tag of the last step in which the leaf there
+    // was dry in both stages (k_stage_wet<2>, on steps whose two stages take the wet list)
+    uint32_t* clean_tag_ = nullptr;
     cudaStream_t st2_ = nullptr;        // the wet-list kernels, beside the dry-leaf writers
     cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
     // the value decode of the levels above the bands, beside the leaf topology (its own
@@ -209,7 +208,7 @@ private:
     {
         int key = (mw_ && use_list(1) ? 1 : 0) | (mw_ && use_list(2) ? 2 : 0) | (timed_ ? 1 << 24 : 0) |
                   (!mw_ && flip_ ? 1 << 23 : 0) | (prop_rec_ ? 1 << 22 : 0) | (prop_learned_ ? 1 << 21 : 0) |
-                  (prop_apply_ ? 1 << 20 : 0) | (clean_ok_ ? 1 << 19 : 0);
+                  (prop_apply_ ? 1 << 20 : 0);
         for (int level = mw::kBandMaxLevel + 1; level < L_; ++level)
             if (sparse_level(level)) key |= 4 << (level - mw::kBandMaxLevel - 1);
         return key;
@@ -295,17 +294,18 @@ private:
         if (use_list(STAGE))
         {
             uint8_t* marks = STAGE == 1 ? dry_ : dry2_;
-            // learned proposal: stage 2 records which leaves stayed dry in both stages (clean_),
-            // and leaves left out by the proposal are frozen only when both stages take the list
-            const mw::PropMask pm = (use_list(1) && use_list(2)) ? prop_mask() : mw::PropMask{};
+            // learned proposal: stage 2 tags the leaves that stayed dry in both stages, and
+            // leaves left out by the proposal are frozen, when both stages take the list
+            const bool lists = use_list(1) && use_list(2);
+            const mw::PropMask pm = lists ? prop_mask() : mw::PropMask{};
             mw::k_stage_wet<T, STAGE><<<grid_wet_, 256, 0, st_>>>(lf_, hin, sc_, P_, d_args_, marks, wet_list_, dry_,
-                                                                  STAGE == 2 ? clean_ : nullptr);
+                                                                  STAGE == 2 && lists ? clean_tag_ : nullptr);
             cudaEventRecord(ev_fork_, st_);
             cudaStreamWaitEvent(st2_, ev_fork_, 0);
             mw::k_mwdg2_stage<T, STAGE, true><<<grid_stage_, mw::kSolverThreads, 0, st2_>>>(lf_, hin, hout, sc_, P_,
                                                                                            d_args_, fric, wet_list_);
             mw::k_stage_dry<T, STAGE><<<grid_dry_, 256, 0, st_>>>(lf_, hin, hout, sc_, P_, fric, marks, dry_, pm,
-                                                                  STAGE == 1 && clean_ok_ ? clean_ : nullptr);
+                                                                  STAGE == 1 ? clean_tag_ : nullptr);
             cudaEventRecord(ev_join_, st2_);
             cudaStreamWaitEvent(st_, ev_join_, 0);
             launches_ += 3;
@@ -642,7 +642,6 @@ template <typename T> void Sim<T>::prepare_args()
 template <typename T> mwdg2_status Sim<T>::launch_step_device()
 {
     prepare_args();
-    step_lists_ = mw_ && !first_ && use_list(1) && use_list(2);
     // step timing: stream events right around the step's device work (after any capture)
     auto rec_step = [&](int k) { if (timing_mode_ == 1) cudaEventRecord(ev_step_[k], st_); };
     auto direct = [&]() {
@@ -986,7 +985,6 @@ template <typename T> mwdg2_status Sim<T>::finish_step(double* dt_out, int64_t* 
     }
     n_leaves_ = sc_host_->n_leaves;
     dt_ = sc_host_->dt_min;
-    clean_ok_ = step_lists_ && clean_ != nullptr;
     first_ = false;
     timestep_++;
     if (dt_out) *dt_out = (double)dt_;
@@ -1035,9 +1033,8 @@ template <typename T> mwdg2_status Sim<T>::prop_alloc()
     }
     if (mwdg2_status s = dalloc(lf_.same, F_)) return s;
     CU(cudaMemset(lf_.same, 0, F_));
-    if (mwdg2_status s = dalloc(clean_, F_)) return s;
-    CU(cudaMemset(clean_, 0, F_));
-    clean_ok_ = false;
+    if (mwdg2_status s = dalloc(clean_tag_, n_all_)) return s;
+    CU(cudaMemset(clean_tag_, 0, sizeof(uint32_t) * (size_t)n_all_));
     if (mwdg2_status s = dalloc(d_act_, (size_t)prop_nC_ * 4)) return s;
     if (mwdg2_status s = dalloc(d_prop_, (size_t)prop_nC_ * 4)) return s;
     if (mwdg2_status s = dalloc(d_sig5_, (size_t)prop_nC_ * 4)) return s;
@@ -1086,7 +1083,7 @@ mwdg2_status Sim<T>::proposal_enable(const float* params, int judge_every, float
     prop_judge_every_ = judge_every;
     prop_thr_ = threshold;
     prop_bound_ = miss_bound;
-    prop_since_judge_ = 0;
+    prop_since_judge_ = judge_every;   // the first step after enabling is a judge step
     prop_fallback_left_ = 0;
     return proposal_record(prop_rec_);
 }

@@ -393,7 +393,7 @@ __device__ __forceinline__ void put_leaf_fv1(const Hier<T>& hout, int a, T h, T 
 template <typename T, int STAGE>
 __device__ __forceinline__ void k_stage_wet_body(int bid, int nb, Leaves<T> lf, Hier<T> hin, Scalars<T>* sc, Params<T> P,
                                                    const StepArgs<T>* args, uint8_t* dry, int32_t* wet,
-                                                   const uint8_t* dry1 = nullptr, uint8_t* clean = nullptr)
+                                                   const uint8_t* dry1 = nullptr, uint32_t* clean_tag = nullptr)
 {
     const T dt = args->dt;
     const Bnd<T>& B = args->B;
@@ -430,7 +430,7 @@ __device__ __forceinline__ void k_stage_wet_body(int bid, int nb, Leaves<T> lf, 
             any_dry |= is_dry;
             dry[i] = is_dry ? 1 : 0;
             if (STAGE == 1 && is_dry) lf.un[0][i] = h0;
-            if (STAGE == 2 && clean) clean[i] = (is_dry && dry1[i]) ? 1 : 0;
+            if (STAGE == 2 && clean_tag && is_dry && dry1[i]) clean_tag[a] = sc->step_tag;
         }
         // warp-aggregated append
         const unsigned mask = __ballot_sync(0xffffffffu, is_wet);
@@ -445,9 +445,9 @@ __device__ __forceinline__ void k_stage_wet_body(int bid, int nb, Leaves<T> lf, 
 template <typename T, int STAGE>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4) k_stage_wet(Leaves<T> lf, Hier<T> hin, Scalars<T>* sc, Params<T> P,
                                                    const StepArgs<T>* args, uint8_t* dry, int32_t* wet,
-                                                   const uint8_t* dry1 = nullptr, uint8_t* clean = nullptr)
+                                                   const uint8_t* dry1 = nullptr, uint32_t* clean_tag = nullptr)
 {
-    k_stage_wet_body<T, STAGE>(blockIdx.x, gridDim.x, lf, hin, sc, P, args, dry, wet, dry1, clean);
+    k_stage_wet_body<T, STAGE>(blockIdx.x, gridDim.x, lf, hin, sc, P, args, dry, wet, dry1, clean_tag);
 }
 
 // The dry leaves of one RK stage, marked by k_stage_wet (bandwidth-bound; it runs beside
@@ -458,18 +458,21 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4) k_stage_wet(Leave
 // pm (learned refinement proposal, applied steps with both stages over the wet list): a
 // leaf inside a subtree the proposal left out (its subtree's encode and decode are skipped
 // too) keeps its state as it stands in the hierarchy where nothing has changed it.
-// Stage 1 skips such a leaf when it is dry, its position holds the same leaf as in the last
-// step (lf.same) and it was dry in both stages of the last step (clean, from the last
-// step's stage-2 wet test; null when that step did not record it): its U^n copy (un) and
-// its U* in the stage hierarchy are then still the ones written when it last changed.
-// Stage 1 marks the leaves it skips (dry[i] = 2); stage 2 writes nothing for such a leaf that
-// is dry in stage 2 as well (dry1: stage 1's marks) and only adds it to the maxima, so a
-// leaf's state is re-inserted at least once after it last changed.
+// Stage 1 leaves such a dry leaf's U* in the stage hierarchy as it stands when the leaf was
+// a leaf dry in both stages of the last step (clean_tag[a], at its hierarchy index, is the
+// last step's tag: written by that step's stage-2 wet test; null when that step did not
+// record it): U* is then still the one written when the leaf last changed. Its U^n copy
+// (un, by leaf position) is rewritten only where the position now holds another leaf than
+// in the last step (lf.same). Stage 1 marks the leaves it freezes (dry[i] = 2); stage 2
+// writes nothing for such a leaf that is dry in stage 2 as well (dry1: stage 1's marks) and
+// only adds it to the maxima, so a leaf's state is re-inserted at least once after it last
+// changed.
 template <typename T, int STAGE>
 __device__ __forceinline__ void k_stage_dry_body(int bid, int nb, Leaves<T> lf, Hier<T> hin, Hier<T> hout, Scalars<T>* sc, Params<T> P,
                                                    bool friction, uint8_t* dry, const uint8_t* dry1, PropMask pm,
-                                                   const uint8_t* clean = nullptr)
+                                                   const uint32_t* clean_tag = nullptr)
 {
+    const uint32_t last_tag = sc->step_tag - 1u;
     const int n = sc->n_leaves;
     const int stride = nb * blockDim.x;
     StateMax<T> mx;
@@ -489,15 +492,17 @@ __device__ __forceinline__ void k_stage_dry_body(int bid, int nb, Leaves<T> lf, 
             a_next = lf.act[i + stride];
         }
         if (!is_dry) continue;
-        if (pm.prop && (STAGE == 2 || clean))
+        bool keep_ustar = false;
+        if (pm.prop && (STAGE == 2 || clean_tag))
         {
             const int lv = lf.lvl[i];
             const bool left_out = lv >= pm.level && pm_out(pm, (a - lvl_idx(lv)) >> (2 * (lv - pm.level)));
-            if (STAGE == 1 && left_out && lf.same[i] && clean[i])
+            if (STAGE == 1 && left_out && clean_tag[a] == last_tag)
             {
                 dry[i] = 2;
                 ++frozen;
-                continue;
+                if (lf.same[i]) continue;
+                keep_ustar = true;   // un only
             }
             if (STAGE == 2 && left_out && dry1[i] == 2)
             {
@@ -525,6 +530,7 @@ __device__ __forceinline__ void k_stage_dry_body(int bid, int nb, Leaves<T> lf, 
             }
 #pragma unroll
             for (int k = 1; k < 9; ++k) lf.un[k][i] = u[k];
+            if (keep_ustar) continue;
         }
         else
         {
@@ -545,9 +551,9 @@ __device__ __forceinline__ void k_stage_dry_body(int bid, int nb, Leaves<T> lf, 
 template <typename T, int STAGE>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 5) k_stage_dry(Leaves<T> lf, Hier<T> hin, Hier<T> hout, Scalars<T>* sc, Params<T> P,
                                                    bool friction, uint8_t* dry, const uint8_t* dry1, PropMask pm,
-                                                   const uint8_t* clean = nullptr)
+                                                   const uint32_t* clean_tag = nullptr)
 {
-    k_stage_dry_body<T, STAGE>(blockIdx.x, gridDim.x, lf, hin, hout, sc, P, friction, dry, dry1, pm, clean);
+    k_stage_dry_body<T, STAGE>(blockIdx.x, gridDim.x, lf, hin, hout, sc, P, friction, dry, dry1, pm, clean_tag);
 }
 
 // One RK2 stage of MWDG2, reading the hierarchy `hin` and writing each leaf's result into

@@ -264,8 +264,9 @@ mwdg2_status mwdg2_proposal_record(mwdg2_sim* sim, int on);
 /* Let the MLP with `params` (MWDG2_MLP_PARAMS floats, copied) choose, from the next step on,
  * the child subtrees of the coarse level that the encode, decode and scale re-encode visit
  * (logit > threshold); subtrees left out keep their flags and values, and so do their
- * leaves that stay dry through the step (wet leaves are updated everywhere). Every
- * judge_every-th step (0: never) runs in full as the judge. The subtrees that needed a step
+ * leaves that stay dry through the step (wet leaves are updated everywhere). The first step
+ * after this call and every judge_every-th step after it (0: never) run in full as the
+ * judge. The subtrees that needed a step
  * are those whose leaves it updated or whose flags gained significance; when the proposal
  * left out more than the fraction miss_bound of them (counted as at least 0.1 % of all
  * subtrees), the next judge_every steps run in full. params = NULL switches the proposal
