@@ -59,6 +59,10 @@ def parse():
     ap.add_argument("--proposal", default=os.path.join(ROOT, "gpu-mwdg2_b200", "proposal_mlp.npz"),
                     help="learned: trained MLP parameters")
     ap.add_argument("--members", type=int, default=64)
+    ap.add_argument("--decode", default="reference", choices=["reference", "keep"],
+                    help="decode of the timed run (mwdg2_set_decode_mode): reference (bit for bit the "
+                         "reference build's) or keep (children of encoded parents keep their values); the "
+                         "catchment line also carries a keep-values window beside the reference one")
     ap.add_argument("--peak-time", type=float, default=1800.0,
                     help="catchment: a second timing window starting at this simulated time (the hydrograph "
                          "peak); <= 0 skips it")
@@ -82,7 +86,7 @@ def workload(a) -> dict:
     return {"workload": f"fBm catchment {1 << a.level}^2 finest cells (max_ref_lvl {a.level}), 2 m cells, "
                         "Hurst 0.8, relief 0-30 m, Manning 0.03, dry start, west point inflow 50 m3/s peak at 30 min, "
                         "epsilon 1e-3",
-            "solver": a.solver, "precision": f"fp{a.precision}", "max_ref_lvl": a.level,
+            "solver": a.solver, "precision": f"fp{a.precision}", "max_ref_lvl": a.level, "decode": a.decode,
             "steps_from": "simulation start (steps W+1..W+K of the run)",
             "l2": "inputs larger than L2 (hierarchy arrays >= 1 GB)"}
 
@@ -481,19 +485,26 @@ def par_ending_at(par: str, t_end: float) -> str:
     return out
 
 
-def learned_window(a, par, t_from, t_end, depth_plain, value_plain, name, volume_plain=None) -> dict:
-    """A window of the plain run again with the learned refinement proposal: a second
-    simulation of the same case (ending at t_end, where the plain run's window ended) with the
-    trained MLP choosing the subtrees the step visits (judge every --judge-every steps),
-    stepped untimed to t_from, then W warm-up and K timed steps as the plain window's; its
-    active-cell updates/s, and after stepping on to t_end the largest depth difference from the
-    plain run at t_end over every finest cell (cell-centre depths)."""
+def learned_window(a, par, t_from, t_end, depth_plain, value_plain, name, volume_plain=None,
+                   mode="learned") -> dict:
+    """A window of the plain run again with the learned refinement proposal (mode "learned")
+    or with the keep-values decode (mode "keep"): a second simulation of the same case
+    (ending at t_end, where the plain run's window ended), for "learned" with the trained MLP
+    choosing the subtrees the step visits (judge every --judge-every steps), stepped untimed to
+    t_from, then W warm-up and K timed steps as the plain window's; its active-cell updates/s,
+    and after stepping on to t_end the largest depth difference from the plain run at t_end
+    over every finest cell (cell-centre depths). Both take the decode of --decode."""
     import numpy as np
     import mwdg2_b200
-    z = np.load(a.proposal)
-    train = json.loads(str(z["summary"]))
     sim = mwdg2_b200.Simulation(par_ending_at(par, t_end), precision=a.precision, timing="step")
-    sim.proposal_enable(z["params"], judge_every=a.judge_every, threshold=train["threshold"], miss_bound=0.02)
+    if a.decode == "keep":
+        sim.set_decode_mode("keep")
+    if mode == "learned":
+        z = np.load(a.proposal)
+        train = json.loads(str(z["summary"]))
+        sim.proposal_enable(z["params"], judge_every=a.judge_every, threshold=train["threshold"], miss_bound=0.02)
+    else:
+        sim.set_decode_mode("keep")
     ok = True
     while ok and sim.info()["time"] < t_from:
         ok = sim.step()[0]
@@ -509,7 +520,7 @@ def learned_window(a, par, t_from, t_end, depth_plain, value_plain, name, volume
             leaves.append(n)
             c = sim.last_step_counters()
             wet.append((c["wet_stage1"], c["wet_stage2"]))
-    st = sim.proposal_stats()
+    st = sim.proposal_stats() if mode == "learned" else None
     while ok:
         ok = sim.step()[0]
     diff = float(np.max(np.abs(finest_depth(sim) - depth_plain)))
@@ -518,26 +529,32 @@ def learned_window(a, par, t_from, t_end, depth_plain, value_plain, name, volume
     sim.close()
     v = sum(leaves) / (sum(ms) / 1e3)
     n_mean = float(np.mean(leaves))
-    return {"value": v, "ms_per_step": sum(ms) / len(ms), "steps": len(ms), "vs_plain": v / value_plain,
-            "leaves_mean": n_mean, "wet_fraction": [float(np.mean([w[k] for w in wet])) / n_mean for k in (0, 1)],
-            "max_depth_diff_vs_plain_m": diff, "compared_at_time": t_done, "plain_time": t_end,
-            "wet_volume_m3": volume, "plain_wet_volume_m3": volume_plain,
-            "proposal": {k: st[k] for k in ("active", "proposed", "subtrees", "learned_steps", "judge_steps",
-                                             "fallbacks", "frozen_leaves")},
-            "mlp": os.path.basename(a.proposal), "judge_every": a.judge_every,
-            "timing": "device time of each step (CUDA events) of a second run of the same case, the plain "
-                      "window's W warm-up and K timed steps from its start time"}
+    out = {"value": v, "ms_per_step": sum(ms) / len(ms), "steps": len(ms), "vs_plain": v / value_plain,
+           "leaves_mean": n_mean, "wet_fraction": [float(np.mean([w[k] for w in wet])) / n_mean for k in (0, 1)],
+           "max_depth_diff_vs_plain_m": diff, "compared_at_time": t_done, "plain_time": t_end,
+           "wet_volume_m3": volume, "plain_wet_volume_m3": volume_plain,
+           "timing": "device time of each step (CUDA events) of a second run of the same case, the plain "
+                     "window's W warm-up and K timed steps from its start time"}
+    if mode == "learned":
+        out["proposal"] = {k: st[k] for k in ("active", "proposed", "subtrees", "learned_steps", "judge_steps",
+                                               "fallbacks", "frozen_leaves")}
+        out["mlp"] = os.path.basename(a.proposal)
+        out["judge_every"] = a.judge_every
+    else:
+        out["decode"] = "keep values (mwdg2_set_decode_mode 1)"
+    return out
 
 
 def run_learned(a):
     """The learned refinement proposal on the 4096^2 catchment: the same
-    case run from t = 0 to --eval-time three times on this GPU -- plain in FP64 (the depth
-    reference), plain in FP32, and in FP32 with the trained MLP proposing the subtrees the
-    encode and decode visit, a full judge step every --judge-every steps. Each run's device
-    time is the sum of its steps' CUDA-event times (input resident, no host copies); the
-    depth error is the largest difference, over every finest cell, of the depth at the cell
-    centre from the FP64 run's at the same simulated time (each run ends exactly at
-    --eval-time). Prints one line for the plain FP32 run and one for the learned run."""
+    case run from t = 0 to --eval-time on this GPU -- plain in FP64 (the depth reference),
+    then in --precision plain, with the trained MLP proposing the subtrees the encode and
+    decode visit (a full judge step every --judge-every steps), and both again with the
+    keep-values decode (mwdg2_set_decode_mode 1). Each run's device time is the sum of its
+    steps' CUDA-event times (input resident, no host copies); the depth error is the largest
+    difference, over every finest cell, of the depth at the cell centre from the FP64 run's
+    at the same simulated time (each run ends exactly at --eval-time). Prints one line per
+    run in --precision."""
     import numpy as np
     import torch
     import cases
@@ -554,8 +571,10 @@ def run_learned(a):
     params = z["params"]
     train = json.loads(str(z["summary"]))
 
-    def run(precision, learned):
+    def run(precision, learned, keep=False):
         sim = mwdg2_b200.Simulation(par, precision=precision, timing="step")
+        if keep:
+            sim.set_decode_mode("keep")
         if learned:
             sim.proposal_enable(params, judge_every=a.judge_every, threshold=train["threshold"], miss_bound=0.02)
         ms, leaves, steps, applied = 0.0, 0, 0, 0
@@ -579,10 +598,11 @@ def run_learned(a):
     # the plain FP64 run is the depth reference; plain and learned run in --precision
     ref = run(64, False)
     plain = ref if a.precision == 64 else run(a.precision, False)
-    learned = run(a.precision, True)
+    runs = (("plain", plain), ("learned", run(a.precision, True)), ("keep", run(a.precision, False, keep=True)),
+            ("learned+keep", run(a.precision, True, keep=True)))
     fp = f"FP{a.precision}"
     lines = []
-    for name, r in (("plain", plain), ("learned", learned)):
+    for name, r in runs:
         err = float(np.max(np.abs(r["depth"] - ref["depth"])))
         line = {"metric": METRIC + f" ({name} {fp} vs plain FP64 depth)", "value": r["leaves"] / (r["ms"] / 1e3),
                 "unit": UNIT, "n_gpus": 1, "steps": r["steps"], "warmup": 0, "ms_per_step": r["ms"] / r["steps"],
@@ -590,15 +610,17 @@ def run_learned(a):
                 "data": "synthetic (seeded fBm DEM, no network)",
                 "config": {"workload": f"fBm catchment {1 << a.level}^2 (max_ref_lvl {a.level}) run from t = 0 to "
                                        f"{a.eval_time:g} s (the hydrograph peak), MWDG2 {fp}",
-                           "proposal": "none" if name == "plain" else
+                           "proposal": "none" if "learned" not in name else
                                        f"trained MLP ({a.proposal.split('/')[-1]}), judge every {a.judge_every} steps",
+                           "decode": "keep values" if "keep" in name else "reference",
                            "depth_reference": "the same case in FP64, plain"},
                 "max_depth_error_m": err, "time": r["time"], "reference_time": ref["time"],
                 "wet_volume_m3": r["wet_volume"], "reference_wet_volume_m3": ref["wet_volume"],
                 "timing": "sum of CUDA-event device times of every step of the run"}
-        if name == "learned":
+        if name != "plain":
             line["vs_plain"] = line["value"] / lines[0]["value"]
-            line["proposal"] = {**learned["stats"], "applied_steps": learned["applied_steps"], "training": train}
+        if "learned" in name:
+            line["proposal"] = {**r["stats"], "applied_steps": r["applied_steps"], "training": train}
         lines.append(line)
     for line in lines:
         print(json.dumps(line), flush=True)
@@ -639,6 +661,7 @@ def main():
     t_init = time.perf_counter()
     # step timing: two events around each step's device work, outside its captured graph
     sim = mwdg2_b200.Simulation(par, precision=a.precision, device=local, timing="step")
+    sim.set_decode_mode(a.decode)
     t_init = time.perf_counter() - t_init   # reading the rasters + device initialisation
     clk = Clocks(local).__enter__()   # sampled from the warm-up through the end-to-end loop
     for _ in range(a.warmup):
@@ -674,9 +697,13 @@ def main():
 
     learned = None
     want_learned = world == 1 and a.workload == "catchment" and a.solver == "mwdg2" and os.path.exists(a.proposal)
+    keep = None
     if want_learned:
         learned = learned_window(a, par, 0.0, sim.info()["time"], finest_depth(sim), value, "learned_window",
                                  wet_volume(sim))
+    if world == 1 and a.workload == "catchment" and a.decode == "reference":
+        keep = learned_window(a, par, 0.0, sim.info()["time"], finest_depth(sim), value, "keep_window",
+                              wet_volume(sim), mode="keep")
 
     # end to end through the C ABI: the library's own time loop (mwdg2_run) over K steps; each
     # step's dt, boundary and point-source values go host->device from pinned memory, and its
@@ -760,6 +787,8 @@ def main():
             "wet_fraction": [float(np.mean([cc[k] for cc in counters])) / n_mean for k in ("wet_stage1", "wet_stage2")]}
     if learned is not None:
         line["learned"] = learned
+    if keep is not None:
+        line["decode_keep"] = keep
     if a.workload == "catchment" and a.peak_time > 0:
         wp = peak_window(sim, a, dist)
         t_end, depth_end = wp.pop("_end_time", None), wp.pop("_end_depth", None)
@@ -767,6 +796,9 @@ def main():
         if want_learned and "value" in wp:
             wp["learned"] = learned_window(a, par, a.peak_time, t_end, depth_end, wp["value"], "learned_peak_window",
                                            wp["wet_volume_m3"])
+        if keep is not None and "value" in wp:
+            wp["decode_keep"] = learned_window(a, par, a.peak_time, t_end, depth_end, wp["value"], "keep_peak_window",
+                                               wp["wet_volume_m3"], mode="keep")
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(par, a, a.cpu_steps)
     sim.close()

@@ -596,9 +596,13 @@ __global__ void __launch_bounds__(256) k_encode_band(Hier<T> hr, Scalars<T>* sc,
 // reference (mra/zero_details.cu).
 // FLAGS = false: values only; the flags of the children are then set by k_extra_sig_level
 // from F_XS, which the encode derived from the same details.
+// keep (the keep-values decode, not in the reference): an encoded parent's children keep
+// the values its encode read, which its decode would return up to rounding; only parents
+// made significant without an encode (refined this step) are decoded, and an encoded
+// parent's extra significance comes from F_XS.
 template <typename T, bool MW, bool FLAGS = true, bool PM = false>
 __device__ __forceinline__ void decode_parent(const Hier<T>& hr, const Scalars<T>* sc, int L, int level, int idx, T eps,
-                                              unsigned& n_done, const PropMask& pm = PropMask{})
+                                              unsigned& n_done, const PropMask& pm = PropMask{}, bool keep = false)
 {
     const int p = lvl_idx(level) + idx;
     // PM: the children of a parent in a subtree the proposal leaves out keep their values
@@ -607,6 +611,12 @@ __device__ __forceinline__ void decode_parent(const Hier<T>& hr, const Scalars<T
     if (!(f & F_SIG)) return;
     const bool enc = (f & F_ENC) != 0;
     const int c = lvl_idx(level + 1) + 4 * idx;
+    if (keep && enc)
+    {
+        ++n_done;
+        if (FLAGS && level <= L - 2 && (f & F_XS)) *reinterpret_cast<uint32_t*>(hr.flags + c) |= 0x01010101u;
+        return;
+    }
     const T mx[3] = {fmax(T(1.0), sc->max_eta), fmax(T(1.0), sc->max_qx), fmax(T(1.0), sc->max_qx)};
     T nd = T(0.0);
 #pragma unroll
@@ -731,9 +741,11 @@ __device__ __forceinline__ T decode_field(const Hier<T>& hr, const Scalars<T>* s
 // Decode levels lo .. lo + depth - 1 top-down (mra/decoding.cu, mra/extra_significance.cu),
 // one thread per parent and field (see k_encode_band); the fields' detail norms are combined
 // in field order, as decode_parent combines them, for extra significance.
+// keep: the keep-values decode (decode_parent): encoded parents are not decoded, and their
+// extra significance comes from F_XS.
 template <typename T, bool MW>
 __device__ __forceinline__ void k_decode_band_body(Hier<T> hr, Scalars<T>* sc, int L, int lo, int depth, T eps,
-                                                                                 PropMask pm = PropMask{})
+                                                                                 PropMask pm = PropMask{}, bool keep = false)
 {
     if (band_left_out(pm, lo)) return;
     static_assert(kBandDepth <= 5, "a band level has at most 4^(kBandDepth - 1) <= 256 parents");
@@ -746,22 +758,28 @@ __device__ __forceinline__ void k_decode_band_body(Hier<T> hr, Scalars<T>* sc, i
         {
             const int fld = t >> sh, j = t & (n - 1);
             const uint8_t f = hr.flags[first + j];
-            if (!(f & F_SIG)) continue;
+            if (!(f & F_SIG) || (keep && (f & F_ENC))) continue;
             s_nd[fld][j] = decode_field<T, MW>(hr, sc, l, base + j, fld, (f & F_ENC) != 0);
         }
         __syncthreads();
         for (int j = threadIdx.x; j < n; j += blockDim.x)
         {
-            if (!(hr.flags[first + j] & F_SIG)) continue;
+            const uint8_t f = hr.flags[first + j];
+            if (!(f & F_SIG)) continue;
             ++done;
             if (l <= L - 2)
             {
-                T nd = T(0.0);
-                nd = fmax(nd, s_nd[0][j]);
-                nd = fmax(nd, s_nd[1][j]);
-                nd = fmax(nd, s_nd[2][j]);
-                if (nd >= extra_eps(eps, L, l, sc))
-                    *reinterpret_cast<uint32_t*>(hr.flags + lvl_idx(l + 1) + 4 * (base + j)) |= 0x01010101u;
+                bool xs;
+                if (keep && (f & F_ENC)) xs = (f & F_XS) != 0;
+                else
+                {
+                    T nd = T(0.0);
+                    nd = fmax(nd, s_nd[0][j]);
+                    nd = fmax(nd, s_nd[1][j]);
+                    nd = fmax(nd, s_nd[2][j]);
+                    xs = nd >= extra_eps(eps, L, l, sc);
+                }
+                if (xs) *reinterpret_cast<uint32_t*>(hr.flags + lvl_idx(l + 1) + 4 * (base + j)) |= 0x01010101u;
             }
         }
         __syncthreads();
@@ -771,9 +789,9 @@ __device__ __forceinline__ void k_decode_band_body(Hier<T> hr, Scalars<T>* sc, i
 }
 template <typename T, bool MW>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4) k_decode_band(Hier<T> hr, Scalars<T>* sc, int L, int lo, int depth, T eps,
-                                                                                 PropMask pm = PropMask{})
+                                                                                 PropMask pm = PropMask{}, bool keep = false)
 {
-    k_decode_band_body<T, MW>(hr, sc, L, lo, depth, eps, pm);
+    k_decode_band_body<T, MW>(hr, sc, L, lo, depth, eps, pm, keep);
 }
 
 // Extra significance of one level of parents from their flags (levels above kBandMaxLevel,
@@ -834,10 +852,11 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4) k_decode_level(Hi
 // in shared memory; the warp's lanes then take the listed parents in turn. A level of 4M
 // parents with a handful significant costs 512K threads that read 8 bytes each instead of
 // 4M threads. Op 0: FULL encode, 1: scale-only re-encode, 2: decode (values only, as
-// k_decode_level).
+// k_decode_level; keep: the keep-values decode of decode_parent, where only the parents
+// refined this step are listed and the encoded ones are just counted).
 template <typename T, bool MW, int OP, bool PM = false>
 __global__ void __launch_bounds__(256) k_level_sparse(Hier<T> hr, Scalars<T>* sc, int L, int level, T eps,
-                                                      PropMask pm = PropMask{})
+                                                      PropMask pm = PropMask{}, bool keep = false)
 {
     if (OP == 1 && sc->min_leaf > level) return;   // see scale_only_needed
     __shared__ int list[8][256];   // per warp: up to 32 lanes x 8 parents
@@ -854,7 +873,11 @@ __global__ void __launch_bounds__(256) k_level_sparse(Hier<T> hr, Scalars<T>* sc
         {
             const uint32_t f = ((j < 4 ? w.x : w.y) >> (8 * (j & 3))) & 0xffu;
             const bool kept = PM && level >= pm.level && pm_out(pm, (int)((first + j) >> (2 * (level - pm.level))));
-            if (f & F_SIG) sig |= kept ? 0u : 1u << j;
+            if (f & F_SIG)
+            {
+                if (OP == 2 && keep && (f & F_ENC)) done += kept ? 0u : 1u;
+                else sig |= kept ? 0u : 1u << j;
+            }
             // FULL encode of a parent that was not significant: only its flag changes (its
             // encode / extra-significance bits from the last step clear, the preflag stays)
             else if (OP == 0 && !kept && (f & ~(uint32_t)F_PRE)) hr.flags[lvl_idx(level) + first + j] = (uint8_t)(f & F_PRE);

@@ -79,6 +79,7 @@ struct SimBase
     virtual mwdg2_status set_timing(int mode) = 0;
     virtual mwdg2_status counters(int64_t* out, int n) = 0;
     virtual mwdg2_status volume(double* out) = 0;
+    virtual mwdg2_status decode_mode(int mode) = 0;
     // learned refinement proposal
     virtual mwdg2_status proposal_record(bool on) = 0;
     virtual mwdg2_status proposal_enable(const float* params, int judge_every, float threshold, float miss_bound) = 0;
@@ -104,7 +105,7 @@ public:
     bool first_step() const override { return first_; }
     int group_key() const override
     {
-        const bool ok = mw_ && !first_ && !finished_ && cs_.epsilon > T(0) && !prop_on() && timing_mode_ == 0 &&
+        const bool ok = mw_ && !first_ && !finished_ && cs_.epsilon > T(0) && !prop_on() && !keep_ && timing_mode_ == 0 &&
                         m_args_ && (cs_.srcs.empty() || m_src_) && cs_.stage_codes.size() <= 64;
         return ok ? (L_ | (sizeof(T) == 8 ? 1 << 8 : 0)) : -1;
     }
@@ -126,6 +127,7 @@ public:
     mwdg2_status set_timing(int mode) override;
     mwdg2_status counters(int64_t* out, int n) override;
     mwdg2_status volume(double* out) override;
+    mwdg2_status decode_mode(int mode) override;
     mwdg2_status proposal_record(bool on) override;
     mwdg2_status proposal_enable(const float* params, int judge_every, float threshold, float miss_bound) override;
     mwdg2_status proposal_stats(double* out, int n) override;
@@ -231,6 +233,9 @@ private:
     // 1 (step): two stream events around the step, outside any graph; 0: none
     int timing_mode_ = 0;
     bool timed_ = false;                // timing_mode_ == 2
+    // keep-values decode (mwdg2_set_decode_mode 1): only the parents refined this step are
+    // decoded; the children of encoded parents keep the values the encode read
+    bool keep_ = false;
     cudaEvent_t ev_[9] = {};
     cudaEvent_t ev_step_[2] = {};
     double last_ms_[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -766,8 +771,9 @@ template <typename T> mwdg2_status Sim<T>::enqueue_device()
         for (size_t k = bands_.size(); k-- > 0;)  // top band first
         {
             const Band& b = bands_[k];
-            if (mw) mw::k_decode_band<T, true><<<b.grid, 256, 0, st_>>>(hr_, sc_, L_, b.lo, b.depth, eps, prop_mask());
-            else mw::k_decode_band<T, false><<<b.grid, 256, 0, st_>>>(hr_, sc_, L_, b.lo, b.depth, eps);
+            if (mw) mw::k_decode_band<T, true><<<b.grid, 256, 0, st_>>>(hr_, sc_, L_, b.lo, b.depth, eps, prop_mask(), keep_);
+            else mw::k_decode_band<T, false><<<b.grid, 256, 0, st_>>>(hr_, sc_, L_, b.lo, b.depth, eps, mw::PropMask{},
+                                                                      keep_);
             ++launches_;
         }
         // the levels above the bands: their flags first (extra significance from F_XS), so
@@ -793,12 +799,13 @@ template <typename T> mwdg2_status Sim<T>::enqueue_device()
             for (int level = mw::kBandMaxLevel + 1; level < L_; ++level)
             {
                 const bool pmk = prop_on() && level >= pm.level;
-                if (sparse_level(level))
+                // keep-values decode: the parents refined this step are few on every level
+                if (keep_ || sparse_level(level))
                 {
                     const int nb = grid_for(((int64_t)1 << (2 * level)) / 8, 256, 1 << 30);
-                    if (pmk) mw::k_level_sparse<T, true, 2, true><<<nb, 256, 0, st_dec_>>>(hr_, sc_, L_, level, eps, pm);
-                    else if (mw) mw::k_level_sparse<T, true, 2><<<nb, 256, 0, st_dec_>>>(hr_, sc_, L_, level, eps);
-                    else mw::k_level_sparse<T, false, 2><<<nb, 256, 0, st_dec_>>>(hr_, sc_, L_, level, eps);
+                    if (pmk) mw::k_level_sparse<T, true, 2, true><<<nb, 256, 0, st_dec_>>>(hr_, sc_, L_, level, eps, pm, keep_);
+                    else if (mw) mw::k_level_sparse<T, true, 2><<<nb, 256, 0, st_dec_>>>(hr_, sc_, L_, level, eps, pm, keep_);
+                    else mw::k_level_sparse<T, false, 2><<<nb, 256, 0, st_dec_>>>(hr_, sc_, L_, level, eps, pm, keep_);
                 }
                 else
                 {
@@ -1586,6 +1593,15 @@ template <typename T> mwdg2_status Sim<T>::set_timing(int mode)
     return MWDG2_OK;
 }
 
+template <typename T> mwdg2_status Sim<T>::decode_mode(int mode)
+{
+    if (mode < 0 || mode > 1) return set_err(MWDG2_ERR_ARG, "set_decode_mode: mode 0 or 1");
+    keep_ = (mode == 1);
+    for (auto& g : graphs_) cudaGraphExecDestroy(g.second.exec);   // they hold the old kernel arguments
+    graphs_.clear();
+    return MWDG2_OK;
+}
+
 template <typename T> mwdg2_status Sim<T>::counters(int64_t* out, int n)
 {
     for (int i = 0; i < n && i < 10; ++i) out[i] = last_cnt_[i];
@@ -2097,6 +2113,12 @@ mwdg2_status mwdg2_volume(mwdg2_sim* s, double* out)
 {
     if (!s || !out) return set_err(MWDG2_ERR_ARG, "null argument");
     return s->impl->volume(out);
+}
+
+mwdg2_status mwdg2_set_decode_mode(mwdg2_sim* s, int mode)
+{
+    if (!s) return set_err(MWDG2_ERR_ARG, "null handle");
+    return s->impl->decode_mode(mode);
 }
 
 mwdg2_status mwdg2_proposal_record(mwdg2_sim* s, int on)

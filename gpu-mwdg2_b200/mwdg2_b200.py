@@ -98,6 +98,8 @@ def lib():
         L.mwdg2_trainer_destroy.argtypes = [vp]
         L.mwdg2_volume.argtypes = [vp, dp]
         L.mwdg2_volume.restype = ctypes.c_int
+        L.mwdg2_set_decode_mode.argtypes = [vp, ctypes.c_int]
+        L.mwdg2_set_decode_mode.restype = ctypes.c_int
         L.mwdg2_proposal_record.argtypes = [vp, ctypes.c_int]
         L.mwdg2_proposal_enable.argtypes = [vp, fp, ctypes.c_int, ctypes.c_float, ctypes.c_float]
         L.mwdg2_proposal_stats.argtypes = [vp, dp, ctypes.c_int]
@@ -261,6 +263,13 @@ class Simulation:
         v = ctypes.c_double()
         _check(lib().mwdg2_volume(self._h, ctypes.byref(v)))
         return v.value
+
+    def set_decode_mode(self, mode: str):
+        """Decode of the following steps (mwdg2_set_decode_mode): "reference" (every
+        significant parent decoded, bit for bit the reference's) or "keep" (children of
+        encoded parents keep their values; only parents refined this step are decoded)."""
+        code = {"reference": 0, "keep": 1}[mode]
+        _check(lib().mwdg2_set_decode_mode(self._h, code))
 
     def proposal_record(self, on: bool = True):
         """Record the proposal's features (step start) and activity labels (step end)."""

@@ -142,6 +142,17 @@ mwdg2_status mwdg2_last_step_counters(mwdg2_sim* sim, int64_t* out, int n);
  * c-prop outputs print states, not volumes). */
 mwdg2_status mwdg2_volume(mwdg2_sim* sim, double* out);
 
+/* Decode of the following steps. 0 (the default): every significant parent's children are
+ * decoded from its scale coefficients and details, as the reference does
+ * (mra/decoding.cu:3-67); trees, neighbours and states follow the reference build bit for
+ * bit. 1 (keep values; no counterpart in the reference): the children of a parent that the
+ * step's encode visited keep the values the encode read (the decode returns them only up to
+ * rounding), and only the parents refined this step are decoded; their extra significance
+ * comes from the encode's detail norms. The same method without the decode's round trip:
+ * in FP32 the depth eta - z of a dry leaf no longer takes the round trip's rounding of eta
+ * every step, and the step skips most of its decode. Graphs captured earlier are dropped. */
+mwdg2_status mwdg2_set_decode_mode(mwdg2_sim* sim, int mode);
+
 void mwdg2_destroy(mwdg2_sim* sim);
 
 /* ---------------------------------------------------------------- batched ensembles

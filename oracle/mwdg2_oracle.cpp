@@ -81,6 +81,12 @@ public:
     std::vector<T> det[4][3][3];  // field (eta,qx,qy,z) x (alpha,beta,gamma) x mode (0,1x,1y)
     std::vector<T> norm;
     std::vector<unsigned char> sig, preflag;
+    // Decode mode of the library's keep-values option (not in the reference): the children
+    // of a parent that this step's encode visited keep the values the encode read, and
+    // only parents made significant without an encode (refined this step) are decoded.
+    // enc[p]: parent p was visited by this step's encode (it was significant at the start).
+    bool keep_values = false;
+    std::vector<unsigned char> enc;
     LeafArrays<T> assem, buf;
     LeafArrays<T> nb[4], buf_nb[4];
     std::vector<unsigned char> flag_ne, flag_sw;
@@ -459,6 +465,7 @@ bool Sim<T>::init(const char* par_path, double eps_override, int solver_override
         if (m == 0 || mw) det[f][t][m].assign(n_det, T(0));
     norm.assign(n_det, T(0));
     sig.assign(n_det, 1);  // mra/init_sig_details.cu
+    enc.assign(n_det, 0);
     assem.alloc(F, true);
     buf.alloc(F, true);
     for (int d = 0; d < 4; ++d) { nb[d].alloc(F, true); buf_nb[d].alloc(F, false); }
@@ -612,7 +619,7 @@ void Sim<T>::encode_flow(bool for_nghbrs)
             const bool was_sig = sig[p] != 0;
             // the multi-block kernel clears the flag of every parent it visits unless it
             // only re-encodes scale coefficients (encode_flow_kernel_mw.cu:78)
-            if (!for_nghbrs) sig[p] = 0;
+            if (!for_nghbrs) { sig[p] = 0; enc[p] = was_sig ? 1 : 0; }
             if (!was_sig) continue;
             const int c = next + 4 * idx;
             T nd = T(0);
@@ -712,6 +719,9 @@ void Sim<T>::decoding()
         {
             const int p = curr + idx;
             if (!sig[p]) continue;
+            // keep-values mode: an encoded parent's children already hold the values its
+            // details were computed from (the decode would return them up to rounding)
+            if (keep_values && enc[p]) continue;
             const int c = next + 4 * idx;
             for (int f = 0; f < 3; ++f)
             {
@@ -1610,6 +1620,13 @@ int oracle_step(void* p, double* dt_out, int* n_leaves_out)
 }
 
 int oracle_num_threads(void) { return omp_get_max_threads(); }
+
+// Keep-values decode (the library's mwdg2_set_decode_mode 1) from the next step on.
+void oracle_set_keep_values(void* p, int on)
+{
+    auto* h = static_cast<OracleHandle*>(p);
+    if (h->f) h->f->keep_values = on != 0; else h->d->keep_values = on != 0;
+}
 
 void oracle_get_leaves(void* p, int* act, int* lvl, int* nb_ids, int* nb_lvls)
 {

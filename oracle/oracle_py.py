@@ -43,6 +43,7 @@ def lib():
         L.oracle_get_hier.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp]
         L.oracle_get_maxes.argtypes = [vp, dp]
         L.oracle_num_threads.restype = ctypes.c_int
+        L.oracle_set_keep_values.argtypes = [vp, ctypes.c_int]
         L.oracle_leaf_topology.restype = ctypes.c_int
         L.oracle_leaf_topology.argtypes = [ctypes.POINTER(ctypes.c_ubyte), ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                            ip, ip, ip, ip]
@@ -139,6 +140,12 @@ class Oracle:
         out = np.zeros(n)
         ok = lib().oracle_get_hier(self._h, field, mode, _p(out, ctypes.c_double))
         return out if ok else None
+
+    def set_keep_values(self, on: bool = True):
+        """Keep-values decode from the next step on (the library's decode mode 1): the
+        children of parents this step's encode visited keep their values; only parents
+        refined this step are decoded."""
+        lib().oracle_set_keep_values(self._h, 1 if on else 0)
 
     def maxes(self) -> np.ndarray:
         out = np.zeros(5)
