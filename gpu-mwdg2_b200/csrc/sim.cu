@@ -184,9 +184,13 @@ private:
     int grid_leaf_ = 0, grid_wet_ = 0, grid_dry_ = 0, grid_stage_ = 0;
     uint8_t* dry_ = nullptr;            // dry marks of RK stage 1 (k_stage_wet -> k_stage_dry)
     uint8_t* dry2_ = nullptr;           // and of stage 2
-    // learned proposal: per hierarchy index, the tag of the last step in which the leaf there
-    // was dry in both stages (k_stage_wet<2>, on steps whose two stages take the wet list)
+    // learned proposal and keep-values decode: per hierarchy index, the tag of the last step
+    // in which the leaf there was dry in both stages (k_stage_wet<2>, on steps whose two
+    // stages take the wet list)
     uint32_t* clean_tag_ = nullptr;
+    // keep-values decode: the dry-leaf writers' mask (nodes of level C + 1, 1 = not frozen):
+    // every subtree may hold frozen leaves but those of the point sources
+    uint8_t* d_keep_prop_ = nullptr;
     cudaStream_t st2_ = nullptr;        // the wet-list kernels, beside the dry-leaf writers
     cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
     // the value decode of the levels above the bands, beside the leaf topology (its own
@@ -239,7 +243,7 @@ private:
     cudaEvent_t ev_[9] = {};
     cudaEvent_t ev_step_[2] = {};
     double last_ms_[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    int64_t last_cnt_[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    int64_t last_cnt_[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     int launches_ = 0;
     // learned refinement proposal (csrc/proposal_sim.cuh): record features and activity labels
     // (prop_rec_), propose the subtrees the encode and decode visit (prop_learned_); every
@@ -264,6 +268,8 @@ private:
     double prop_last_[6] = {0, 0, 0, 0, 0, 0};   // active, missed, proposed, applied, frozen leaves, needed
     double prop_judge_rate_ = 0.0;            // missed / active at the last judge step
     mwdg2_status prop_alloc();
+    mwdg2_status freeze_alloc();        // same-position marks, clean tags (proposal, keep values)
+    mw::PropMask keep_mask() const { return mw::PropMask{d_keep_prop_, prop_C_ + 1}; }
     // outputs
     std::chrono::steady_clock::time_point t_start_;
     double time_mra_ = 0, time_solver_ = 0;
@@ -300,9 +306,11 @@ private:
         {
             uint8_t* marks = STAGE == 1 ? dry_ : dry2_;
             // learned proposal: stage 2 tags the leaves that stayed dry in both stages, and
-            // leaves left out by the proposal are frozen, when both stages take the list
+            // leaves left out by the proposal are frozen, when both stages take the list;
+            // keep-values decode: the decode leaves every persistent leaf as it stands, so
+            // the dry leaves of every subtree but the point sources' may be frozen
             const bool lists = use_list(1) && use_list(2);
-            const mw::PropMask pm = lists ? prop_mask() : mw::PropMask{};
+            const mw::PropMask pm = !lists ? mw::PropMask{} : keep_ && d_keep_prop_ ? keep_mask() : prop_mask();
             mw::k_stage_wet<T, STAGE><<<grid_wet_, 256, 0, st_>>>(lf_, hin, sc_, P_, d_args_, marks, wet_list_, dry_,
                                                                   STAGE == 2 && lists ? clean_tag_ : nullptr);
             cudaEventRecord(ev_fork_, st_);
@@ -907,6 +915,7 @@ template <typename T> mwdg2_status Sim<T>::collect_step()
     last_cnt_[7] = mw ? sc_host_->wet[1] : 0;
     last_cnt_[8] = (int64_t)(sizeof(mw::StepArgs<T>) + sizeof(mw::Src<T>) * cs_.srcs.size());
     last_cnt_[9] = (int64_t)scal_bytes_;
+    last_cnt_[10] = mw ? (int64_t)sc_host_->prop_frozen : 0;
     return MWDG2_OK;
 }
 
@@ -1019,6 +1028,21 @@ template <typename T> mwdg2_status Sim<T>::volume(double* out)
     return MWDG2_OK;
 }
 
+template <typename T> mwdg2_status Sim<T>::freeze_alloc()
+{
+    if (!lf_.same)
+    {
+        if (mwdg2_status s = dalloc(lf_.same, F_)) return s;
+        CU(cudaMemset(lf_.same, 0, F_));
+    }
+    if (!clean_tag_)
+    {
+        if (mwdg2_status s = dalloc(clean_tag_, n_all_)) return s;
+        CU(cudaMemset(clean_tag_, 0, sizeof(uint32_t) * (size_t)n_all_));
+    }
+    return MWDG2_OK;
+}
+
 template <typename T> mwdg2_status Sim<T>::prop_alloc()
 {
     if (!mw_) return set_err(MWDG2_ERR_STATE, "the refinement proposal applies to MWDG2 only");
@@ -1038,10 +1062,7 @@ template <typename T> mwdg2_status Sim<T>::prop_alloc()
         if (!nodes.empty())
             CU(cudaMemcpy(d_prop_src_, nodes.data(), sizeof(int32_t) * nodes.size(), cudaMemcpyHostToDevice));
     }
-    if (mwdg2_status s = dalloc(lf_.same, F_)) return s;
-    CU(cudaMemset(lf_.same, 0, F_));
-    if (mwdg2_status s = dalloc(clean_tag_, n_all_)) return s;
-    CU(cudaMemset(clean_tag_, 0, sizeof(uint32_t) * (size_t)n_all_));
+    if (mwdg2_status s = freeze_alloc()) return s;
     if (mwdg2_status s = dalloc(d_act_, (size_t)prop_nC_ * 4)) return s;
     if (mwdg2_status s = dalloc(d_prop_, (size_t)prop_nC_ * 4)) return s;
     if (mwdg2_status s = dalloc(d_sig5_, (size_t)prop_nC_ * 4)) return s;
@@ -1596,6 +1617,18 @@ template <typename T> mwdg2_status Sim<T>::set_timing(int mode)
 template <typename T> mwdg2_status Sim<T>::decode_mode(int mode)
 {
     if (mode < 0 || mode > 1) return set_err(MWDG2_ERR_ARG, "set_decode_mode: mode 0 or 1");
+    CU(cudaSetDevice(device_));
+    if (mode == 1 && mw_ && !d_keep_prop_)
+    {
+        if (mwdg2_status s = freeze_alloc()) return s;
+        const int C = mw::proposal_level(L_);
+        const int64_t n = (int64_t)1 << (2 * (C + 1));
+        std::vector<uint8_t> mask((size_t)n, 0);
+        for (const auto& src : cs_.srcs) mask[(size_t)(src.code >> (2 * (L_ - (C + 1))))] = 1;
+        if (mwdg2_status s = dalloc(d_keep_prop_, (size_t)n)) return s;
+        CU(cudaMemcpy(d_keep_prop_, mask.data(), (size_t)n, cudaMemcpyHostToDevice));
+        prop_C_ = C;
+    }
     keep_ = (mode == 1);
     for (auto& g : graphs_) cudaGraphExecDestroy(g.second.exec);   // they hold the old kernel arguments
     graphs_.clear();
@@ -1604,7 +1637,7 @@ template <typename T> mwdg2_status Sim<T>::decode_mode(int mode)
 
 template <typename T> mwdg2_status Sim<T>::counters(int64_t* out, int n)
 {
-    for (int i = 0; i < n && i < 10; ++i) out[i] = last_cnt_[i];
+    for (int i = 0; i < n && i < 11; ++i) out[i] = last_cnt_[i];
     return MWDG2_OK;
 }
 

@@ -457,7 +457,9 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4) k_stage_wet(Leave
 // U^n, which is re-inserted into the hierarchy and enters the next step's maxima.
 // pm (learned refinement proposal, applied steps with both stages over the wet list): a
 // leaf inside a subtree the proposal left out (its subtree's encode and decode are skipped
-// too) keeps its state as it stands in the hierarchy where nothing has changed it.
+// too) keeps its state as it stands in the hierarchy where nothing has changed it. With the
+// keep-values decode, which rewrites no leaf that persists, pm leaves out every subtree but
+// those holding point sources.
 // Stage 1 leaves such a dry leaf's U* in the stage hierarchy as it stands when the leaf was
 // a leaf dry in both stages of the last step (clean_tag[a], at its hierarchy index, is the
 // last step's tag: written by that step's stage-2 wet test; null when that step did not

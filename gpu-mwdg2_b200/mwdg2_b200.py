@@ -310,10 +310,10 @@ class Simulation:
         return dict(zip(keys, a.tolist()))
 
     def last_step_counters(self) -> dict:
-        out = np.zeros(10, np.int64)
-        _check(lib().mwdg2_last_step_counters(self._h, _p(out, ctypes.c_int64), 10))
+        out = np.zeros(11, np.int64)
+        _check(lib().mwdg2_last_step_counters(self._h, _p(out, ctypes.c_int64), 11))
         return dict(zip(("encoded", "reencoded", "decoded", "leaves", "detail_slots", "launches", "wet_stage1",
-                         "wet_stage2", "h2d_bytes", "d2h_bytes"), out.tolist()))
+                         "wet_stage2", "h2d_bytes", "d2h_bytes", "frozen_leaves"), out.tolist()))
 
 
 def _opts(precision, epsilon, solver, dirroot, write_outputs, device, timing) -> Opts:

@@ -134,7 +134,8 @@ mwdg2_status mwdg2_set_timing(mwdg2_sim* sim, int mode);
  * [3] leaves (N_a), [4] detail slots (T = get_lvl_idx(L) - 3), [5] kernels launched in the
  * step, [6] / [7] MWDG2 leaves not dry in RK stage 1 / stage 2 (0 for HWFV1), [8] bytes the
  * step copied host->device (dt, boundary and point-source values), [9] bytes it copied
- * device->host (its scalars and the stage-point values). n <= 10. */
+ * device->host (its scalars and the stage-point values), [10] dry leaves that the RK stages
+ * left as they stood (keep-values decode or learned proposal; MWDG2). n <= 11. */
 mwdg2_status mwdg2_last_step_counters(mwdg2_sim* sim, int64_t* out, int n);
 
 /* Water volume of the current state, sum over leaves of h0 x leaf area (m^3), reduced on
@@ -150,7 +151,11 @@ mwdg2_status mwdg2_volume(mwdg2_sim* sim, double* out);
  * rounding), and only the parents refined this step are decoded; their extra significance
  * comes from the encode's detail norms. The same method without the decode's round trip:
  * in FP32 the depth eta - z of a dry leaf no longer takes the round trip's rounding of eta
- * every step, and the step skips most of its decode. Graphs captured earlier are dropped. */
+ * every step, and the step skips most of its decode. Since nothing then rewrites a leaf
+ * that persists, an MWDG2 leaf that was dry in both RK stages of the last step and is dry
+ * again keeps its state as it stands (the dry-leaf writers skip it; the leaves holding point
+ * sources excepted), on steps whose two stages take the wet list. Graphs captured earlier
+ * are dropped. */
 mwdg2_status mwdg2_set_decode_mode(mwdg2_sim* sim, int mode);
 
 void mwdg2_destroy(mwdg2_sim* sim);

@@ -6,7 +6,9 @@ rounding, mra/decoding.cu:3-67).
 * Against the CPU oracle's keep-values option (FP64): leaves, neighbours and significance
   flags bit-exact every step, state within 1e-10 relative to max(1, |value|), dt within
   1e-9, on a partly wet fBm catchment with Manning friction and the slope limiter (wet-list
-  stages from step 2) and on a dry-start catchment with a point inflow, MWDG2 and HWFV1.
+  stages from step 2) and on a dry-start catchment with a point inflow, MWDG2 and HWFV1;
+  the MWDG2 runs leave the leaves that stay dry as they stand (frozen: the oracle writes
+  them, to the same values up to the last bit of eta = h + z).
 * Against this library's reference decode (FP64, 30 steps of the inflow catchment): the
   same trees every step and states within 1e-9 relative: the two decodes differ by the
   round trip's rounding only.
@@ -52,11 +54,13 @@ def test_keep_values_matches_oracle(tmp_path, solver, case):
     orc = oracle_py.Oracle(c.par, 64)
     sim.set_decode_mode("keep")
     orc.set_keep_values(True)
+    frozen = 0
     try:
         for s in range(1, steps + 1):
             ok, dt, n = sim.step()
             ok2, dt2, n2 = orc.step()
             assert ok and ok2 and n == n2, f"step {s}: leaves {n} vs {n2}"
+            frozen += sim.last_step_counters()["frozen_leaves"]
             lv, lo = sim.leaves(), orc.leaves()
             if solver == "hwfv1":
                 lv.pop("nb_lvls")
@@ -71,6 +75,8 @@ def test_keep_values_matches_oracle(tmp_path, solver, case):
     finally:
         sim.close()
         orc.close()
+    # MWDG2 steps with both stages over the wet list freeze the leaves that stay dry
+    assert (frozen > 0) == (solver == "mwdg2"), frozen
 
 
 @pytest.mark.parametrize("solver", ["mwdg2", "hwfv1"])
