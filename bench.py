@@ -86,7 +86,8 @@ def workload(a) -> dict:
     return {"workload": f"fBm catchment {1 << a.level}^2 finest cells (max_ref_lvl {a.level}), 2 m cells, "
                         "Hurst 0.8, relief 0-30 m, Manning 0.03, dry start, west point inflow 50 m3/s peak at 30 min, "
                         "epsilon 1e-3",
-            "solver": a.solver, "precision": f"fp{a.precision}", "max_ref_lvl": a.level, "decode": a.decode,
+            "solver": a.solver, "precision": f"fp{a.precision}", "max_ref_lvl": a.level,
+            "decode": getattr(a, "decode", "reference"),
             "steps_from": "simulation start (steps W+1..W+K of the run)",
             "l2": "inputs larger than L2 (hierarchy arrays >= 1 GB)"}
 
