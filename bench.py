@@ -299,7 +299,9 @@ def run_ensemble(a):
     mwdg2_batch_step, against the same members each stepped alone, one after another. Both
     are timed on the host clock around synchronised loops (the batch has one stream per
     member); a step of a member updates its leaves once. Every member takes W warm-up steps,
-    then K timed steps (members that reach their end time stop earlier)."""
+    then K timed steps (members that reach their end time stop earlier). With --decode keep
+    both take the keep-values decode, and the line adds the same members stepped one after
+    another with the reference decode (the plain form)."""
     import numpy as np
     import torch
     import cases
@@ -315,6 +317,8 @@ def run_ensemble(a):
     sizes = [1 << (int(open(p).read().split("max_ref_lvl")[1].split()[0])) for p in pars]
 
     with mwdg2_b200.Batch(pars, precision=a.precision) as b:
+        for i in range(len(pars)):
+            b.member(i).set_decode_mode(a.decode)
         for _ in range(a.warmup):
             b.step()
         torch.cuda.synchronize()
@@ -327,21 +331,26 @@ def run_ensemble(a):
         torch.cuda.synchronize()
         t_batch = time.perf_counter() - t0
 
-    t_seq, upd_seq = 0.0, 0
-    for p in pars:
-        s = mwdg2_b200.Simulation(p, precision=a.precision)
-        for _ in range(a.warmup):
-            s.step()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for _ in range(a.steps):
-            ok, _, n = s.step()
-            if not ok:
-                break
-            upd_seq += n
-        torch.cuda.synchronize()
-        t_seq += time.perf_counter() - t0
-        s.close()
+    def sequential(mode):
+        t_seq, upd_seq = 0.0, 0
+        for p in pars:
+            s = mwdg2_b200.Simulation(p, precision=a.precision)
+            s.set_decode_mode(mode)
+            for _ in range(a.warmup):
+                s.step()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(a.steps):
+                ok, _, n = s.step()
+                if not ok:
+                    break
+                upd_seq += n
+            torch.cuda.synchronize()
+            t_seq += time.perf_counter() - t0
+            s.close()
+        return t_seq, upd_seq
+
+    t_seq, upd_seq = sequential(a.decode)
     line = {"metric": "active-cell updates/s (batched ensemble of adaptive MWDG2 time steps)",
             "value": upd / t_batch, "unit": UNIT, "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
             "higher_is_better": True, "impl": "ours-batch", "dtype": f"f{a.precision}",
@@ -354,7 +363,11 @@ def run_ensemble(a):
                        "timing": "host clock around synchronised loops"},
             "batch": {"seconds": t_batch, "member_steps": member_steps, "leaf_updates": upd},
             "sequential": {"value": upd_seq / t_seq, "seconds": t_seq, "leaf_updates": upd_seq},
-            "batch_over_sequential": (upd / t_batch) / (upd_seq / t_seq)}
+            "batch_over_sequential": (upd / t_batch) / (upd_seq / t_seq), "decode": a.decode}
+    if a.decode != "reference":
+        t_ref, upd_ref = sequential("reference")
+        line["sequential_reference_decode"] = {"value": upd_ref / t_ref, "seconds": t_ref, "leaf_updates": upd_ref}
+        line["batch_over_sequential_reference_decode"] = (upd / t_batch) / (upd_ref / t_ref)
     print(json.dumps(line), flush=True)
 
 
