@@ -24,6 +24,12 @@ def test_defaults_are_one_gpu_and_three_warmup_steps():
     assert "4096^2" in w["workload"] and w["max_ref_lvl"] == 12 and "L2" in w["l2"]
 
 
+def test_decode_defaults_to_the_reference_decode():
+    a = _parse()
+    assert a.decode == "reference" and bench.workload(a)["decode"] == "reference"
+    assert bench.workload(_parse("--decode", "keep"))["decode"] == "keep"
+
+
 def test_urban_workload_defaults_to_8192():
     a = _parse("--workload", "urban")
     assert a.level == 13
