@@ -62,6 +62,7 @@ def test_null_handle_calls_are_rejected():
     lib = mwdg2_b200.lib()
     assert lib.mwdg2_step(None, None, None) == 6
     assert lib.mwdg2_info(None, None, 0) == 6
+    assert lib.mwdg2_set_decode_mode(None, 1) == 6
 
 
 def _static_topology():
