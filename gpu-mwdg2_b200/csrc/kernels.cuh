@@ -24,6 +24,12 @@ template <typename T> struct Hier
 {
     T* s[4][3];
     uint8_t* flags;
+    // Keep-values decode, stage hierarchy only (null otherwise): per hierarchy index,
+    // (step tag << 1) | changed for the step in which the slot's value was last made
+    // current; changed = 1 where that step wrote a value (RK stage 1 at a leaf, the scale
+    // re-encode at a parent), 0 where it confirmed the one standing (a frozen dry leaf, a
+    // parent whose children all stood). See encode_parent.
+    uint32_t* tag = nullptr;
 };
 
 template <typename T> struct Leaves
@@ -356,6 +362,23 @@ __device__ __forceinline__ void encode_parent(const Hier<T>& hr, const Scalars<T
     if (!FULL)
     {
         if (!was_sig) return;
+        uint32_t mark = 0;
+        if (hr.tag)
+        {
+            // keep-values decode: a parent made current in the last step whose four children
+            // all stand unchanged in this one (frozen leaves, parents confirmed below) keeps
+            // its scale coefficients, which this encode would compute again from the same
+            // values; children are 4 consecutive slots, 16-byte aligned (lvl_idx(l) is a
+            // multiple of 4 for l >= 1)
+            const uint32_t now = sc->step_tag << 1;
+            const uint4 ct = *reinterpret_cast<const uint4*>(hr.tag + c);
+            if (ct.x == now && ct.y == now && ct.z == now && ct.w == now && (hr.tag[p] >> 1) == sc->step_tag - 1u)
+            {
+                hr.tag[p] = now;
+                return;
+            }
+            mark = now | 1u;
+        }
 #pragma unroll
         for (int fld = 0; fld < 3; ++fld)
         {
@@ -374,6 +397,7 @@ __device__ __forceinline__ void encode_parent(const Hier<T>& hr, const Scalars<T
                 hr.s[fld][0][p] = hw_scale(k);
             }
         }
+        if (mark) hr.tag[p] = mark;
         ++n_done;
         return;
     }

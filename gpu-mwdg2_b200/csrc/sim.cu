@@ -191,6 +191,8 @@ private:
     // keep-values decode: the dry-leaf writers' mask (nodes of level C + 1, 1 = not frozen):
     // every subtree may hold frozen leaves but those of the point sources
     uint8_t* d_keep_prop_ = nullptr;
+    // keep-values decode: the stage hierarchy's slot tags (mw::Hier::tag)
+    uint32_t* hs_tag_ = nullptr;
     cudaStream_t st2_ = nullptr;        // the wet-list kernels, beside the dry-leaf writers
     cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
     // the value decode of the levels above the bands, beside the leaf topology (its own
@@ -1628,8 +1630,15 @@ template <typename T> mwdg2_status Sim<T>::decode_mode(int mode)
         if (mwdg2_status s = dalloc(d_keep_prop_, (size_t)n)) return s;
         CU(cudaMemcpy(d_keep_prop_, mask.data(), (size_t)n, cudaMemcpyHostToDevice));
         prop_C_ = C;
+        if (mwdg2_status s = dalloc(hs_tag_, n_all_)) return s;
     }
     keep_ = (mode == 1);
+    if (mw_)
+    {
+        // no slot counts as current from before the switch
+        if (hs_tag_) CU(cudaMemset(hs_tag_, 0xff, sizeof(uint32_t) * (size_t)n_all_));
+        hs_.tag = keep_ ? hs_tag_ : nullptr;
+    }
     for (auto& g : graphs_) cudaGraphExecDestroy(g.second.exec);   // they hold the old kernel arguments
     graphs_.clear();
     return MWDG2_OK;

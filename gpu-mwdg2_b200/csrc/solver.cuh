@@ -338,7 +338,7 @@ __device__ __forceinline__ bool leaf_is_dry(const Hier<T>& hr, T own_h0, const i
 // Leaf state u (h, qx, qy by mode, the layout of Leaves::un) into the hierarchy at `a`,
 // depths as surface elevations eta = h + z (mra/reinsert_assem_sol.cu:3-32).
 template <typename T>
-__device__ __forceinline__ void put_leaf(const Hier<T>& hr, int a, const T (&u)[9], const T (&z)[3])
+__device__ __forceinline__ void put_leaf(const Hier<T>& hr, int a, const T (&u)[9], const T (&z)[3], uint32_t mark = 0)
 {
 #pragma unroll
     for (int m = 0; m < 3; ++m)
@@ -347,6 +347,7 @@ __device__ __forceinline__ void put_leaf(const Hier<T>& hr, int a, const T (&u)[
         hr.s[1][m][a] = u[3 + m];
         hr.s[2][m][a] = u[6 + m];
     }
+    if (hr.tag) hr.tag[a] = mark;   // the stage hierarchy of the keep-values decode
 }
 
 // Running maxima of the state at the end of a step, as the next step's
@@ -475,6 +476,7 @@ __device__ __forceinline__ void k_stage_dry_body(int bid, int nb, Leaves<T> lf, 
                                                    const uint32_t* clean_tag = nullptr)
 {
     const uint32_t last_tag = sc->step_tag - 1u;
+    const uint32_t wmark = (sc->step_tag << 1) | 1u;   // a written stage-hierarchy slot (Hier::tag)
     const int n = sc->n_leaves;
     const int stride = nb * blockDim.x;
     StateMax<T> mx;
@@ -503,6 +505,7 @@ __device__ __forceinline__ void k_stage_dry_body(int bid, int nb, Leaves<T> lf, 
             {
                 dry[i] = 2;
                 ++frozen;
+                if (hout.tag) hout.tag[a] = wmark & ~1u;   // U* stands
                 if (lf.same[i]) continue;
                 keep_ustar = true;   // un only
             }
@@ -541,7 +544,7 @@ __device__ __forceinline__ void k_stage_dry_body(int bid, int nb, Leaves<T> lf, 
             mx.add(u, z[0]);
             if (P.dt_leaf) P.dt_leaf[i] = P.initial_tstep;
         }
-        put_leaf(hout, a, u, z);
+        put_leaf(hout, a, u, z, wmark);
     }
     if (STAGE == 2) mx.flush(sc);
     if (STAGE == 1 && pm.prop)
@@ -580,6 +583,7 @@ __device__ __forceinline__ void k_mwdg2_stage_body(int bid, int nb, Leaves<T> lf
     bool nan_seen = false;
     unsigned n_wet = 0;
     const T max_h = (STAGE == 1) ? fmax(T(1.0), sc->max_h) : sc->max_h2;
+    const uint32_t wmark = (sc->step_tag << 1) | 1u;   // a written stage-hierarchy slot (Hier::tag)
     for (int k = bid * blockDim.x + threadIdx.x; k < n; k += nb * blockDim.x)
     {
         const int i = LIST ? wet[k] : k;
@@ -631,7 +635,7 @@ __device__ __forceinline__ void k_mwdg2_stage_body(int bid, int nb, Leaves<T> lf
                 for (int k = 0; k < 9; ++k) u[k] = lf.un[k][i];
                 mx.add(u, own.z[0]);
             }
-            put_leaf(hout, a, u, own.z);
+            put_leaf(hout, a, u, own.z, wmark);
             if (STAGE == 2 && P.dt_leaf) P.dt_leaf[i] = P.initial_tstep;
             dt_loc = fmin(dt_loc, P.initial_tstep);
             continue;
@@ -721,16 +725,16 @@ __device__ __forceinline__ void k_mwdg2_stage_body(int bid, int nb, Leaves<T> lf
                 nan_seen |= (u[0] != u[0]);
                 mx.add(u, own.z[0]);
             }
-            put_leaf(hout, a, u, own.z);
+            put_leaf(hout, a, u, own.z, wmark);
         }
-        else if (STAGE == 1) put_leaf(hout, a, pre, own.z);
+        else if (STAGE == 1) put_leaf(hout, a, pre, own.z, wmark);
         else
         {
             T u[9];
 #pragma unroll
             for (int k = 0; k < 9; ++k) u[k] = lf.un[k][i];
             mx.add(u, own.z[0]);
-            put_leaf(hout, a, u, own.z);
+            put_leaf(hout, a, u, own.z, wmark);
         }
         if (STAGE == 2 && P.dt_leaf) P.dt_leaf[i] = leaf_dt;
         dt_loc = fmin(dt_loc, leaf_dt);
