@@ -154,8 +154,9 @@ mwdg2_status mwdg2_volume(mwdg2_sim* sim, double* out);
  * every step, and the step skips most of its decode. Since nothing then rewrites a leaf
  * that persists, an MWDG2 leaf that was dry in both RK stages of the last step and is dry
  * again keeps its state as it stands (the dry-leaf writers skip it; the leaves holding point
- * sources excepted), on steps whose two stages take the wet list. Graphs captured earlier
- * are dropped. */
+ * sources excepted), on steps whose two stages take the wet list, and the scale re-encode
+ * between the stages keeps a parent whose four children all stand unchanged. Results are
+ * those of the same decode without these skips. Graphs captured earlier are dropped. */
 mwdg2_status mwdg2_set_decode_mode(mwdg2_sim* sim, int mode);
 
 void mwdg2_destroy(mwdg2_sim* sim);
