@@ -1635,8 +1635,9 @@ template <typename T> mwdg2_status Sim<T>::decode_mode(int mode)
     keep_ = (mode == 1);
     if (mw_)
     {
-        // no slot counts as current from before the switch
-        if (hs_tag_) CU(cudaMemset(hs_tag_, 0xff, sizeof(uint32_t) * (size_t)n_all_));
+        // no slot counts as current from before the switch (on the simulation's stream, ahead
+        // of its next step: the legacy stream does not order with a non-blocking stream)
+        if (hs_tag_) CU(cudaMemsetAsync(hs_tag_, 0xff, sizeof(uint32_t) * (size_t)n_all_, st_));
         hs_.tag = keep_ ? hs_tag_ : nullptr;
     }
     for (auto& g : graphs_) cudaGraphExecDestroy(g.second.exec);   // they hold the old kernel arguments
