@@ -8,7 +8,8 @@ rounding, mra/decoding.cu:3-67).
   1e-9, on a partly wet fBm catchment with Manning friction and the slope limiter (wet-list
   stages from step 2) and on a dry-start catchment with a point inflow, MWDG2 and HWFV1;
   the MWDG2 runs leave the leaves that stay dry as they stand (frozen: the oracle writes
-  them, to the same values up to the last bit of eta = h + z).
+  them, to the same values up to the last bit of eta = h + z), and their scale re-encode
+  keeps the parents whose children all stand (the oracle computes them again).
 * Against this library's reference decode (FP64, 30 steps of the inflow catchment): the
   same trees every step and states within 1e-9 relative: the two decodes differ by the
   round trip's rounding only.
